@@ -1,0 +1,237 @@
+/*
+ * qpsdm_engine.h -- C ABI of the B200 Q-compensated Kirchhoff PSDM engine.
+ *
+ * This is the drop-in boundary for the imaging path of resetlla/q_psdm.  The
+ * reference has no plugin API: its hot path sits behind the per-trace C++
+ * call psdm_kernel(segy tr, ~75 scalars ...) (src/q-psdm.cu:252-283, body
+ * :2063-2244), called by the consumer threads (src/q-psdm.cu:1928-2061),
+ * with line state set up by qpsdm() (src/q-psdm.cu:1298-1376, :1495-1515,
+ * :1653-1691) and tables loaded by get_ttt_all() (src/q-psdm.cu:2382-2622).
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Plain C types and pointers; no CUDA or torch types in signatures.
+ *     Streams are passed as void* (a cudaStream_t; NULL = the engine's own).
+ *   - Every call returns an int status (QPSDM_OK == 0).  The library never
+ *     exits the process; qpsdm_last_error() gives the message.
+ *   - One engine handle per host thread; a handle is bound to one device.
+ *   - Host pointers are read during the call (or, for the _async calls,
+ *     until the next qpsdm_fence()).  Device pointers ("d_" prefix) must be
+ *     memory of the engine's device.
+ */
+#ifndef QPSDM_ENGINE_H_
+#define QPSDM_ENGINE_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QPSDM_ABI_VERSION 1
+#define QPSDM_NAZ 18 /* azimuth sectors, src/q-psdm.cu:1177 */
+#define QPSDM_SU_HDR_BYTES 240
+
+enum {
+  QPSDM_OK = 0,
+  QPSDM_EINVAL = 1,   /* bad argument or size */
+  QPSDM_ECUDA = 2,    /* CUDA runtime error */
+  QPSDM_ENOMEM = 3,   /* device or pinned allocation failed */
+  QPSDM_ESTATE = 4,   /* call out of order (e.g. submit before begin_offset) */
+  QPSDM_ETIMEOUT = 5, /* a bounded device wait gave up */
+  QPSDM_ENOTSUP = 6,
+  QPSDM_ENOKERNEL = 7 /* no sm_100a image for this device */
+};
+
+enum { QPSDM_MODE_COMPAT = 0, QPSDM_MODE_PHYSICS = 1 };
+enum { QPSDM_PANEL_FP32 = 0, QPSDM_PANEL_BF16 = 1, QPSDM_PANEL_FP16 = 2 };
+
+typedef struct qpsdm_engine qpsdm_engine;
+
+/* Traveltime / t* table descriptor, byte-identical to ttt_desc_t
+ * (src/q-psdm.cu:103-109) and to the 16-byte records of Lxxx.{tidx,qidx}. */
+typedef struct {
+  int64_t idx; /* float offset of the cell's block in the data array */
+  uint16_t nys, nxs, dys, dxs; /* local surface grid: nodes and spacing (m) */
+} qpsdm_ttt_desc;
+
+/* Line-independent parameters: mirrors CPUParamsNoLine
+ * (src/q-psdm.cu:111-147) plus the engine's own options.
+ * qpsdm_static_params_init() fills the derived members the way qpsdm()
+ * does (src/q-psdm.cu:1201-1287). */
+typedef struct {
+  /* from the command line / par.dat */
+  float dyi, dxi;  /* image line and cdp spacing (m) */
+  int nxi, nzi;    /* image cdps per line, depth samples */
+  int ntl;         /* samples per input trace */
+  double scaled;   /* coordinate scale of the data (getscale(scalco)) */
+  int fci;         /* first image cdp */
+  float dzi;       /* image depth step (m) */
+  float dt;        /* input sample interval (s) */
+  float fc;        /* reference frequency (Hz) of the dispersion law */
+  float f1, f3, f4;/* band: low cut, high-cut start and end (Hz) */
+  float threshold; /* gain limit G (linear) */
+  float contract, taperzone; /* degrees on input, radians after init */
+  float fxv1, fyv1, exv1, eyv1; /* velocity-grid bbox padded +-2 km / +-1 km */
+  float dzii;      /* table depth-node spacing (m) */
+  /* derived by qpsdm_static_params_init */
+  float eps;       /* azimuth table step, 0.001 */
+  int nfft, nffti; /* npfar(ntl), npfar(2*ntl) */
+  float dt1;       /* resampled interval 1/(nffti*df) */
+  float df, dw;    /* 1/(nfft*dt), 2*pi*df */
+  float lnG, coef1, coef2, coef3, coef4; /* gain-limit law */
+  /* engine options */
+  int mode;        /* QPSDM_MODE_* */
+  int panel_dtype; /* QPSDM_PANEL_* (physics mode) */
+  int nbins;       /* t* bins of the compensated panels (physics mode) */
+  float dtstar;    /* t* bin spacing (s) */
+  int max_batch;   /* largest ntr of one submit (sizes device buffers) */
+  int kahan;       /* 1 = compensated FP32 image accumulation (physics) */
+  int reserved[8];
+} qpsdm_static_params;
+
+/* Per-line state: mirrors the line part of CPUParamsWithLine
+ * (src/q-psdm.cu:149-179) and the line buffers of GPUParamsWithLine
+ * (src/q-psdm.cu:195-213).  Replaces the per-line H2D block of qpsdm()
+ * (src/q-psdm.cu:1463-1515) and get_ttt_all() (src/q-psdm.cu:2382-2622).
+ * All pointers are host memory, copied during qpsdm_set_line. */
+typedef struct {
+  double fxi, cyi;       /* x of the first image cdp, y of this line */
+  const float *dipx1, *dipx2, *dipy1, *dipy2; /* [nxi][nzi] dip tangents */
+  const int *nf3;        /* [nxi][nzi] high-cut bin (physics; may be NULL) */
+  const float *q;        /* [nxi][nzi] dw/(2Q) field (may be NULL) */
+  /* traveltime (ttt) and t* (qqq) tables in the reference layout */
+  int nxg, nzg, nxi1, nzi1;
+  int ttt_cdp1, ttt_cdp2; /* absolute cdp range of the tables */
+  const qpsdm_ttt_desc *ttt_desc, *qqq_desc; /* [nxg*nzg], may be NULL in compat */
+  const float *ttt, *qqq;                    /* table data */
+  int64_t ttt_len, qqq_len;                  /* floats in ttt, qqq */
+} qpsdm_line_params;
+
+/* One offset group inside one x block: mirrors the per-offset members of
+ * CPUParamsWithLine and the window split of qpsdm()
+ * (src/q-psdm.cu:1593-1691).  qpsdm_offset_params_init() derives them. */
+typedef struct {
+  int ioffs;
+  int ixstart, ixend;          /* image block [ixstart, ixend) */
+  int itb1, itb2, nsb;         /* FFT windows */
+  float tdstart1, tdstart2, tdmid;
+  int nf1, nww, ncoef1;
+  float df, dw;
+  int aznx1[QPSDM_NAZ], aznx2[QPSDM_NAZ]; /* aperture (cdps) per azimuth */
+  int azny1[QPSDM_NAZ], azny2[QPSDM_NAZ]; /* aperture (lines) per azimuth */
+  int zero_image;              /* 1 = clear the block image (opcrp) */
+} qpsdm_offset_params;
+
+/* ---- parameter derivation (host only, no device work) -------------------*/
+
+/* npfar(): smallest valid real prime-factor FFT length >= nmin
+ * (src/fft.cc:491-494, get_opt_n_fftw src/fft.cc:3721). */
+int qpsdm_npfar(int nmin);
+
+/* Fills eps, nfft, nffti, dt1, df, dw, lnG, coef1..4 and converts contract
+ * and taperzone to radians, as qpsdm() does (src/q-psdm.cu:1201-1287). */
+int qpsdm_static_params_init(qpsdm_static_params *p);
+
+/* Azimuth sector table (src/q-psdm.cu:1167-1193); writes up to cap ints,
+ * returns the table length (2001 for eps = 0.001) or -1. */
+int qpsdm_build_iaztab(float eps, int *iaztab, int cap);
+
+/* Window split and bins of one offset group (src/q-psdm.cu:1593-1645). */
+int qpsdm_offset_params_init(const qpsdm_static_params *p, int ixstart,
+                             int ixend, qpsdm_offset_params *o);
+
+/* ---- engine lifetime -----------------------------------------------------*/
+
+/* Replaces the per-consumer set-up of qpsdm() (src/q-psdm.cu:1298-1376).
+ * iaztab: naztab ints (host).  Allocates all device buffers for max_batch
+ * traces up front. */
+int qpsdm_engine_create(const qpsdm_static_params *p, const int *iaztab,
+                        int naztab, int device, qpsdm_engine **out);
+int qpsdm_engine_destroy(qpsdm_engine *e);
+const char *qpsdm_last_error(const qpsdm_engine *e);
+
+/* ---- line / offset state ---------------------------------------------------*/
+
+/* Replaces get_ttt_all x2 + the dip/nf3/Q uploads of qpsdm()
+ * (src/q-psdm.cu:1449-1515). */
+int qpsdm_set_line(qpsdm_engine *e, const qpsdm_line_params *l);
+
+/* Replaces the per-offset set-up of qpsdm() (src/q-psdm.cu:1593-1691). */
+int qpsdm_begin_offset(qpsdm_engine *e, const qpsdm_offset_params *o);
+
+/* ---- traces --------------------------------------------------------------*/
+
+/* Replaces producer -> queue -> consumer -> psdm_kernel for ntr traces
+ * (src/q-psdm.cu:1862-2061, :2063-2244).  records: ntr SU records of
+ * 240 + 4*ns bytes, host memory, big-endian on disk layout when
+ * big_endian != 0 (as swaptr() decodes, src/segy.cc:6395) else native.
+ * Copies through the engine's pinned staging ring and returns when the
+ * host buffer may be reused; device work continues asynchronously. */
+int qpsdm_submit_traces(qpsdm_engine *e, const void *records, int ntr, int ns,
+                        int big_endian);
+
+/* Same, records already resident in device memory (no copy). */
+int qpsdm_submit_traces_device(qpsdm_engine *e, const void *d_records, int ntr,
+                               int ns, int big_endian);
+
+/* Waits for all submitted work; returns QPSDM_ETIMEOUT / QPSDM_ECUDA on a
+ * device-side error. */
+int qpsdm_fence(qpsdm_engine *e);
+
+/* Replaces the D2H + host sum + /nsb of qpsdm() (src/q-psdm.cu:1745-1765).
+ * host_img: [nxb][nzi] floats (nxb = ixend - ixstart). */
+int qpsdm_get_image(qpsdm_engine *e, float *host_img, int apply_nsb_scale);
+
+/* Device pointer of the block image [nxb][nzi] (FP32) for zero-copy use. */
+int qpsdm_image_device_ptr(qpsdm_engine *e, float **d_img);
+
+/* Runs the engine's kernels on `stream` (a cudaStream_t of the engine's
+ * device) instead of its own stream; NULL restores the engine's stream.
+ * Lets a caller order engine work with its own kernels, time it with its own
+ * events, or capture it into a CUDA graph. */
+int qpsdm_set_stream(qpsdm_engine *e, void *stream);
+
+/* Kernel timing: with profiling on, every launch of the engine is bracketed
+ * by CUDA events on the stream it runs on.  qpsdm_profile_get sums the
+ * elapsed device time (ms) and launches of one kernel class since the last
+ * enable (waits for the stream).  Kernel classes: */
+enum { QPSDM_K_GATE = 0, QPSDM_K_PRE = 1, QPSDM_K_IMAGE = 2, QPSDM_K_OTHER = 3 };
+int qpsdm_profile_enable(qpsdm_engine *e, int on);
+int qpsdm_profile_get(qpsdm_engine *e, int kernel_class, double *total_ms,
+                      int64_t *launches);
+
+/* Counters since begin_offset: traces accepted by the gate and point-traces
+ * evaluated (one per image point inside a trace's aperture). */
+int qpsdm_get_counters(qpsdm_engine *e, int64_t *traces_accepted,
+                       int64_t *point_traces);
+
+/* Per-trace spectra of the last submit (re, im: [ntr][2*nww], rejected
+ * traces untouched), as psdm_kernel leaves them in red/imd
+ * (src/q-psdm.cu:2186-2219).  Device pointers, valid until the next submit. */
+int qpsdm_spectra_device_ptr(qpsdm_engine *e, float **d_re, float **d_im);
+
+/* Per-trace gate results of the last submit: [ntr][8] ints
+ * (status, cdpx, cdpy, iaz, ixi1, ixi2, ntibeg, izimin) and [ntr][4] floats
+ * (sx, sy, gx, gy relative to fxi, cyi).  Device pointers. */
+int qpsdm_gate_device_ptr(qpsdm_engine *e, int **d_ints, float **d_geom);
+
+/* ---- standalone kernels (device pointers) ---------------------------------*/
+
+/* Batched real-to-complex FFT, unnormalised, e^{-iwt} (the convention of
+ * pfarc with isign = -1, src/fft.cc:1838-1910).  n: an npfar length.
+ * d_in [batch][n] floats, d_out [batch][n/2+1] interleaved complex. */
+int qpsdm_fft_r2c(const float *d_in, int n, int batch, float *d_out,
+                  void *stream);
+
+/* Batched complex-to-real inverse, unnormalised, e^{+iwt}
+ * (pfacr with isign = +1, src/fft.cc:1768-1836). */
+int qpsdm_fft_c2r(const float *d_in, int n, int batch, float *d_out,
+                  void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QPSDM_ENGINE_H_ */

@@ -1,0 +1,216 @@
+"""ctypes front-end of the C oracle and of the reference's compiled CPU code.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+and by the ``cpu_baseline`` leg of ``bench.py`` as the checker.  The product
+path (``q_psdm_b200``) never imports this module.
+
+* ``liboracle.so``  -- C restatement of the reference path (qpsdm_oracle.c,
+  physics_oracle.c), built by ``oracle/Makefile``.
+* ``_ref/libqpsdm_refcpu.so`` -- the reference's own fft.cc / psdmpkg.cc /
+  segy.cc compiled in place (present only where the reference sources were
+  available when ``build()`` ran).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+_ref = None
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+def build(ref: bool | None = None) -> None:
+    """Compile liboracle.so (and oracle/_ref when the reference is present)."""
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+    if ref is None:
+        ref = os.path.isdir("/root/reference/src")
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "ref-gpu"], check=True)
+
+
+class GateParams(C.Structure):
+    _fields_ = [
+        ("scaled", C.c_double),
+        ("fxv1", C.c_float), ("fyv1", C.c_float),
+        ("exv1", C.c_float), ("eyv1", C.c_float),
+        ("fxi", C.c_double), ("cyi", C.c_double),
+        ("dxi", C.c_float), ("dyi", C.c_float), ("eps", C.c_float),
+        ("nzi", C.c_int), ("ixstart", C.c_int), ("ixend", C.c_int),
+        ("iaztab", C.POINTER(C.c_int)),
+        ("aznx1", C.POINTER(C.c_int)), ("aznx2", C.POINTER(C.c_int)),
+        ("azny1", C.POINTER(C.c_int)), ("azny2", C.POINTER(C.c_int)),
+    ]
+
+
+class ImageParams(C.Structure):
+    _fields_ = [
+        ("nzi", C.c_int), ("nxb", C.c_int), ("ixstart", C.c_int), ("nt", C.c_int),
+        ("dt1", C.c_float), ("dxi", C.c_float), ("dzi", C.c_float),
+        ("taperzone", C.c_float),
+        ("tcdp1", C.c_int), ("tcdp2", C.c_int),
+    ]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build(ref=False)
+        L = C.CDLL(path)
+        L.orc_npfa.argtypes = [C.c_int]
+        L.orc_npfar.argtypes = [C.c_int]
+        L.orc_pfa_table.argtypes = [_i32p, C.c_int]
+        L.orc_build_iaztab.argtypes = [C.c_float, _i32p, C.c_int]
+        L.orc_derive_static.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float,
+                                        C.c_float, _i32p, _f32p]
+        L.orc_derive_static.restype = None
+        L.orc_window_split.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float,
+                                       _i32p, _f32p]
+        L.orc_window_split.restype = None
+        L.orc_gate_trace.argtypes = [C.POINTER(GateParams), C.c_int, C.c_int,
+                                     C.c_int, C.c_int, _i32p, _f32p]
+        L.orc_gain.argtypes = [_f32p, C.c_int, C.c_float]
+        L.orc_gain.restype = None
+        L.orc_fetch_and_taper.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p]
+        L.orc_fetch_and_taper.restype = None
+        L.orc_rdft.argtypes = [_f32p, C.c_int, _f64p, _f64p]
+        L.orc_rdft.restype = None
+        L.orc_preprocess_trace.argtypes = [_f32p, C.c_int, C.c_float, C.c_int,
+                                           C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.c_float, _f32p, _f32p]
+        L.orc_preprocess_trace.restype = None
+        L.orc_image_compat.argtypes = [C.POINTER(ImageParams), C.c_int, _f32p,
+                                       _i32p, _f32p, _f32p, _f32p, _f32p, _f32p,
+                                       C.POINTER(C.c_longlong)]
+        L.orc_image_compat.restype = None
+        L.orc_scale_image.argtypes = [_f32p, C.c_longlong, C.c_int]
+        L.orc_scale_image.restype = None
+        L.orc_num_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def ref_cpu():
+    """The reference's compiled CPU code, or None when it was not built."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libqpsdm_refcpu.so")
+        if not os.path.exists(path):
+            return None
+        R = C.CDLL(path)
+        R.ref_npfar.argtypes = [C.c_int]
+        R.ref_npfa.argtypes = [C.c_int]
+        R.ref_pfarc.argtypes = [C.c_int, C.c_int, _f32p, _f32p]
+        R.ref_pfarc.restype = None
+        R.ref_fetch_and_taper.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p]
+        R.ref_getscale.argtypes = [C.c_short]
+        R.ref_getscale.restype = C.c_float
+        R.ref_preprocess_traces.argtypes = [_f32p, C.c_int, C.c_int, C.c_float,
+                                            C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_float, _f32p, _f32p,
+                                            C.c_int]
+        R.ref_preprocess_traces.restype = None
+        _ref = R
+    return _ref
+
+
+# --------------------------------------------------------------------------
+# thin numpy helpers
+# --------------------------------------------------------------------------
+def npfar(n: int) -> int:
+    return lib().orc_npfar(int(n))
+
+
+def iaztab(eps: float = 0.001) -> np.ndarray:
+    tab = np.zeros(4096, np.int32)
+    n = lib().orc_build_iaztab(eps, tab, tab.size)
+    return tab[:n].copy()
+
+
+def derive_static(ntl, dt, threshold=600.0, contract=3.0, taperzone=8.0):
+    oi = np.zeros(2, np.int32)
+    of = np.zeros(10, np.float32)
+    lib().orc_derive_static(ntl, dt, threshold, contract, taperzone, oi, of)
+    keys_f = ["df", "dw", "dt1", "lnG", "coef1", "coef2", "coef3", "coef4",
+              "contract", "taperzone"]
+    d = {"nfft": int(oi[0]), "nffti": int(oi[1])}
+    d.update({k: np.float32(v) for k, v in zip(keys_f, of)})
+    return d
+
+
+def window_split(ntl, dt, f1=1.0, f4=140.0):
+    oi = np.zeros(7, np.int32)
+    of = np.zeros(5, np.float32)
+    lib().orc_window_split(ntl, dt, f1, f4, oi, of)
+    keys_i = ["itb1", "itb2", "nsb", "nf1", "nf4", "nww", "ncoef1"]
+    keys_f = ["tdstart1", "tdstart2", "tdmid", "df", "dw"]
+    d = {k: int(v) for k, v in zip(keys_i, oi)}
+    d.update({k: np.float32(v) for k, v in zip(keys_f, of)})
+    return d
+
+
+def fetch_and_taper(data, it1, it2):
+    data = np.ascontiguousarray(data, np.float32)
+    out = np.zeros(it2 - it1 + 1, np.float32)
+    lib().orc_fetch_and_taper(data, data.size, it1, it2, out)
+    return out
+
+
+def rdft(x):
+    x = np.ascontiguousarray(x, np.float32)
+    n = x.size
+    re = np.zeros(n // 2 + 1)
+    im = np.zeros(n // 2 + 1)
+    lib().orc_rdft(x, n, re, im)
+    return re + 1j * im
+
+
+def preprocess_trace(trace, dt, w):
+    """w: window_split() dict.  Returns (re, im) float32 [2*nww]."""
+    trace = np.ascontiguousarray(trace, np.float32)
+    nww = w["nww"]
+    re = np.zeros(2 * nww, np.float32)
+    im = np.zeros(2 * nww, np.float32)
+    lib().orc_preprocess_trace(trace, trace.size, dt, w["itb1"], w["itb2"],
+                               w["nsb"], w["nf1"], nww, w["dw"], re, im)
+    return re, im
+
+
+def gate_traces(gp: GateParams, hdr: np.ndarray):
+    """hdr [ntr,4] int32 (sx, sy, gx, gy).  Returns (ints [ntr,8], geom [ntr,4])."""
+    hdr = np.ascontiguousarray(hdr, np.int32)
+    ntr = hdr.shape[0]
+    ints = np.zeros((ntr, 8), np.int32)
+    geom = np.zeros((ntr, 4), np.float32)
+    oi = np.zeros(8, np.int32)
+    of = np.zeros(4, np.float32)
+    L = lib()
+    for i in range(ntr):
+        L.orc_gate_trace(C.byref(gp), int(hdr[i, 0]), int(hdr[i, 1]),
+                         int(hdr[i, 2]), int(hdr[i, 3]), oi, of)
+        ints[i] = oi
+        geom[i] = of
+    return ints, geom
+
+
+def image_compat(ip: ImageParams, geom, ints3, dips, img=None):
+    """Accumulate accepted traces.  geom [n,4] f32, ints3 [n,3] i32
+    (ixi1, ixi2, izimin), dips (dipx1, dipx2, dipy1, dipy2) each [nxi*nzi]."""
+    geom = np.ascontiguousarray(geom, np.float32)
+    ints3 = np.ascontiguousarray(ints3, np.int32)
+    if img is None:
+        img = np.zeros(ip.nxb * ip.nzi, np.float32)
+    npt = C.c_longlong(0)
+    d = [np.ascontiguousarray(x, np.float32).ravel() for x in dips]
+    lib().orc_image_compat(C.byref(ip), geom.shape[0], geom.ravel(), ints3.ravel(),
+                           d[0], d[1], d[2], d[3], img, C.byref(npt))
+    return img, int(npt.value)

@@ -1,0 +1,111 @@
+"""Reference-compat path on the GPU, through the C ABI, against the C oracle.
+
+Gate results and the accumulated image are bit-exact (integer indices and
+IEEE float arithmetic in the same order); spectra agree with the oracle's
+double-precision DFT to single-precision rounding.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.compat_case import engine_run, make_case, oracle_run
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", params=["small", "block", "singular"])
+def case(request):
+    c = make_case(request.param)
+    ints, geom, img, npt = oracle_run(c)
+    c["o_ints"], c["o_geom"], c["o_img"], c["o_npt"] = ints, geom, img, npt
+    return c
+
+
+def test_gate_bit_exact(cuda, case):
+    eng, img, ints, geom, re, im = engine_run(case)
+    try:
+        assert np.array_equal(ints[:, 0], case["o_ints"][:, 0])
+        ok = ints[:, 0] == 3
+        # status, cdpx, cdpy, iaz for every trace that passed the bbox test
+        pb = ints[:, 0] >= 1
+        assert np.array_equal(ints[pb][:, :4], case["o_ints"][pb][:, :4])
+        assert np.array_equal(ints[ok], case["o_ints"][ok])
+        assert np.array_equal(geom[ok].view(np.uint32), case["o_geom"][ok].view(np.uint32))
+    finally:
+        eng.close()
+
+
+def test_image_bit_exact(cuda, case):
+    eng, img, *_ = engine_run(case)
+    try:
+        assert img.shape == case["o_img"].shape
+        assert np.array_equal(img, case["o_img"], equal_nan=True)
+        if case["name"] == "singular":
+            assert np.isnan(img).sum() == np.isnan(case["o_img"]).sum() >= 1
+        _, npt = eng.counters()
+        assert npt == case["o_npt"]
+    finally:
+        eng.close()
+
+
+def test_spectra_match_oracle(cuda, case):
+    eng, img, ints, geom, re, im = engine_run(case)
+    eng.close()
+    w = case["window"]
+    ok = np.nonzero(ints[:, 0] == 3)[0]
+    for i in ok[:: max(1, len(ok) // 24)]:
+        ore, oim = O.preprocess_trace(case["traces"][i], np.float32(0.002), w)
+        scale = max(np.abs(ore).max(), np.abs(oim).max())
+        assert np.abs(re[i] - ore).max() <= 3e-6 * scale, i
+        assert np.abs(im[i] - oim).max() <= 3e-6 * scale, i
+
+
+def test_batching_preserves_bits(cuda):
+    c = make_case("small")
+    _, _, ref, _ = oracle_run(c)
+    n = c["hdr"].shape[0]
+    eng, img, *_ = engine_run(c, batches=[700, 1, 600, n - 1301], max_batch=1024)
+    eng.close()
+    assert np.array_equal(img, ref)
+    # host path splitting a submit larger than max_batch
+    eng, img2, *_ = engine_run(c, batches=[n], max_batch=500)
+    eng.close()
+    assert np.array_equal(img2, ref)
+
+
+def test_little_endian_records(cuda):
+    c = make_case("block")
+    _, _, ref, _ = oracle_run(c)
+    eng, img, *_ = engine_run(c, big_endian=False)
+    eng.close()
+    assert np.array_equal(img, ref)
+
+
+def test_empty_and_rejected_batches(cuda):
+    c = make_case("small")
+    c["hdr"] = c["hdr"][-16:-9].copy()   # the reject/edge traces only
+    c["traces"] = c["traces"][-16:-9].copy()
+    ints, _, ref, npt = oracle_run(c)
+    eng, img, gi, *_ = engine_run(c)
+    try:
+        assert np.array_equal(gi[:, 0], ints[:, 0])
+        assert np.array_equal(img, ref)
+        eng.submit(np.zeros((0, 240 + 4 * 1000), np.uint8))
+        assert np.array_equal(eng.get_image(False), ref)
+    finally:
+        eng.close()
+
+
+def test_nsb_scale_and_errors(cuda):
+    from q_psdm_b200 import engine as E
+    c = make_case("small")
+    _, _, ref, _ = oracle_run(c)
+    eng, img, *_ = engine_run(c)
+    try:
+        scaled = eng.get_image(True)
+        assert np.array_equal(scaled, (ref / np.float32(c["window"]["nsb"])).astype(np.float32))
+        bad = np.zeros((1, 240 + 4 * 999), np.uint8)
+        with pytest.raises(E.QpsdmError):
+            eng.submit(bad)  # ns != ntl
+    finally:
+        eng.close()
