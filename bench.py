@@ -46,7 +46,7 @@ F_PT_COMPAT = 35
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="compat", choices=["compat"])
@@ -136,7 +136,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -207,7 +207,11 @@ def run_ours(args, rank, world, dist):
     wl = Workload(rank)
     p = wl.static(args.form, max_batch=wl.ntr)
     eng = E.Engine(p, device=dev)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the engine runs on it and the step events are
+    # recorded on it (torch's default stream handle is 0, which the C ABI
+    # reads as "the engine's own stream")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
     eng.set_line(**wl.line_args(p.contract))
     az = wl.aperture()

@@ -214,3 +214,95 @@ def image_compat(ip: ImageParams, geom, ints3, dips, img=None):
     lib().orc_image_compat(C.byref(ip), geom.shape[0], geom.ravel(), ints3.ravel(),
                            d[0], d[1], d[2], d[3], img, C.byref(npt))
     return img, int(npt.value)
+
+
+# --------------------------------------------------------------------------
+# physics mode (FP64)
+# --------------------------------------------------------------------------
+class PhysParams(C.Structure):
+    _fields_ = [
+        ("nzi", C.c_int), ("nxb", C.c_int), ("ixstart", C.c_int), ("nt", C.c_int),
+        ("nbins", C.c_int),
+        ("dt1", C.c_double), ("dxi", C.c_double), ("dzi", C.c_double),
+        ("taperzone", C.c_double), ("dtstar", C.c_double), ("dzii", C.c_double),
+        ("tcdp1", C.c_int), ("tcdp2", C.c_int),
+        ("nxg", C.c_int), ("nzg", C.c_int), ("nxi1", C.c_int), ("nzi1", C.c_int),
+    ]
+
+
+def physics_filter(nfft, dt, f3, f4, fc, threshold, nbins, dtstar):
+    """[nbins, nfft/2+1] complex128: (-i ww_k) A(pi f t*_b) e^{-2i f t*_b ln(f/fc)} / nfft.
+
+    ww is the -i*w band ramp of qpsdm() (src/q-psdm.cu:1207-1250: w below
+    n3, w(n3) cos^2 taper from n3 to n4, zero from n4); A is the gain-limited
+    exponential whose constants qpsdm() derives from the threshold G
+    (src/q-psdm.cu:1277-1283): e^x up to ln G, the quadratic
+    G(1 + u - 2.5 u^2), u = x - ln G, up to ln G + 0.2, then 1.1 G."""
+    nk = nfft // 2 + 1
+    df = 1.0 / (nfft * float(dt))
+    dw = 2 * np.pi * df
+    n3 = int(float(np.float32(f3)) / df + 0.5)
+    n4 = int(float(np.float32(f4)) / df + 0.5)
+    k = np.arange(nk)
+    ww = np.where(k < n3, k * dw,
+                  np.where(k < n4, n3 * dw * np.cos((k - n3) / max(n4 - n3, 1) * np.pi / 2) ** 2,
+                           0.0))
+    G = float(threshold)
+    lnG = np.log(G)
+    f = k * df
+    out = np.zeros((nbins, nk), np.complex128)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        lnf = np.where(f > 0, np.log(np.where(f > 0, f, 1.0) / fc), 0.0)
+    for b in range(nbins):
+        ts = b * float(dtstar)
+        x = np.pi * f * ts
+        u = x - lnG
+        a = np.where(x <= lnG, np.exp(np.minimum(x, lnG)),
+                     np.where(x <= lnG + 0.2, G * (1 + u - 2.5 * u * u), 1.1 * G))
+        out[b] = (-1j * ww) * a * np.exp(-2j * f * ts * lnf) / nfft
+    out[:, 0] = 0.0
+    return out
+
+
+def physics_panels(traces, dt, nfft, nffti, filt):
+    """[ntr, nbins, nffti] float64 compensated panels of float32 traces."""
+    traces = np.ascontiguousarray(traces, np.float32)
+    ntr, ntl = traces.shape
+    x = np.empty_like(traces)
+    L = lib()
+    g = np.empty(ntl, np.float32)
+    for i in range(ntr):
+        g[:] = traces[i]
+        L.orc_gain(g, ntl, dt)
+        L.orc_fetch_and_taper(g, ntl, 0, ntl - 1, x[i])
+    X = np.fft.rfft(x.astype(np.float64), n=nfft, axis=1)
+    out = np.empty((ntr, filt.shape[0], nffti))
+    for b in range(filt.shape[0]):
+        out[:, b, :] = np.fft.irfft(X * filt[b][None, :], n=nffti, axis=1) * nffti
+    return out
+
+
+def physics_image(pp: PhysParams, geom, ints3, panels, dips, tables, img=None):
+    """FP64 image [nxb*nzi] of accepted traces; tables: dict with ttt_desc,
+    qqq_desc (uint8 [n,16] or structured), ttt, qqq (float32)."""
+    L = lib()
+    if not hasattr(L, "_phys_bound"):
+        L.orc_physics_image.argtypes = [C.POINTER(PhysParams), C.c_int, _f32p, _i32p, _f64p,
+                                        _f32p, _f32p, _f32p, _f32p, C.c_void_p, _f32p,
+                                        C.c_void_p, _f32p, _f64p, C.POINTER(C.c_longlong)]
+        L.orc_physics_image.restype = None
+        L._phys_bound = True
+    if img is None:
+        img = np.zeros(pp.nxb * pp.nzi)
+    dtab = np.ascontiguousarray(tables["ttt_desc"]).view(np.uint8)
+    qtab = np.ascontiguousarray(tables["qqq_desc"]).view(np.uint8)
+    npt = C.c_longlong(0)
+    d = [np.ascontiguousarray(x, np.float32).ravel() for x in dips]
+    L.orc_physics_image(C.byref(pp), int(np.asarray(geom).shape[0]),
+                        np.ascontiguousarray(geom, np.float32).ravel(),
+                        np.ascontiguousarray(ints3, np.int32).ravel(),
+                        np.ascontiguousarray(panels, np.float64).ravel(),
+                        d[0], d[1], d[2], d[3], dtab.ctypes.data,
+                        np.ascontiguousarray(tables["ttt"], np.float32), qtab.ctypes.data,
+                        np.ascontiguousarray(tables["qqq"], np.float32), img, C.byref(npt))
+    return img, int(npt.value)

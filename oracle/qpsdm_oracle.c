@@ -360,7 +360,12 @@ static inline float compat_point(const orc_image_params *p, const float *g,
   float tany1c = tany1 - tz * (1.0f + tany1 * tany1);
   float tany2c = tany2 + tz * (1.0f + tany2 * tany2);
   *masked = 1;
-  if (tanx <= tanx1c || tanx2c <= tanx || tany <= tany1c || tany2c <= tany)
+  /* Same test as the reference's `tanx <= tanx1c || ...` reject for every
+   * number; a NaN tangent (0/0 at z = 0 when source, receiver and node are
+   * collinear) is rejected as well, which is what the reference binary does
+   * (its --use_fast_math divisions leave a tiny nonzero numerator there, so
+   * the tangent is +-inf and fails the test). */
+  if (!(tanx > tanx1c && tanx < tanx2c && tany > tany1c && tany < tany2c))
     return 0.0f;
   float w = 1.0f;
   if (tanx < tanx1) w *= (tanx - tanx1c) / (tanx1 - tanx1c);

@@ -253,7 +253,11 @@ __global__ void __launch_bounds__(kCompatBz *kCompatBx)
       const float uy = __fadd_rn(__fdiv_rn(gm.y, ds), __fdiv_rn(gm.w, dg));
       const float uz = __fadd_rn(__fdiv_rn(z, ds), __fdiv_rn(z, dg));
       const float tanx = __fdiv_rn(ux, uz), tany = __fdiv_rn(uy, uz);
-      if (tanx <= tanx1c || tanx2c <= tanx || tany <= tany1c || tany2c <= tany) continue;
+      // The reference rejects `tanx <= tanx1c || tanx2c <= tanx || ...`; the
+      // negated form agrees for every number and also rejects a NaN tangent
+      // (0/0 at z = 0 for collinear source, receiver and node), as the
+      // reference binary does: its approximate divisions give +-inf there.
+      if (!(tanx > tanx1c && tanx < tanx2c && tany > tany1c && tany < tany2c)) continue;
       float w = 1.0f;
       if (tanx < tanx1) w = __fmul_rn(w, __fdiv_rn(__fsub_rn(tanx, tanx1c), __fsub_rn(tanx1, tanx1c)));
       if (tanx > tanx2) w = __fmul_rn(w, __fdiv_rn(__fsub_rn(tanx2c, tanx), __fsub_rn(tanx2c, tanx2)));

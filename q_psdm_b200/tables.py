@@ -1,0 +1,180 @@
+"""Traveltime (ttt) and t* (qqq) tables in the reference's layout.
+
+Format (src/q-psdm.cu:103-109, :2382-2627, example examples/traveltime/Lxxx.tidx):
+
+* index file ``Lxxx.tidx`` / ``Lxxx.qidx``: header ``cdp1, cdp2 (int32),
+  dx, dz (float32), nzg, nxg, nzi1, nxi1 (int32)``, then ``nxg*nzg``
+  16-byte descriptors ``{int64 idx; uint16 nys, nxs, dys, dxs}``,
+  descriptor of cell (ixg, izg) at ``ixg*nzg + izg`` (depth fastest, as the
+  shipped index shows: apertures grow along each run of nzg records).
+* data file ``L<line>.ttt`` / ``.qqq``: native float32; the block of a cell
+  starts at ``idx`` and holds ``nys*nxs*nxi1*nzi1`` values.
+
+The reference never states the order inside a block nor where a cell's
+surface grid sits (its kernel stub never reads the tables).  This engine
+fixes both, and the writer below follows them:
+
+* block order ``[iys][ixs][ixl][izl]`` (depth fastest: "in each grid the z is
+  contiguous", src/q-psdm.cu:1112-1114);
+* the local surface grid is centred on the cell: node (iys, ixs) lies at
+  ``x = xc + (ixs - (nxs-1)/2) * dxs``, ``y = (iys - (nys-1)/2) * dys``
+  relative to the image line, with ``xc`` the x of the cell's middle cdp;
+* image depth z maps to table node ``z / dzii`` (dzii the table depth
+  spacing), cell ``izg = node / nzi1`` (src/q-psdm.cu:2344-2349), linear
+  between nodes; surface positions are bilinear between grid nodes; a
+  surface position outside a cell's grid has no table value (masked).
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+DESC_DTYPE = np.dtype([("idx", "<i8"), ("nys", "<u2"), ("nxs", "<u2"),
+                       ("dys", "<u2"), ("dxs", "<u2")])
+
+
+@dataclass
+class LineTables:
+    cdp1: int          # absolute first cdp of the tables
+    cdp2: int
+    dx: float          # cdp spacing (m)
+    dz: float          # stored in the header (velocity dz of the reference)
+    nxg: int
+    nzg: int
+    nxi1: int          # cdps per cell
+    nzi1: int          # depth nodes per cell
+    dzii: float        # depth-node spacing (m)
+    desc: np.ndarray   # DESC_DTYPE [nxg*nzg]
+    ttt: np.ndarray    # float32
+    qqq: np.ndarray    # float32 (t*, s), same layout and descriptors
+
+    def as_engine_dict(self):
+        d = self.desc.view(np.uint8).reshape(-1, 16).copy()
+        return dict(nxg=self.nxg, nzg=self.nzg, nxi1=self.nxi1, nzi1=self.nzi1,
+                    cdp1=self.cdp1, cdp2=self.cdp2, ttt_desc=d, qqq_desc=d,
+                    ttt=self.ttt, qqq=self.qqq)
+
+
+def cell_surface_nodes(tab: LineTables, ixg: int, izg: int, fci: int):
+    """(x, y) of every node of a cell's surface grid, relative to (fxi, line)."""
+    d = tab.desc[ixg * tab.nzg + izg]
+    xc = ((tab.cdp1 - fci) + ixg * tab.nxi1 + 0.5 * (tab.nxi1 - 1)) * tab.dx
+    xs = xc + (np.arange(d["nxs"]) - 0.5 * (d["nxs"] - 1)) * d["dxs"]
+    ys = (np.arange(d["nys"]) - 0.5 * (d["nys"] - 1)) * d["dys"]
+    return xs, ys
+
+
+def build_line_tables(time_fn, tstar_fn, *, fci: int, nxi: int, dxi: float, zmax: float,
+                      dzii: float, nxi1: int, nzi1: int, surf_dx: int, surf_dy: int,
+                      half_x: float, half_y: float, cdp1: int | None = None,
+                      cdp2: int | None = None, dz_header: float = 8.0,
+                      nz_cells: int | None = None) -> LineTables:
+    """Tables of one image line.
+
+    time_fn(px, py, x, z) / tstar_fn(...) give traveltime and t* from surface
+    point (px, py) to image point (x, line, z); coordinates relative to the
+    first image cdp and the line; broadcastable numpy arrays.  Each cell's
+    surface grid spans +-half_x, +-half_y around the cell at surf_dx/surf_dy
+    spacing (odd node counts)."""
+    cdp1 = fci if cdp1 is None else cdp1
+    cdp2 = fci + nxi - 1 if cdp2 is None else cdp2
+    ncdp = cdp2 - cdp1 + 1
+    nxg = -(-ncdp // nxi1)
+    nnodes = int(np.floor(zmax / dzii)) + 2          # node below zmax for the lerp
+    nzg = nz_cells or -(-nnodes // nzi1)
+    nxs = 2 * int(np.ceil(half_x / surf_dx)) + 1
+    nys = 2 * int(np.ceil(half_y / surf_dy)) + 1
+    desc = np.zeros(nxg * nzg, DESC_DTYPE)
+    block = nys * nxs * nxi1 * nzi1
+    ttt = np.zeros(nxg * nzg * block, np.float32)
+    qqq = np.zeros_like(ttt)
+    tab = LineTables(cdp1, cdp2, dxi, dz_header, nxg, nzg, nxi1, nzi1, dzii, desc, ttt, qqq)
+    off = 0
+    for ixg in range(nxg):
+        for izg in range(nzg):
+            k = ixg * nzg + izg
+            desc[k] = (off, nys, nxs, surf_dy, surf_dx)
+            xs, ys = cell_surface_nodes(tab, ixg, izg, fci)
+            x = ((cdp1 - fci) + ixg * nxi1 + np.arange(nxi1)) * dxi
+            z = (izg * nzi1 + np.arange(nzi1)) * dzii
+            PY, PX, X, Z = np.meshgrid(ys, xs, x, z, indexing="ij")
+            ttt[off:off + block] = time_fn(PX, PY, X, Z).astype(np.float32).ravel()
+            qqq[off:off + block] = tstar_fn(PX, PY, X, Z).astype(np.float32).ravel()
+            off += block
+    return tab
+
+
+def linear_gradient_tables(sv, *, fci: int, nxi: int, dxi: float, zmax: float,
+                           sub: int = 4, nxi1: int = 16, half_x: float = 900.0,
+                           half_y: float = 900.0) -> LineTables:
+    """Analytic v(z) = v0 + k z tables (constant Q: t* = t / Q), subsampled
+    `sub` times in depth and surface position relative to the 10 m grid."""
+    from .synth import traveltime
+
+    def tfn(px, py, x, z):
+        return traveltime(sv, np.hypot(px - x, py), z)
+
+    def qfn(px, py, x, z):
+        return traveltime(sv, np.hypot(px - x, py), z) / sv.q
+
+    dzii = sub * sv.dzi
+    nnodes = int(np.floor(zmax / dzii)) + 2
+    return build_line_tables(tfn, qfn, fci=fci, nxi=nxi, dxi=dxi, zmax=zmax, dzii=dzii,
+                             nxi1=nxi1, nzi1=nnodes, surf_dx=int(sub * sv.dxi),
+                             surf_dy=int(sub * sv.dyi), half_x=half_x, half_y=half_y)
+
+
+# ---------------------------------------------------------------------------
+# file I/O in the reference's format
+# ---------------------------------------------------------------------------
+def write_index(path: str, tab: LineTables) -> None:
+    hdr = np.array([tab.cdp1, tab.cdp2], "<i4").tobytes()
+    hdr += np.array([tab.dx, tab.dz], "<f4").tobytes()
+    hdr += np.array([tab.nzg, tab.nxg, tab.nzi1, tab.nxi1], "<i4").tobytes()
+    with open(path, "wb") as f:
+        f.write(hdr)
+        f.write(tab.desc.tobytes())
+
+
+def read_index(path: str):
+    b = open(path, "rb").read()
+    cdp1, cdp2 = np.frombuffer(b[:8], "<i4")
+    dx, dz = np.frombuffer(b[8:16], "<f4")
+    nzg, nxg, nzi1, nxi1 = np.frombuffer(b[16:32], "<i4")
+    n = int(nxg) * int(nzg)
+    if len(b) < 32 + 16 * n:
+        raise ValueError(f"{path}: index size error ({len(b)} bytes for {n} cells)")
+    desc = np.frombuffer(b[32:32 + 16 * n], DESC_DTYPE).copy()
+    return dict(cdp1=int(cdp1), cdp2=int(cdp2), dx=float(dx), dz=float(dz), nzg=int(nzg),
+                nxg=int(nxg), nzi1=int(nzi1), nxi1=int(nxi1), desc=desc)
+
+
+def write_line(ttpath: str, line: int, tab: LineTables) -> None:
+    os.makedirs(ttpath, exist_ok=True)
+    write_index(os.path.join(ttpath, "Lxxx.tidx"), tab)
+    write_index(os.path.join(ttpath, "Lxxx.qidx"), tab)
+    tab.ttt.astype("=f4").tofile(os.path.join(ttpath, f"L{line}.ttt"))
+    tab.qqq.astype("=f4").tofile(os.path.join(ttpath, f"L{line}.qqq"))
+
+
+def load_line(ttpath: str, line: int, line1: int, line2: int, torq: str = "t") -> np.ndarray:
+    """Data of `line`, linearly interpolated between the nearest existing line
+    files below and above it within [line1, line2] (src/q-psdm.cu:2488-2600)."""
+    suff = "ttt" if torq == "t" else "qqq"
+    lo = next((l for l in range(line, line1 - 1, -1)
+               if os.path.exists(os.path.join(ttpath, f"L{l}.{suff}"))), -1)
+    hi = next((l for l in range(line, line2 + 1)
+               if os.path.exists(os.path.join(ttpath, f"L{l}.{suff}"))), -1)
+    if lo == -1 or hi == -1:
+        raise FileNotFoundError(f"no {suff} table brackets line {line} in {ttpath}")
+    a = np.fromfile(os.path.join(ttpath, f"L{lo}.{suff}"), "=f4")
+    if lo == hi:
+        return a
+    b = np.fromfile(os.path.join(ttpath, f"L{hi}.{suff}"), "=f4")
+    if b.size != a.size:
+        raise ValueError("table sizes of the bracketing lines differ")
+    c2 = np.float32(1.0 * (line - lo) / (hi - lo))
+    c1 = np.float32(1.0 - c2)
+    return (a * c1 + b * c2).astype(np.float32)

@@ -52,8 +52,9 @@ def _extra_traces(sv, rng):
 
 def make_case(name: str = "small", seed: int = 7):
     """name: "small" (full line), "block" (an x block, wider aperture) or
-    "singular" (a zero-offset trace exactly above image nodes: the reference's
-    ray-direction formula divides 0 by 0 at z = 0 and its image holds NaN)."""
+    "singular" (a zero-offset trace exactly above image nodes: the
+    ray-direction formula divides 0 by 0 at z = 0; the NaN tangent is
+    rejected like any tangent outside the dip limits)."""
     sv = synth.config1(seed)
     rng = np.random.default_rng(seed)
     line = 64
@@ -179,7 +180,8 @@ def engine_run(case, device=0, batches=None, big_endian=True, max_batch=4096):
         c0 += b
     assert c0 == ntr
     img = eng.get_image(apply_nsb_scale=False)
-    last = batches[-1]
+    # device-side per-trace outputs hold the last launched batch only
+    last = batches[-1] if batches[-1] <= max_batch else batches[-1] % max_batch or max_batch
     di, dg = eng.gate_device_ptrs()
     dre, dim = eng.spectra_device_ptrs()
     nww = o.nww

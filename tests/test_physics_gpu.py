@@ -1,0 +1,78 @@
+"""Physics mode on the GPU through the C ABI against the FP64 oracle.
+
+Tolerances (image NRMSE against FP64): FP32 panels 1e-5, BF16 and FP16
+panels 1e-3 (the gate the method is held to).  Point-trace counts are exact.
+"""
+import numpy as np
+import pytest
+
+from tests.physics_case import engine, make_case, nrmse, oracle_run, records
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    c = make_case(nshots=2)
+    c["o_img"], c["o_npt"], c["o_ints"] = oracle_run(c)
+    assert np.abs(c["o_img"]).max() > 0
+    return c
+
+
+@pytest.mark.parametrize("dtype,tol", [(0, 1e-5), (1, 1e-3), (2, 1e-3)])
+def test_image_nrmse(cuda, case, dtype, tol):
+    eng, p, o = engine(case, panel_dtype=dtype)
+    try:
+        eng.submit(records(case))
+        img = eng.get_image(False)
+        _, npt = eng.counters()
+    finally:
+        eng.close()
+    assert np.isfinite(img).all()
+    assert npt == case["o_npt"]
+    e = nrmse(img, case["o_img"])
+    print(f"dtype {dtype}: NRMSE {e:.3e}")
+    assert e <= tol
+
+
+def test_kahan_and_batches(cuda, case):
+    rec = records(case)
+    eng, p, o = engine(case, kahan=1, max_batch=700)
+    try:
+        eng.submit(rec[:300])
+        eng.submit(rec[300:])
+        img = eng.get_image(False)
+    finally:
+        eng.close()
+    assert nrmse(img, case["o_img"]) <= 1e-5
+
+
+def test_block_and_little_endian(cuda):
+    c = make_case(nshots=1, shots=[10], ixstart=30, ixend=100, half_x=60, half_y=40)
+    ref, npt, _ = oracle_run(c)
+    eng, p, o = engine(c)
+    try:
+        eng.submit(records(c, big_endian=False), big_endian=False)
+        img = eng.get_image(False)
+        _, n = eng.counters()
+    finally:
+        eng.close()
+    assert n == npt
+    assert nrmse(img, ref) <= 1e-5
+
+
+def test_missing_tables_rejected(cuda, case):
+    from q_psdm_b200 import engine as E
+    eng, p, o = engine(case)
+    try:
+        sv = case["sv"]
+        with pytest.raises(E.QpsdmError):
+            eng.set_line(fxi=case["fxi"], cyi=case["cyi"],
+                         dips=case["dips"].reshape(4, sv.nxi, sv.nzi))
+        bad = case["tab"].as_engine_dict()
+        bad["ttt"] = bad["ttt"][:100]
+        with pytest.raises(E.QpsdmError):
+            eng.set_line(fxi=case["fxi"], cyi=case["cyi"],
+                         dips=case["dips"].reshape(4, sv.nxi, sv.nzi), tables=bad)
+    finally:
+        eng.close()
