@@ -1,6 +1,7 @@
 """Physics mode on the GPU through the C ABI against the FP64 oracle.
 
-Tolerances (image NRMSE against FP64): FP32 panels 1e-5, BF16 and FP16
+Tolerances (image NRMSE against FP64): FP32 panels 5e-5 (FP32 rounding of
+t = ts + tg, ~1e-7 s, against the highest panel frequencies), BF16 and FP16
 panels 1e-3 (the gate the method is held to).  Point-trace counts are exact.
 """
 import numpy as np
@@ -19,7 +20,7 @@ def case():
     return c
 
 
-@pytest.mark.parametrize("dtype,tol", [(0, 1e-5), (1, 1e-3), (2, 1e-3)])
+@pytest.mark.parametrize("dtype,tol", [(0, 5e-5), (1, 1e-3), (2, 1e-3)])
 def test_image_nrmse(cuda, case, dtype, tol):
     eng, p, o = engine(case, panel_dtype=dtype)
     try:
@@ -44,7 +45,7 @@ def test_kahan_and_batches(cuda, case):
         img = eng.get_image(False)
     finally:
         eng.close()
-    assert nrmse(img, case["o_img"]) <= 1e-5
+    assert nrmse(img, case["o_img"]) <= 5e-5
 
 
 def test_block_and_little_endian(cuda):
@@ -58,7 +59,7 @@ def test_block_and_little_endian(cuda):
     finally:
         eng.close()
     assert n == npt
-    assert nrmse(img, ref) <= 1e-5
+    assert nrmse(img, ref) <= 5e-5
 
 
 def test_missing_tables_rejected(cuda, case):
