@@ -41,7 +41,8 @@ enum {
   QPSDM_ESTATE = 4,   /* call out of order (e.g. submit before begin_offset) */
   QPSDM_ETIMEOUT = 5, /* a bounded device wait gave up */
   QPSDM_ENOTSUP = 6,
-  QPSDM_ENOKERNEL = 7 /* no sm_100a image for this device */
+  QPSDM_ENOKERNEL = 7, /* no sm_100a image for this device */
+  QPSDM_ESIZE = 8      /* request larger than a fixed built-in capacity */
 };
 
 enum { QPSDM_MODE_COMPAT = 0, QPSDM_MODE_PHYSICS = 1 };
@@ -229,6 +230,21 @@ int qpsdm_fft_r2c(const float *d_in, int n, int batch, float *d_out,
  * (pfacr with isign = +1, src/fft.cc:1768-1836). */
 int qpsdm_fft_c2r(const float *d_in, int n, int batch, float *d_out,
                   void *stream);
+
+/* Same transform and result as qpsdm_fft_r2c, for callers that may not
+ * allocate device memory (a host framework whose own pool owns all of HBM,
+ * or a latency-critical caller that cannot take the device synchronisation
+ * an allocation may cause).  No counterpart in the reference.
+ * Allocates nothing: its twiddle tables live in a fixed device array built
+ * into the library (QPSDM_FFT_NOALLOC_MAX_N + 1 complex floats, 64 KiB per
+ * GPU that loads the library, held until exit).  n above
+ * QPSDM_FFT_NOALLOC_MAX_N returns QPSDM_ESIZE.  Every call shares that array:
+ * calls that overlap on the GPU race and must be serialised.  The first call
+ * on a device looks up the array's device address; make it before any
+ * stream capture. */
+#define QPSDM_FFT_NOALLOC_MAX_N 8192
+int qpsdm_fft_r2c_noalloc(const float *d_in, int n, int batch, float *d_out,
+                          void *stream);
 
 #ifdef __cplusplus
 }

@@ -97,7 +97,10 @@ SYMBOLS = [
     ("qpsdm_gate_device_ptr", _I, [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     ("qpsdm_fft_r2c", _I, [_P, _I, _I, _P, _P]),
     ("qpsdm_fft_c2r", _I, [_P, _I, _I, _P, _P]),
+    ("qpsdm_fft_r2c_noalloc", _I, [_P, _I, _I, _P, _P]),
 ]
+FFT_NOALLOC_MAX_N = 8192
+ESIZE = 8
 
 _lib = None
 

@@ -153,3 +153,84 @@ extern "C" int qpsdm_fft_c2r(const float *d_in, int n, int batch, float *d_out,
   k_irfft_batch<<<batch, 256, sm, (cudaStream_t)stream>>>((const float2 *)d_in, d_out, p);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free batched real FFT.
+//
+// Some callers of this library must not allocate device memory: a host
+// framework that owns every byte of HBM through its own pool and forbids
+// cudaMalloc behind its back, or a latency-critical caller that cannot take
+// the implicit device synchronisation a cudaMalloc may cause.  qpsdm_fft_r2c
+// allocates its twiddle tables on the first use of each length; this variant
+// keeps them in one fixed file-scope device array instead, which every GPU
+// that loads the library holds until the process exits.
+//
+// The array is shared by every call on a device and keeps the last call's
+// twiddles; each call rewrites the part it uses before its kernel runs, so
+// nothing needs clearing.  Calls that overlap on the GPU (concurrent streams)
+// race on the array and must be serialised by the caller.  The first call on
+// a device looks up the array's device address (cudaGetSymbolAddress); make
+// that first call before any stream capture.
+// ---------------------------------------------------------------------------
+namespace qpsdm {
+
+constexpr int kNoAllocMaxDevices = 64;
+// m twiddles + (m + 1) split twiddles, m = n / 2 <= QPSDM_FFT_NOALLOC_MAX_N / 2
+static __device__ __align__(256) float2 g_noalloc_twiddles[QPSDM_FFT_NOALLOC_MAX_N + 1];
+static std::mutex g_noalloc_mu;
+static float2 *g_noalloc_dev_ptr[kNoAllocMaxDevices];
+
+// Device address of g_noalloc_twiddles on the current device; set up once per
+// device with that device current.  In host code the array's name is only a
+// host-side stand-in, never a usable device address.
+static int noalloc_twiddle_ptr(float2 **out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
+    return QPSDM_ECUDA;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_dev_ptr[dev]) {
+    void *ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_twiddles) != cudaSuccess || !ptr)
+      return QPSDM_ECUDA;
+    g_noalloc_dev_ptr[dev] = (float2 *)ptr;
+  }
+  *out = g_noalloc_dev_ptr[dev];
+  return QPSDM_OK;
+}
+
+}  // namespace qpsdm
+
+extern "C" int qpsdm_fft_r2c_noalloc(const float *d_in, int n, int batch,
+                                     float *d_out, void *stream) {
+  if (!d_in || !d_out || batch < 0) return QPSDM_EINVAL;
+  if (n > QPSDM_FFT_NOALLOC_MAX_N) return QPSDM_ESIZE;
+  if (n < 2 || (n & 1)) return QPSDM_EINVAL;
+  if (batch == 0) return QPSDM_OK;
+  FftPlan p{};
+  p.n = n;
+  p.m = n / 2;
+  if (!factor_radices(p.m, p)) return QPSDM_EINVAL;
+  float2 *tw = nullptr;
+  int rc = noalloc_twiddle_ptr(&tw);
+  if (rc) return rc;
+  // the same double-precision twiddles, rounded once, that qpsdm_fft_r2c uses
+  static thread_local float2 h[QPSDM_FFT_NOALLOC_MAX_N + 1];
+  for (int e = 0; e < p.m; ++e) {
+    double a = -2.0 * M_PI * (double)e / (double)p.m;
+    h[e] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  for (int k = 0; k <= p.m; ++k) {
+    double a = -2.0 * M_PI * (double)k / (double)n;
+    h[p.m + k] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  // pageable source: returns once h has been staged, so h may be reused
+  if (cudaMemcpyAsync(tw, h, sizeof(float2) * (2 * (size_t)p.m + 1), cudaMemcpyHostToDevice,
+                      (cudaStream_t)stream) != cudaSuccess)
+    return QPSDM_ECUDA;
+  p.tw_m = tw;
+  p.tw_n = tw + p.m;
+  const size_t sm = fft_smem_bytes(p.m);
+  if ((rc = fft_set_smem_attr((const void *)k_rfft_batch, sm))) return rc;
+  k_rfft_batch<<<batch, 256, sm, (cudaStream_t)stream>>>(d_in, (float2 *)d_out, p);
+  return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
+}
