@@ -1,27 +1,40 @@
 """Benchmark of the imaging path: Gpoint-traces/s on one or more B200s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--form compat|plain|batched]
+                    [--form batched|plain|compat]
 
-A step images one shot gather (config 2 geometry: 96x96 receivers, nt=2000,
-dt=2 ms) into one 512-cdp x 400-depth image line.  A point-trace is one
-(image point, trace) pair inside the trace's aperture; the engine counts
-them on the device.  `value` is measured with the records already resident
-in HBM (qpsdm_submit_traces_device); `e2e` goes through the host API
-(qpsdm_submit_traces from host records, get_image every step).  L2 is
-flushed (a 256 MiB write) before every timed step; only the step is timed.
+Workload: configuration 2's geometry (200 shots x 96 x 96 receivers, nt=2000,
+dt=2 ms, image 512 x 512 x 400 at 10 m), seeded synthetic traces, analytic
+v(z) = 1800 + 0.5 z traveltime / t* tables subsampled 8x (constant Q = 80).
+A point-trace is one (image point, trace) pair inside the trace's aperture;
+the engine counts them on the device.
+
+Forms (a step = one pass over one batch):
+  batched  4 shot gathers (36864 traces) into a brick of 8 image lines; BF16
+           t* panels computed once per trace and shared by the brick;
+           receiver-grouped persistent kernel.  The headline.
+  plain    1 shot gather into 1 image line, FP32 panels, launch per shot and
+           per line, as the reference organises its work.
+  compat   the reference's own (stub) kernel semantics, 1 shot into 1 line.
+With --form batched the plain form is also timed in the same run and
+reported under "forms" (the north star's plain-vs-batched ratio).
+
+`value`: records resident in HBM, CUDA events on the engine's stream around
+each step, L2 flushed (256 MiB write) before each step.  `e2e`: the host API
+with records in pinned host memory (qpsdm_submit_traces) and the image read
+back (qpsdm_get_image) every step, wall clock.
 
 Multi-GPU (torchrun): every rank images its own shots into its own image
-(weak scaling, no data-path collective); timings are reduced with max.
+brick (weak scaling, no data-path collective); timings are reduced with max.
 
---impl reference times the reference's own CPU path on the host cores: the
-reference's preprocessing (fetch_and_taper + pfarc compiled from its sources
-into oracle/_ref, when present) plus the CPU restatement of image_depth_gpu
-(oracle/), on a bounded sample of each step's traces.
+--impl reference times the reference's own CPU path for the imaging step on
+the host cores: its preprocessing compiled from its sources (oracle/_ref) plus
+the CPU restatement of its imaging kernel (oracle/), bounded samples.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -36,20 +49,24 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Gpoint-traces/s, plain vs batched+BF16+surrogate form, at NRMSE<=1e-3 vs FP64"
-PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
-# Floating-point operations of one point-trace of the stub kernel
-# (src/q-psdm.cu:2303-2378): 2 sub, 2x(3 mul/add + sqrt), 3x(2 div + add),
-# 2 div, 7 mul/div (ds/dg ratio), 3 double (div, add, mul), 2 (v*tr, +=).
-F_PT_COMPAT = 35
+# FP32 operations per point-trace.  Physics: 42 table
+# interpolation, 14 ray geometry and weights, 6 time/t* pick, 2 accumulate.
+# Compat: the stub body of image_depth_gpu (src/q-psdm.cu:2303-2378).
+F_PT = {"batched": 64, "plain": 64, "compat": 35}
+FORMS = {  # shots per step, lines per step, panel dtype, physics form
+    "batched": (4, 8, 1, 1),
+    "plain": (1, 1, 0, 0),
+    "compat": (1, 1, 0, None),
+}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="compat", choices=["compat"])
+    ap.add_argument("--form", default="batched", choices=list(FORMS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -59,64 +76,86 @@ def parse():
 # workload
 # ---------------------------------------------------------------------------
 class Workload:
-    """Config 2 geometry, one image line, shot gathers as steps."""
+    """Configuration 2 geometry; steps are shot gathers near the image lines."""
 
-    LINE = 256
-    HALF_CDPS, HALF_LINES = 200, 100   # aperture: +-2 km in x, +-1 km in y
+    LINE0 = 252                      # first image line of the brick
+    HALF_CDPS, HALF_LINES = 200, 100  # aperture: +-2 km in x, +-1 km in y
 
     def __init__(self, rank: int = 0):
         from q_psdm_b200 import synth
         self.synth = synth
         self.sv = synth.config2(seed=11)
         self.rank = rank
-        sv = self.sv
-        # shots whose midpoints reach the line (|sy - line| small), per rank
-        ly = sv.line_y(self.LINE)
-        order = np.argsort(np.abs(sv.shots[:, 1] - ly), kind="stable")
-        self.shot_ids = order
-        self.ntr = len(sv.receivers)
-        self.nt = sv.ntl
-        self.dt = np.float32(sv.dt)
+        ly = self.sv.line_y(self.LINE0 + 4)
+        self.shot_ids = np.argsort(np.abs(self.sv.shots[:, 1] - ly), kind="stable")
+        self.ntr_shot = len(self.sv.receivers)
         self._rec = {}
+        self._tab = None
 
-    def records(self, k: int, big_endian=True):
-        """SU records of the k-th shot of this rank (cached)."""
+    def shot(self, k: int) -> int:
+        return int(self.shot_ids[(self.rank * 7 + k) % len(self.shot_ids)])
+
+    def records(self, k: int, nshots: int) -> np.ndarray:
+        """SU records (big-endian) of shots k*nshots .. k*nshots+nshots-1."""
         from q_psdm_b200 import engine as E
-        sid = int(self.shot_ids[(self.rank * 7 + k) % len(self.shot_ids)])
-        key = (sid, big_endian)
-        if key not in self._rec:
-            sx, sy, gx, gy = self.synth.trace_geometry(self.sv, [sid])
-            tr = self.synth.make_traces(self.sv, [sid])
-            self._rec[key] = E.encode_su(sx, sy, gx, gy, tr, dt_us=2000,
-                                         scalco=self.sv.scalco, big_endian=big_endian)
-        return self._rec[key]
+        out = []
+        for j in range(k * nshots, k * nshots + nshots):
+            sid = self.shot(j)
+            if sid not in self._rec:
+                sx, sy, gx, gy = self.synth.trace_geometry(self.sv, [sid])
+                tr = self.synth.make_traces(self.sv, [sid])
+                self._rec[sid] = E.encode_su(sx, sy, gx, gy, tr, dt_us=2000,
+                                             scalco=self.sv.scalco)
+            out.append(self._rec[sid])
+        return np.concatenate(out)
+
+    def tables(self):
+        if self._tab is None:
+            from q_psdm_b200 import tables as T
+            sv = self.sv
+            self._tab = T.linear_gradient_tables(
+                sv, fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi, zmax=(sv.nzi - 1) * sv.dzi, sub=8,
+                nxi1=16, half_x=2500.0, half_y=1200.0)
+        return self._tab
 
     def static(self, form: str, max_batch: int):
         from q_psdm_b200 import engine as E
         sv = self.sv
-        return E.static_params(nxi=sv.nxi, nzi=sv.nzi, ntl=sv.ntl, dt=float(sv.dt),
-                               dxi=sv.dxi, dyi=sv.dyi, dzi=sv.dzi, fci=sv.fci,
-                               scaled=sv.scaled, fxv=sv.fxv, fyv=sv.fyv, nxv=sv.nxi,
-                               nyv=sv.nyi, fc=30.0, max_batch=max_batch)
+        _, _, dtype, pform = FORMS[form]
+        kw = dict(nxi=sv.nxi, nzi=sv.nzi, ntl=sv.ntl, dt=float(sv.dt), dxi=sv.dxi, dyi=sv.dyi,
+                  dzi=sv.dzi, fci=sv.fci, scaled=sv.scaled, fxv=sv.fxv, fyv=sv.fyv,
+                  nxv=sv.nxi, nyv=sv.nyi, fc=30.0, max_batch=max_batch)
+        if pform is None:
+            return E.static_params(**kw)
+        return E.static_params(**kw, mode=1, panel_dtype=dtype, nbins=16, dtstar=0.002,
+                               form=pform, dzii=self.tables().dzii)
 
-    def line_args(self, contract_rad):
+    def lines(self, form: str, contract_rad: float):
         sv = self.sv
+        nl = FORMS[form][1]
         dips = self.synth.dip_fields(sv.nxi, sv.nzi, contract_rad)
-        return dict(fxi=sv.fxv, cyi=sv.line_y(self.LINE), dips=dips)
+        tab = None if FORMS[form][3] is None else self.tables().as_engine_dict()
+        return [dict(fxi=sv.fxv, cyi=sv.line_y(self.LINE0 + i), dips=dips, tables=tab)
+                for i in range(nl)]
 
     def aperture(self):
         return self.synth.aperture_tables(self.HALF_CDPS, self.HALF_LINES)
 
     def config(self, form):
         sv = self.sv
-        return {"workload": f"config2 {form}: one shot gather ({self.ntr} traces, "
-                            f"nt={sv.ntl}, dt=2ms) per step into a {sv.nxi}x{sv.nzi} image "
-                            f"line ({sv.nxi}x{sv.nyi}x{sv.nzi} volume, 10 m)",
-                "form": form, "traces_per_step": self.ntr, "image_line": [sv.nxi, sv.nzi],
-                "aperture_cdps": [self.HALF_CDPS, self.HALF_CDPS],
-                "aperture_lines": [self.HALF_LINES, self.HALF_LINES],
-                "l2": "flushed (256 MiB write) before every timed step",
-                "data": "synthetic, seeded"}
+        ns, nl, dtype, _ = FORMS[form]
+        return {"workload": f"config2 ({len(sv.shots)} shots x 96x96 receivers, nt={sv.ntl}, "
+                            f"dt=2ms, image {sv.nxi}x{sv.nyi}x{sv.nzi} @10m), form {form}: "
+                            f"{ns} shot gather(s) x {nl} image line(s) of {sv.nxi}x{sv.nzi} "
+                            f"per step",
+                "form": form, "shots_per_step": ns, "lines_per_step": nl,
+                "traces_per_step": ns * self.ntr_shot,
+                "panels": {0: "fp32", 1: "bf16", 2: "fp16"}[dtype] if FORMS[form][3] is not None
+                else "none (stub kernel)",
+                "tables": "analytic v(z)=1800+0.5z traveltime and t* (Q=80), surface and depth "
+                          "subsampled 8x, reference ttt/qqq layout",
+                "aperture_cdps": self.HALF_CDPS, "aperture_lines": self.HALF_LINES,
+                "l2": "flushed (256 MiB write) before every timed step"}
 
 
 # ---------------------------------------------------------------------------
@@ -138,8 +177,7 @@ class ClockSampler:
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                  "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            threading.Thread(target=self._read, daemon=True).start()
         except Exception:
             self.proc = None
 
@@ -173,11 +211,8 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# ---------------------------------------------------------------------------
-# our arm
-# ---------------------------------------------------------------------------
 def fp32_peak_tflops(torch):
-    """Measured FP32 (non-tensor) throughput: cuBLAS SGEMM with TF32 off."""
+    """Measured FP32 (non-tensor) throughput: cuBLAS SGEMM 8192^3, TF32 off."""
     torch.backends.cuda.matmul.allow_tf32 = False
     n = 8192
     a = torch.randn(n, n, device="cuda")
@@ -193,216 +228,280 @@ def fp32_peak_tflops(torch):
         e1.record()
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1))
-    del a, b
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def run_ours(args, rank, world, dist):
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True):
     import torch
-    from q_psdm_b200 import engine as E
     from q_psdm_b200 import _lib
+    from q_psdm_b200 import engine as E
 
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
-    wl = Workload(rank)
-    p = wl.static(args.form, max_batch=wl.ntr)
+    ns, nl, _, _ = FORMS[form]
+    p = wl.static(form, max_batch=ns * wl.ntr_shot)
     eng = E.Engine(p, device=dev)
-    # a dedicated stream: the engine runs on it and the step events are
-    # recorded on it (torch's default stream handle is 0, which the C ABI
-    # reads as "the engine's own stream")
-    stream = torch.cuda.Stream()
+    stream = torch.cuda.Stream()  # non-default: its handle is never 0
     torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
-    eng.set_line(**wl.line_args(p.contract))
+    eng.set_lines(wl.lines(form, p.contract))
     az = wl.aperture()
     o = E.offset_params(p, 0, p.nxi, aznx1=az[0], aznx2=az[1], azny1=az[2], azny2=az[3])
     eng.begin_offset(o)
-
-    nsteps = args.warmup + args.steps
-    nshots = min(nsteps, 4)
-    recs = [wl.records(k) for k in range(nshots)]
+    nbatch = 2
+    recs = [wl.records(k, ns) for k in range(nbatch)]
     drecs = [torch.from_numpy(r).cuda() for r in recs]
+    ntr = recs[0].shape[0]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def step(k):
-        eng.submit_device(drecs[k % nshots].data_ptr(), wl.ntr)
-
-    for k in range(args.warmup):
-        step(k)
+    for k in range(warmup):
+        eng.submit_device(drecs[k % nbatch].data_ptr(), ntr)
     torch.cuda.synchronize()
     _, npt0 = eng.counters()
     eng.profile(True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev)
-    clocks.start()
-    times = []
-    for k in range(args.steps):
+    clk = ClockSampler(dev)
+    if clocks:
+        clk.start()
+    ev = []
+    for k in range(steps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        step(args.warmup + k)
+        eng.submit_device(drecs[k % nbatch].data_ptr(), ntr)
         e1.record(stream)
-        times.append((e0, e1))
+        ev.append((e0, e1))
     torch.cuda.synchronize()
-    clk = clocks.stop()
-    if dist:
-        dist.barrier()
-    ms = sum(a.elapsed_time(b) for a, b in times)
+    ck = clk.stop() if clocks else None
+    ms = sum(a.elapsed_time(b) for a, b in ev)
     _, npt1 = eng.counters()
     npt = npt1 - npt0
-    img_ms, img_launches = eng.kernel_time(_lib.K_IMAGE)
-    launches = sum(eng.kernel_time(c)[1] for c in range(4))
+    kt = {name: eng.kernel_time(c) for name, c in
+          (("gate", _lib.K_GATE), ("panels", _lib.K_PRE), ("image", _lib.K_IMAGE),
+           ("grouping", _lib.K_OTHER))}
     eng.profile(False)
-
-    tot = torch.tensor([ms, float(npt)], dtype=torch.float64, device="cuda")
+    t = torch.tensor([ms, float(npt)], dtype=torch.float64, device="cuda")
     if dist:
-        t_max = tot[0:1].clone()
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-        n_sum = tot[1:2].clone()
-        dist.all_reduce(n_sum, op=dist.ReduceOp.SUM)
-        ms_max, npt_all = float(t_max.item()), float(n_sum.item())
+        tm, tn = t[0:1].clone(), t[1:2].clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tn, op=dist.ReduceOp.SUM)
+        ms_max, npt_all = float(tm.item()), float(tn.item())
     else:
         ms_max, npt_all = ms, float(npt)
-    value = npt_all / (ms_max * 1e-3) / 1e9
+    out = {"value": npt_all / (ms_max * 1e-3) / 1e9, "ms_per_step": ms_max / steps,
+           "point_traces_per_step": npt_all / steps, "clocks": ck,
+           "kernel_ms_per_step": {k: v[0] / steps for k, v in kt.items()},
+           "launches": int(sum(v[1] for v in kt.values())),
+           "image_ms_per_launch": kt["image"][0] / max(kt["image"][1], 1),
+           "image_launches": kt["image"][1], "npt": npt}
 
-    # ---- end to end through the host API ---------------------------------
-    e2e = None
-    if not args.no_e2e:
-        host_recs = recs
+    if e2e:
         eng.set_stream(None)
         eng.begin_offset(o)
-        img_host = None
-        eng.submit(host_recs[0])
-        img_host = eng.get_image(True)
+        pinned = [torch.empty(r.shape, dtype=torch.uint8).pin_memory() for r in recs]
+        for pr, r in zip(pinned, recs):
+            pr.numpy()[:] = r
+        hosts = [pr.numpy() for pr in pinned]
+        eng.submit(hosts[0])
+        img = eng.get_image(True)
         _, n0 = eng.counters()
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
-        for k in range(args.steps):
-            eng.submit(host_recs[k % nshots])
-            img_host = eng.get_image(True)
+        for k in range(steps):
+            eng.submit(hosts[k % nbatch])
+            img = eng.get_image(True)
         t1 = time.perf_counter()
         _, n1 = eng.counters()
-        t = torch.tensor([t1 - t0], dtype=torch.float64, device="cuda")
-        n = torch.tensor([float(n1 - n0)], dtype=torch.float64, device="cuda")
+        te = torch.tensor([t1 - t0], dtype=torch.float64, device="cuda")
+        nn = torch.tensor([float(n1 - n0)], dtype=torch.float64, device="cuda")
         if dist:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dist.all_reduce(n, op=dist.ReduceOp.SUM)
-        e2e = {"value": float(n.item()) / float(t.item()) / 1e9, "unit": "Gpoint-traces/s",
-               "h2d_bytes_per_step": int(host_recs[0].nbytes),
-               "d2h_bytes_per_step": int(img_host.nbytes),
-               "path": "qpsdm_submit_traces (host SU records -> pinned staging -> H2D) + "
-                       "qpsdm_get_image every step"}
-
-    result = None
-    if rank == 0:
-        peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-        fp32 = fp32_peak_tflops(torch)
-        peak_note = "fp32 peak measured in this run: cuBLAS SGEMM 8192^3, TF32 off"
-        achieved = npt / args.steps * F_PT_COMPAT / (img_ms / max(img_launches, 1) * 1e-3) / 1e12 \
-            if img_launches else None
-        per_launch_npt = npt / max(img_launches, 1)
-        roof = {"bound": "fp32", "kernel": "k_image_compat",
-                "achieved": achieved, "peak": fp32, "unit": "TFLOP/s",
-                "frac": (achieved / fp32) if achieved else None,
-                "traffic": None,
-                "flop_per_point_trace": F_PT_COMPAT,
-                "point_traces_per_launch": per_launch_npt,
-                "kernel_ms_per_launch": img_ms / max(img_launches, 1),
-                "peak_source": peak_note,
-                "note": "imaging is an FP32 CUDA-core gather/accumulate, not HBM or "
-                        "tensor bound; traffic per launch from ncu is in profiles/"}
-        if os.path.exists(peaks_path):
-            roof["hbm_peak_gbs_measured"] = json.load(open(peaks_path)).get("hbm_gbs")
-        result = {
-            "metric": METRIC, "value": value, "unit": "Gpoint-traces/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic", "config": wl.config(args.form),
-            "roofline": roof, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
-            "point_traces_per_step": npt_all / args.steps,
-        }
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+            dist.all_reduce(nn, op=dist.ReduceOp.SUM)
+        out["e2e"] = {"value": float(nn.item()) / float(te.item()) / 1e9,
+                      "unit": "Gpoint-traces/s", "h2d_bytes_per_step": int(recs[0].nbytes),
+                      "d2h_bytes_per_step": int(img.nbytes),
+                      "path": "qpsdm_submit_traces from pinned host SU records (DMA) + "
+                              "qpsdm_get_image every step"}
     eng.close()
-    return result, wl
+    torch.cuda.set_stream(torch.cuda.default_stream())
+    return out
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    wl = Workload(rank)
+    head = run_form(args.form, wl, args, dev, dist, steps=args.steps, warmup=args.warmup,
+                    e2e=not args.no_e2e)
+    forms = {args.form: {k: head[k] for k in ("value", "ms_per_step", "point_traces_per_step",
+                                              "kernel_ms_per_step")}}
+    if args.form == "batched":
+        pl = run_form("plain", wl, args, dev, dist, steps=max(3, args.steps // 2),
+                      warmup=2, e2e=False, clocks=False)
+        forms["plain"] = {k: pl[k] for k in ("value", "ms_per_step", "point_traces_per_step",
+                                             "kernel_ms_per_step")}
+        forms["batched_over_plain"] = head["value"] / pl["value"]
+    if rank != 0:
+        return None, wl
+    fp32 = fp32_peak_tflops(torch)
+    npt_launch = head["npt"] / max(head["image_launches"], 1)
+    achieved = npt_launch * F_PT[args.form] / (head["image_ms_per_launch"] * 1e-3) / 1e12
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    roof = {"bound": "fp32", "kernel": {"batched": "k_image_batched", "plain": "k_image_plain",
+                                        "compat": "k_image_compat"}[args.form],
+            "achieved": achieved, "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32,
+            "traffic": None, "flop_per_point_trace": F_PT[args.form],
+            "point_traces_per_launch": npt_launch,
+            "kernel_ms_per_launch": head["image_ms_per_launch"],
+            "peak_source": "measured in this run: cuBLAS SGEMM 8192^3, TF32 off (of measured)",
+            "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),
+            "note": "imaging is a data-dependent FP32 gather/accumulate (not a dense "
+                    "contraction, not HBM-bound); DRAM traffic per launch from ncu is in "
+                    "profiles/"}
+    res = {"metric": METRIC, "value": head["value"], "unit": "Gpoint-traces/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 (bf16 panels)" if args.form == "batched" else "f32",
+           "data": "synthetic", "config": wl.config(args.form), "roofline": roof,
+           "e2e": head.get("e2e"), "gpu_launches": head["launches"], "clocks": head["clocks"],
+           "point_traces_per_step": head["point_traces_per_step"],
+           "kernel_ms_per_step": head["kernel_ms_per_step"], "forms": forms}
+    return res, wl
 
 
 # ---------------------------------------------------------------------------
-# CPU arm (reference CPU path / cpu_baseline)
+# CPU legs
 # ---------------------------------------------------------------------------
-def cpu_path_rate(wl: Workload, ntrace_sample: int, budget_s: float = 12.0):
-    """Reference CPU path on a bounded sample of one shot: preprocessing by the
-    reference's compiled code (or the oracle when oracle/_ref is absent) and
-    the stub imaging by the C restatement, all host threads."""
-    from oracle import oracle as O
+def _gate_params(O, wl, line):
     sv = wl.sv
-    st = O.derive_static(sv.ntl, np.float32(sv.dt), 600.0, 3.0, 8.0)
-    w = O.window_split(sv.ntl, np.float32(sv.dt), 1.0, 140.0)
-    iaz = O.iaztab()
     az = np.stack(wl.aperture()).astype(np.int32)
-    ly = sv.line_y(wl.LINE)
-    keep = [iaz] + [np.ascontiguousarray(az[i]) for i in range(4)]
-    import ctypes as C
+    keep = [O.iaztab()] + [np.ascontiguousarray(az[i]) for i in range(4)]
     ip = lambda x: x.ctypes.data_as(C.POINTER(C.c_int))
     gp = O.GateParams(scaled=sv.scaled, fxv1=np.float32(sv.fxv - 2000.0),
                       fyv1=np.float32(sv.fyv - 1000.0),
                       exv1=np.float32(sv.fxv + sv.nxi * sv.dxi + 2000.0),
-                      eyv1=np.float32(sv.fyv + sv.nyi * sv.dyi + 1000.0), fxi=sv.fxv, cyi=ly,
-                      dxi=sv.dxi, dyi=sv.dyi, eps=0.001, nzi=sv.nzi, ixstart=0, ixend=sv.nxi,
-                      iaztab=ip(keep[0]), aznx1=ip(keep[1]), aznx2=ip(keep[2]),
-                      azny1=ip(keep[3]), azny2=ip(keep[4]))
+                      eyv1=np.float32(sv.fyv + sv.nyi * sv.dyi + 1000.0), fxi=sv.fxv,
+                      cyi=sv.line_y(line), dxi=sv.dxi, dyi=sv.dyi, eps=0.001, nzi=sv.nzi,
+                      ixstart=0, ixend=sv.nxi, iaztab=ip(keep[0]), aznx1=ip(keep[1]),
+                      aznx2=ip(keep[2]), azny1=ip(keep[3]), azny2=ip(keep[4]))
+    gp._keep = keep
+    return gp
+
+
+def _hdr_traces(rec):
+    hdr = np.stack([rec[:, o:o + 4].copy().view(">i4").ravel() for o in (72, 76, 80, 84)],
+                   axis=1).astype(np.int32)
+    return hdr, rec[:, 240:].copy().view(">f4").astype(np.float32)
+
+
+def cpu_compat_rate(wl, budget_s=10.0):
+    """The reference's CPU path of one image line: gate, its preprocessing
+    (compiled reference code when oracle/_ref exists, else the oracle) and the
+    C restatement of its imaging kernel, all host threads."""
+    from oracle import oracle as O
+    sv = wl.sv
+    line = wl.LINE0
+    st = O.derive_static(sv.ntl, np.float32(sv.dt), 600.0, 3.0, 8.0)
+    w = O.window_split(sv.ntl, np.float32(sv.dt), 1.0, 140.0)
+    gp = _gate_params(O, wl, line)
     ipar = O.ImageParams(nzi=sv.nzi, nxb=sv.nxi, ixstart=0, nt=st["nffti"], dt1=st["dt1"],
                          dxi=sv.dxi, dzi=sv.dzi, taperzone=st["taperzone"], tcdp1=0,
                          tcdp2=sv.nxi - 1)
     dips = [d.ravel() for d in wl.synth.dip_fields(sv.nxi, sv.nzi, float(st["contract"]))]
-    rec = wl.records(0)
-    hdr = np.stack([rec[:, o:o + 4].copy().view(">i4").ravel() for o in (72, 76, 80, 84)],
-                   axis=1).astype(np.int32)
-    traces = rec[:, 240:].copy().view(">f4").astype(np.float32)
+    hdr, traces = _hdr_traces(wl.records(0, 1))
     R = O.ref_cpu()
-    kind = "reference" if R is not None else "port"
     nthr = os.cpu_count() or 1
     img = np.zeros(sv.nxi * sv.nzi, np.float32)
-    # grow the sample until it costs ~budget_s
-    n = min(ntrace_sample, hdr.shape[0])
-    t_total, npt_total, ntr_total = 0.0, 0, 0
-    idx0 = 0
+    n, t_tot, npt_tot, ntr_tot, i0 = 256, 0.0, 0, 0, 0
     while True:
-        sl = slice(idx0 % hdr.shape[0], idx0 % hdr.shape[0] + n)
+        sl = slice(i0 % hdr.shape[0], i0 % hdr.shape[0] + n)
         h, tr = hdr[sl], traces[sl]
         t0 = time.perf_counter()
         ints, geom = O.gate_traces(gp, h)
         ok = ints[:, 0] == 3
         nok = int(ok.sum())
-        re = np.zeros((max(nok, 1), 2 * w["nww"]), np.float32)
-        im = np.zeros_like(re)
+        npt = 0
         if nok:
+            re = np.zeros((nok, 2 * w["nww"]), np.float32)
+            im = np.zeros_like(re)
             if R is not None:
                 R.ref_preprocess_traces(np.ascontiguousarray(tr[ok]), nok, sv.ntl,
                                         np.float32(sv.dt), w["itb1"], w["itb2"], w["nsb"],
                                         w["nf1"], w["nww"], w["dw"], re, im, nthr)
             else:
-                for i, j in enumerate(np.nonzero(ok)[0]):
-                    re[i], im[i] = O.preprocess_trace(tr[j], np.float32(sv.dt), w)
+                for k, j in enumerate(np.nonzero(ok)[0]):
+                    re[k], im[k] = O.preprocess_trace(tr[j], np.float32(sv.dt), w)
             _, npt = O.image_compat(ipar, geom[ok], np.ascontiguousarray(ints[ok][:, [4, 5, 7]]),
                                     dips, img)
-        else:
-            npt = 0
-        t_total += time.perf_counter() - t0
-        npt_total += npt
-        ntr_total += n
-        idx0 += n
-        if t_total >= budget_s or ntr_total >= 4 * hdr.shape[0]:
+        t_tot += time.perf_counter() - t0
+        npt_tot += npt
+        ntr_tot += n
+        i0 += n
+        if t_tot >= budget_s or ntr_tot >= 8 * hdr.shape[0]:
             break
-        if t_total < budget_s / 8:
+        if t_tot < budget_s / 8:
             n = min(hdr.shape[0], n * 2)
-    return {"value": npt_total / t_total / 1e9, "unit": "Gpoint-traces/s", "cores": nthr,
+    kind = "reference" if R is not None else "port"
+    return {"value": npt_tot / t_tot / 1e9, "unit": "Gpoint-traces/s", "cores": nthr,
             "kind": kind,
-            "sample": f"{ntr_total} traces of a config-2 shot gather into the 512x400 line "
-                      f"({npt_total} point-traces, {t_total:.1f} s): gate + reference "
-                      f"preprocessing ({'oracle/_ref' if R is not None else 'oracle port'}) "
-                      f"+ C restatement of image_depth_gpu, {nthr} threads"}
+            "sample": f"{ntr_tot} traces of a config-2 shot gather into one 512x400 line "
+                      f"({npt_tot} point-traces, {t_tot:.1f} s): gate + the reference's "
+                      f"preprocessing ({'compiled from its sources' if R is not None else 'oracle'})"
+                      f" + C restatement of image_depth_gpu, {nthr} threads"}
+
+
+def cpu_physics_rate(wl, budget_s=10.0):
+    """The physics method on the CPU (the FP64 restatement: numpy panels + C
+    imaging, all host threads) on a bounded sample of one shot and one line."""
+    from oracle import oracle as O
+    sv = wl.sv
+    line = wl.LINE0
+    st = O.derive_static(sv.ntl, np.float32(sv.dt), 600.0, 3.0, 8.0)
+    gp = _gate_params(O, wl, line)
+    tab = wl.tables()
+    pp = O.PhysParams(nzi=sv.nzi, nxb=sv.nxi, ixstart=0, nt=st["nffti"], nbins=16,
+                      dt1=float(st["dt1"]), dxi=sv.dxi, dzi=sv.dzi,
+                      taperzone=float(st["taperzone"]), dtstar=float(np.float32(0.002)),
+                      dzii=tab.dzii, tcdp1=tab.cdp1 - sv.fci, tcdp2=tab.cdp2 - sv.fci,
+                      nxg=tab.nxg, nzg=tab.nzg, nxi1=tab.nxi1, nzi1=tab.nzi1)
+    filt = O.physics_filter(st["nfft"], np.float32(sv.dt), 130.0, 140.0, 30.0, 600.0, 16, 0.002)
+    dips = [d.ravel() for d in wl.synth.dip_fields(sv.nxi, sv.nzi, float(st["contract"]))]
+    hdr, traces = _hdr_traces(wl.records(0, 1))
+    nthr = os.cpu_count() or 1
+    img = np.zeros(sv.nxi * sv.nzi)
+    rng = np.random.default_rng(1)
+    n, t_tot, npt_tot, ntr_tot = 8, 0.0, 0, 0
+    while True:
+        idx = rng.choice(hdr.shape[0], n, replace=False)
+        t0 = time.perf_counter()
+        ints, geom = O.gate_traces(gp, hdr[idx])
+        ok = ints[:, 0] == 3
+        npt = 0
+        if ok.any():
+            pan = O.physics_panels(traces[idx][ok], np.float32(sv.dt), st["nfft"], st["nffti"],
+                                   filt)
+            _, npt = O.physics_image(pp, geom[ok], ints[ok][:, [4, 5, 7]], pan, dips,
+                                     tab.as_engine_dict(), img)
+        t_tot += time.perf_counter() - t0
+        npt_tot += npt
+        ntr_tot += n
+        if t_tot >= budget_s or ntr_tot >= 4096:
+            break
+        if t_tot < budget_s / 8:
+            n = min(512, n * 2)
+    return {"value": npt_tot / t_tot / 1e9, "unit": "Gpoint-traces/s", "cores": nthr,
+            "kind": "port",
+            "sample": f"{ntr_tot} random traces of a config-2 shot into one 512x400 line "
+                      f"({npt_tot} point-traces, {t_tot:.1f} s): the FP64 CPU restatement of "
+                      f"the physics method (numpy float64 panels + C imaging), {nthr} threads"}
 
 
 def run_reference(args, rank, world):
@@ -410,12 +509,12 @@ def run_reference(args, rank, world):
         return None
     wl = Workload(0)
     for _ in range(args.warmup):
-        cpu_path_rate(wl, 64, budget_s=0.5)
+        cpu_compat_rate(wl, budget_s=0.3)
     vals = []
     t0 = time.perf_counter()
     info = None
     for _ in range(args.steps):
-        info = cpu_path_rate(wl, 256, budget_s=max(1.0, 60.0 / max(args.steps, 1)))
+        info = cpu_compat_rate(wl, budget_s=max(1.0, 60.0 / max(args.steps, 1)))
         vals.append(info["value"])
     el = time.perf_counter() - t0
     v = float(np.mean(vals))
@@ -446,7 +545,8 @@ def main():
     else:
         res, wl = run_ours(args, rank, world, dist)
         if res is not None and not args.no_cpu:
-            res["cpu_baseline"] = cpu_path_rate(wl, 256)
+            res["cpu_baseline"] = (cpu_compat_rate(wl) if args.form == "compat"
+                                   else cpu_physics_rate(wl))
     if res is not None:
         print(json.dumps(res), flush=True)
     if dist:

@@ -89,8 +89,19 @@ typedef struct {
   float dtstar;    /* t* bin spacing (s) */
   int max_batch;   /* largest ntr of one submit (sizes device buffers) */
   int kahan;       /* 1 = compensated FP32 image accumulation (physics) */
-  int reserved[8];
+  int form;        /* physics: QPSDM_FORM_PLAIN or QPSDM_FORM_BATCHED */
+  int use_graph;   /* batched form: replay each batch as a captured CUDA graph */
+  int tile_z, tile_x; /* batched image tile (0 = autotuned) */
+  int reserved[4];
 } qpsdm_static_params;
+
+/* Physics forms.  PLAIN: one pass per trace in submission order with table
+ * lookups per point-trace (source terms reused while consecutive traces share
+ * a source).  BATCHED: traces of a batch grouped by receiver position and
+ * source; source terms built once per shot and image tile, receiver terms
+ * once per receiver position, a persistent kernel over image tiles, and t*
+ * panels stored as neighbouring-bin pairs. */
+enum { QPSDM_FORM_PLAIN = 0, QPSDM_FORM_BATCHED = 1 };
 
 /* Per-line state: mirrors the line part of CPUParamsWithLine
  * (src/q-psdm.cu:149-179) and the line buffers of GPUParamsWithLine
@@ -159,6 +170,13 @@ const char *qpsdm_last_error(const qpsdm_engine *e);
  * (src/q-psdm.cu:1449-1515). */
 int qpsdm_set_line(qpsdm_engine *e, const qpsdm_line_params *l);
 
+/* A brick of nlines image lines imaged together: every submitted trace is
+ * gated and imaged for each line (the reference's line loop,
+ * src/q-psdm.cu:1427, run over the same traces), and the image becomes
+ * [nlines][nxb][nzi].  In the batched physics form the compensated panels of
+ * a trace are computed once and shared by all lines of the brick. */
+int qpsdm_set_lines(qpsdm_engine *e, const qpsdm_line_params *lines, int nlines);
+
 /* Replaces the per-offset set-up of qpsdm() (src/q-psdm.cu:1593-1691). */
 int qpsdm_begin_offset(qpsdm_engine *e, const qpsdm_offset_params *o);
 
@@ -202,6 +220,13 @@ enum { QPSDM_K_GATE = 0, QPSDM_K_PRE = 1, QPSDM_K_IMAGE = 2, QPSDM_K_OTHER = 3 }
 int qpsdm_profile_enable(qpsdm_engine *e, int on);
 int qpsdm_profile_get(qpsdm_engine *e, int kernel_class, double *total_ms,
                       int64_t *launches);
+
+/* Batched physics form: the image-kernel variant the autotuner chose on the
+ * first batch (tile depth x cdps, minimum resident blocks per SM) and the
+ * timing of every variant (ms, up to nms values).  Returns the number of
+ * variants, or a negative/error status.  No reference counterpart. */
+int qpsdm_tuning_info(qpsdm_engine *e, int *variant, int *tile_z, int *tile_x,
+                      int *min_blocks, float *ms, int nms);
 
 /* Counters since begin_offset: traces accepted by the gate and point-traces
  * evaluated (one per image point inside a trace's aperture). */

@@ -41,7 +41,8 @@ class StaticParams(C.Structure):
         ("coef3", C.c_float), ("coef4", C.c_float),
         ("mode", C.c_int), ("panel_dtype", C.c_int), ("nbins", C.c_int),
         ("dtstar", C.c_float), ("max_batch", C.c_int), ("kahan", C.c_int),
-        ("reserved", C.c_int * 8),
+        ("form", C.c_int), ("use_graph", C.c_int), ("tile_z", C.c_int), ("tile_x", C.c_int),
+        ("reserved", C.c_int * 4),
     ]
 
 
@@ -83,6 +84,7 @@ SYMBOLS = [
     ("qpsdm_engine_destroy", _I, [_P]),
     ("qpsdm_last_error", C.c_char_p, [_P]),
     ("qpsdm_set_line", _I, [_P, C.POINTER(LineParams)]),
+    ("qpsdm_set_lines", _I, [_P, C.POINTER(LineParams), _I]),
     ("qpsdm_begin_offset", _I, [_P, C.POINTER(OffsetParams)]),
     ("qpsdm_submit_traces", _I, [_P, _P, _I, _I, _I]),
     ("qpsdm_submit_traces_device", _I, [_P, _P, _I, _I, _I]),
@@ -90,6 +92,8 @@ SYMBOLS = [
     ("qpsdm_get_image", _I, [_P, _P, _I]),
     ("qpsdm_image_device_ptr", _I, [_P, C.POINTER(C.c_void_p)]),
     ("qpsdm_set_stream", _I, [_P, _P]),
+    ("qpsdm_tuning_info", _I, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                               C.POINTER(C.c_int), _P, _I]),
     ("qpsdm_profile_enable", _I, [_P, _I]),
     ("qpsdm_profile_get", _I, [_P, _I, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("qpsdm_get_counters", _I, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),

@@ -45,10 +45,11 @@ struct qpsdm_engine {
   float *d_geom = nullptr;
   unsigned *d_err = nullptr;
   unsigned long long *d_npt = nullptr;
-  // line
+  // lines of the image brick
   bool line_set = false;
-  qpsdm_line_params line{};
-  float *d_dips = nullptr;
+  std::vector<qpsdm_line_params> lines;
+  int lines_cap = 0;     // lines the per-line buffers hold
+  float *d_dips = nullptr;  // [line][4][nxi][nzi]
   size_t nxz = 0;
   // offset
   bool offset_set = false;
@@ -216,26 +217,45 @@ extern "C" int qpsdm_engine_destroy(qpsdm_engine *e) {
   return QPSDM_OK;
 }
 
-extern "C" int qpsdm_set_line(qpsdm_engine *e, const qpsdm_line_params *l) {
-  if (!e || !l) return QPSDM_EINVAL;
-  if (!l->dipx1 || !l->dipx2 || !l->dipy1 || !l->dipy2)
-    return fail(e, QPSDM_EINVAL, "dip fields are required");
+extern "C" int qpsdm_set_lines(qpsdm_engine *e, const qpsdm_line_params *l, int nlines) {
+  if (!e || !l || nlines <= 0) return QPSDM_EINVAL;
+  for (int il = 0; il < nlines; ++il)
+    if (!l[il].dipx1 || !l[il].dipx2 || !l[il].dipy1 || !l[il].dipy2)
+      return fail(e, QPSDM_EINVAL, "dip fields are required");
   DeviceGuard g(e->device);
   CK(cudaStreamSynchronize(e->s_comp));
   e->nxz = (size_t)e->p.nxi * e->p.nzi;
-  if (!e->d_dips) CK(cudaMalloc(&e->d_dips, sizeof(float) * 4 * e->nxz));
-  const float *f[4] = {l->dipx1, l->dipx2, l->dipy1, l->dipy2};
-  for (int i = 0; i < 4; ++i)
-    CK(cudaMemcpy(e->d_dips + i * e->nxz, f[i], sizeof(float) * e->nxz,
-                  cudaMemcpyHostToDevice));
+  if (nlines > e->lines_cap) {  // per-line dip fields and gate results
+    cudaFree(e->d_dips);
+    cudaFree(e->d_ints);
+    cudaFree(e->d_geom);
+    e->d_dips = nullptr;
+    e->d_ints = nullptr;
+    e->d_geom = nullptr;
+    e->lines_cap = 0;
+    CK(cudaMalloc(&e->d_dips, sizeof(float) * 4 * e->nxz * nlines));
+    CK(cudaMalloc(&e->d_ints, sizeof(int) * kGateInts * (size_t)e->p.max_batch * nlines));
+    CK(cudaMalloc(&e->d_geom, sizeof(float) * kGateF * (size_t)e->p.max_batch * nlines));
+    e->lines_cap = nlines;
+  }
+  for (int il = 0; il < nlines; ++il) {
+    const float *f[4] = {l[il].dipx1, l[il].dipx2, l[il].dipy1, l[il].dipy2};
+    for (int i = 0; i < 4; ++i)
+      CK(cudaMemcpy(e->d_dips + (size_t)il * 4 * e->nxz + i * e->nxz, f[i],
+                    sizeof(float) * e->nxz, cudaMemcpyHostToDevice));
+  }
   if (e->p.mode == QPSDM_MODE_PHYSICS) {
-    int rc = physics_set_line(e->phys, e->p, *l, e->s_comp, &e->err);
+    int rc = physics_set_lines(e->phys, e->p, l, nlines, e->s_comp, &e->err);
     if (rc) return rc;
   }
-  e->line = *l;
+  e->lines.assign(l, l + nlines);
   e->line_set = true;
   e->offset_set = false;
   return QPSDM_OK;
+}
+
+extern "C" int qpsdm_set_line(qpsdm_engine *e, const qpsdm_line_params *l) {
+  return qpsdm_set_lines(e, l, 1);
 }
 
 extern "C" int qpsdm_begin_offset(qpsdm_engine *e, const qpsdm_offset_params *o) {
@@ -260,14 +280,14 @@ extern "C" int qpsdm_begin_offset(qpsdm_engine *e, const qpsdm_offset_params *o)
   if ((rc = grow(e, &e->d_re, &cap_re, need))) return rc;
   if ((rc = grow(e, &e->d_im, &cap_im, need))) return rc;
   e->spec_cap = cap_re;
-  const size_t nimg = (size_t)(o->ixend - o->ixstart) * e->p.nzi;
+  const size_t nimg = (size_t)(o->ixend - o->ixstart) * e->p.nzi * e->lines.size();
   const bool realloc_img = e->img_cap < nimg;
   if ((rc = grow(e, &e->d_img, &e->img_cap, nimg))) return rc;
   if (o->zero_image || realloc_img || !e->offset_set)
     CK(cudaMemsetAsync(e->d_img, 0, sizeof(float) * nimg, e->s_comp));
   CK(cudaMemsetAsync(e->d_npt, 0, sizeof(unsigned long long), e->s_comp));
   if (e->p.mode == QPSDM_MODE_PHYSICS) {
-    rc = physics_begin_offset(e->phys, e->p, *o, e->s_comp, &e->err);
+    rc = physics_begin_offset(e->phys, e->p, *o, (int)e->lines.size(), e->s_comp, &e->err);
     if (rc) return rc;
   }
   e->off = *o;
@@ -280,64 +300,78 @@ namespace {
 
 // Kernels of one batch whose records are in device memory.
 int process_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
-  GateArgs g{};
-  g.scaled = e->p.scaled;
-  g.fxi = e->line.fxi;
-  g.cyi = e->line.cyi;
-  g.fxv1 = e->p.fxv1;
-  g.fyv1 = e->p.fyv1;
-  g.exv1 = e->p.exv1;
-  g.eyv1 = e->p.eyv1;
-  g.dxi = e->p.dxi;
-  g.dyi = e->p.dyi;
-  g.eps = e->p.eps;
-  g.nzi = e->p.nzi;
-  g.ixstart = e->off.ixstart;
-  g.ixend = e->off.ixend;
-  g.naztab = e->naztab;
-  g.iaztab = e->d_iaztab;
-  memcpy(g.az[0], e->off.aznx1, sizeof(int) * QPSDM_NAZ);
-  memcpy(g.az[1], e->off.aznx2, sizeof(int) * QPSDM_NAZ);
-  memcpy(g.az[2], e->off.azny1, sizeof(int) * QPSDM_NAZ);
-  memcpy(g.az[3], e->off.azny2, sizeof(int) * QPSDM_NAZ);
-  e->prof.begin(QPSDM_K_GATE, e->s_comp);
-  int rc = launch_gate(d_rec, (int)e->rec_bytes, ntr, be, g, e->d_ints, e->d_geom,
-                       e->d_err, e->s_comp);
-  e->prof.end(e->s_comp);
-  if (rc) return fail(e, rc, "gate launch failed");
+  const int nlines = (int)e->lines.size();
+  const int nxb = e->off.ixend - e->off.ixstart;
+  const size_t ints_ls = (size_t)kGateInts * e->p.max_batch;  // per-line strides
+  const size_t geom_ls = (size_t)kGateF * e->p.max_batch;
+  const size_t img_ls = (size_t)nxb * e->p.nzi;
+  // gate every line of the brick (src/q-psdm.cu:2107-2171 for each line's cyi)
+  for (int il = 0; il < nlines; ++il) {
+    const qpsdm_line_params &ln = e->lines[il];
+    GateArgs g{};
+    g.scaled = e->p.scaled;
+    g.fxi = ln.fxi;
+    g.cyi = ln.cyi;
+    g.fxv1 = e->p.fxv1;
+    g.fyv1 = e->p.fyv1;
+    g.exv1 = e->p.exv1;
+    g.eyv1 = e->p.eyv1;
+    g.dxi = e->p.dxi;
+    g.dyi = e->p.dyi;
+    g.eps = e->p.eps;
+    g.nzi = e->p.nzi;
+    g.ixstart = e->off.ixstart;
+    g.ixend = e->off.ixend;
+    g.naztab = e->naztab;
+    g.iaztab = e->d_iaztab;
+    memcpy(g.az[0], e->off.aznx1, sizeof(int) * QPSDM_NAZ);
+    memcpy(g.az[1], e->off.aznx2, sizeof(int) * QPSDM_NAZ);
+    memcpy(g.az[2], e->off.azny1, sizeof(int) * QPSDM_NAZ);
+    memcpy(g.az[3], e->off.azny2, sizeof(int) * QPSDM_NAZ);
+    e->prof.begin(QPSDM_K_GATE, e->s_comp);
+    int rc = launch_gate(d_rec, (int)e->rec_bytes, ntr, be, g, e->d_ints + il * ints_ls,
+                         e->d_geom + il * geom_ls, e->d_err, e->s_comp);
+    e->prof.end(e->s_comp);
+    if (rc) return fail(e, rc, "gate launch failed");
+  }
   if (e->p.mode == QPSDM_MODE_COMPAT) {
-    SpectraArgs a{};
-    a.ntl = e->p.ntl;
-    a.nsb = e->off.nsb;
-    a.itb1 = e->off.itb1;
-    a.itb2 = e->off.itb2;
-    a.nf1 = e->off.nf1;
-    a.nww = e->off.nww;
-    a.dt = e->p.dt;
-    a.taper200 = e->d_taper200;
-    a.omega = e->d_omega;
-    e->prof.begin(QPSDM_K_PRE, e->s_comp);
-    rc = launch_spectra(d_rec, (int)e->rec_bytes, ntr, be, e->d_ints, a, e->d_re,
-                        e->d_im, e->s_comp);
-    e->prof.end(e->s_comp);
-    if (rc) return fail(e, rc, "spectra launch failed");
-    CompatImageArgs c{};
-    c.nzi = e->p.nzi;
-    c.nxb = e->off.ixend - e->off.ixstart;
-    c.ixstart = e->off.ixstart;
-    c.nt = e->p.nffti;
-    c.dt1 = e->p.dt1;
-    c.dxi = e->p.dxi;
-    c.dzi = e->p.dzi;
-    c.taperzone = e->p.taperzone;
-    c.tcdp1 = e->line.ttt_cdp1 - e->p.fci;
-    c.tcdp2 = e->line.ttt_cdp2 - e->p.fci;
-    c.nxz = e->nxz;
-    e->prof.begin(QPSDM_K_IMAGE, e->s_comp);
-    rc = launch_image_compat(e->d_img, c, e->d_dips, e->d_ints, e->d_geom, ntr,
-                             e->d_npt, e->s_comp);
-    e->prof.end(e->s_comp);
-    if (rc) return fail(e, rc, "image launch failed");
+    // the reference preprocesses and images each trace once per line
+    for (int il = 0; il < nlines; ++il) {
+      const qpsdm_line_params &ln = e->lines[il];
+      SpectraArgs a{};
+      a.ntl = e->p.ntl;
+      a.nsb = e->off.nsb;
+      a.itb1 = e->off.itb1;
+      a.itb2 = e->off.itb2;
+      a.nf1 = e->off.nf1;
+      a.nww = e->off.nww;
+      a.dt = e->p.dt;
+      a.taper200 = e->d_taper200;
+      a.omega = e->d_omega;
+      e->prof.begin(QPSDM_K_PRE, e->s_comp);
+      int rc = launch_spectra(d_rec, (int)e->rec_bytes, ntr, be, e->d_ints + il * ints_ls, a,
+                              e->d_re, e->d_im, e->s_comp);
+      e->prof.end(e->s_comp);
+      if (rc) return fail(e, rc, "spectra launch failed");
+      CompatImageArgs c{};
+      c.nzi = e->p.nzi;
+      c.nxb = nxb;
+      c.ixstart = e->off.ixstart;
+      c.nt = e->p.nffti;
+      c.dt1 = e->p.dt1;
+      c.dxi = e->p.dxi;
+      c.dzi = e->p.dzi;
+      c.taperzone = e->p.taperzone;
+      c.tcdp1 = ln.ttt_cdp1 - e->p.fci;
+      c.tcdp2 = ln.ttt_cdp2 - e->p.fci;
+      c.nxz = e->nxz;
+      e->prof.begin(QPSDM_K_IMAGE, e->s_comp);
+      rc = launch_image_compat(e->d_img + il * img_ls, c, e->d_dips + (size_t)il * 4 * e->nxz,
+                               e->d_ints + il * ints_ls, e->d_geom + il * geom_ls, ntr,
+                               e->d_npt, e->s_comp);
+      e->prof.end(e->s_comp);
+      if (rc) return fail(e, rc, "image launch failed");
+    }
     return QPSDM_OK;
   }
   PhysicsBatch b{};
@@ -345,16 +379,20 @@ int process_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
   b.rec_bytes = (int)e->rec_bytes;
   b.ntr = ntr;
   b.big_endian = be;
+  b.nlines = nlines;
   b.d_ints = e->d_ints;
+  b.ints_ls = ints_ls;
   b.d_geom = e->d_geom;
+  b.geom_ls = geom_ls;
   b.d_taper200 = e->d_taper200;
   b.d_dips = e->d_dips;
   b.nxz = e->nxz;
   b.d_img = e->d_img;
+  b.img_ls = img_ls;
   b.d_npt = e->d_npt;
   b.d_err = e->d_err;
   b.prof = &e->prof;
-  return physics_process(e->phys, e->p, e->line, e->off, b, e->s_comp, &e->err);
+  return physics_process(e->phys, e->p, e->lines.data(), e->off, b, e->s_comp, &e->err);
 }
 
 }  // namespace
@@ -380,15 +418,24 @@ extern "C" int qpsdm_submit_traces(qpsdm_engine *e, const void *records, int ntr
   if (ntr < 0) return fail(e, QPSDM_EINVAL, "negative ntr");
   DeviceGuard g(e->device);
   const uint8_t *src = (const uint8_t *)records;
+  // Records already in page-locked memory are copied by DMA directly; others
+  // go through the engine's pinned staging slots.
+  cudaPointerAttributes pa;
+  const bool pinned = cudaPointerGetAttributes(&pa, records) == cudaSuccess &&
+                      pa.type == cudaMemoryTypeHost;
+  cudaGetLastError();  // a pageable pointer may leave an error behind
   while (ntr > 0) {
     const int n = ntr < e->p.max_batch ? ntr : e->p.max_batch;
     const size_t bytes = e->rec_bytes * n;
     const int s = e->slot;
     CK(cudaEventSynchronize(e->ev_stage_free[s]));
-    memcpy(e->h_stage[s], src, bytes);
+    if (!pinned) memcpy(e->h_stage[s], src, bytes);
     CK(cudaStreamWaitEvent(e->s_copy, e->ev_rec_free[s], 0));
-    CK(cudaMemcpyAsync(e->d_rec[s], e->h_stage[s], bytes, cudaMemcpyHostToDevice, e->s_copy));
+    CK(cudaMemcpyAsync(e->d_rec[s], pinned ? src : e->h_stage[s], bytes,
+                       cudaMemcpyHostToDevice, e->s_copy));
     CK(cudaEventRecord(e->ev_stage_free[s], e->s_copy));
+    // a caller's pinned buffer may be reused once the call returns
+    if (pinned) CK(cudaEventSynchronize(e->ev_stage_free[s]));
     CK(cudaEventRecord(e->ev_rec_ready[s], e->s_copy));
     CK(cudaStreamWaitEvent(e->s_comp, e->ev_rec_ready[s], 0));
     int rc = process_batch(e, e->d_rec[s], n, be);
@@ -422,7 +469,7 @@ extern "C" int qpsdm_get_image(qpsdm_engine *e, float *host_img, int apply_nsb_s
   int rc = qpsdm_fence(e);
   if (rc) return rc;
   DeviceGuard g(e->device);
-  const size_t n = (size_t)(e->off.ixend - e->off.ixstart) * e->p.nzi;
+  const size_t n = (size_t)(e->off.ixend - e->off.ixstart) * e->p.nzi * e->lines.size();
   if (e->p.mode == QPSDM_MODE_PHYSICS) {
     rc = physics_finalize_image(e->phys, e->d_img, n, e->s_comp, &e->err);
     if (rc) return rc;
@@ -457,6 +504,13 @@ extern "C" int qpsdm_profile_get(qpsdm_engine *e, int cls, double *ms, int64_t *
   if (ms) *ms = e->prof.total_ms(cls);
   if (launches) *launches = e->prof.launches[cls];
   return QPSDM_OK;
+}
+
+extern "C" int qpsdm_tuning_info(qpsdm_engine *e, int *variant, int *tile_z, int *tile_x,
+                                 int *min_blocks, float *ms, int nms) {
+  if (!e) return QPSDM_EINVAL;
+  if (!e->phys) return fail(e, QPSDM_ESTATE, "no physics state");
+  return physics_tuning(e->phys, variant, tile_z, tile_x, min_blocks, ms, nms);
 }
 
 extern "C" int qpsdm_image_device_ptr(qpsdm_engine *e, float **d_img) {

@@ -51,15 +51,21 @@ __device__ __forceinline__ void stockham_pass(const float2 *__restrict__ in,
     float2 t = twm[e * rootstride];
     w[e] = inverse ? cconj(t) : t;
   }
+  // j / Ns as a multiply-high: magic = ceil(2^32 / Ns) is exact for
+  // j, Ns < 2^16 (the error j * (magic - 2^32/Ns) / 2^32 < 2^-16 <= 1/Ns).
+  const unsigned magic =
+      Ns > 1 ? (unsigned)((0x100000000ull + (unsigned)Ns - 1) / (unsigned)Ns) : 0u;
   for (int j = threadIdx.x; j < nb; j += blockDim.x) {
     float2 v[P];
 #pragma unroll
     for (int r = 0; r < P; ++r) v[r] = in[j + r * nb];
-    const int k = j % Ns;
+    const int jq = Ns > 1 ? (int)__umulhi((unsigned)j, magic) : j;
+    const int k = j - jq * Ns;
     if (Ns > 1) {
+      // k * r * twstride < Ns * P * (m / (Ns * P)) = m: no reduction needed
 #pragma unroll
       for (int r = 1; r < P; ++r) {
-        float2 t = twm[(k * r * twstride) % m];
+        float2 t = twm[k * r * twstride];
         v[r] = cmul(v[r], inverse ? cconj(t) : t);
       }
     }
@@ -76,6 +82,38 @@ __device__ __forceinline__ void stockham_pass(const float2 *__restrict__ in,
       o[2] = csub(a, c);
       o[1] = cadd(b, dm);
       o[3] = csub(b, dm);
+    } else if (P & 1) {
+      // Odd P: pair inputs r and P-r.  With s_r = v_r + v_{P-r},
+      // d_r = v_r - v_{P-r}, C_k = v_0 + sum_r s_r cos(2 pi r k / P) and
+      // S_k = sum_r d_r sin(2 pi r k / P), the forward outputs are
+      // o_k = C_k - i S_k and o_{P-k} = C_k + i S_k (signs swap for the
+      // inverse): a quarter of the real multiplies of the direct sum.
+      constexpr int H = (P - 1) / 2;
+      float2 s[H + 1], d[H + 1];
+      float2 o0 = v[0];
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        s[r] = cadd(v[r], v[P - r]);
+        d[r] = csub(v[r], v[P - r]);
+        o0 = cadd(o0, s[r]);
+      }
+      o[0] = o0;
+#pragma unroll
+      for (int k = 1; k <= H; ++k) {
+        float2 c = v[0], sn = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int r = 1; r <= H; ++r) {
+          const float cs = w[(r * k) % P].x;    // cos(2 pi r k / P)
+          const float sv = -w[(r * k) % P].y;   // sin(2 pi r k / P) (forward table)
+          c.x += s[r].x * cs;
+          c.y += s[r].y * cs;
+          sn.x += d[r].x * sv;
+          sn.y += d[r].y * sv;
+        }
+        // -i*S = (S.y, -S.x); the inverse table is conjugated, which flips sv
+        o[k] = make_float2(c.x + sn.y, c.y - sn.x);
+        o[P - k] = make_float2(c.x - sn.y, c.y + sn.x);
+      }
     } else {
 #pragma unroll
       for (int q = 0; q < P; ++q) {
@@ -89,7 +127,7 @@ __device__ __forceinline__ void stockham_pass(const float2 *__restrict__ in,
         o[q] = acc;
       }
     }
-    const int base = (j / Ns) * Ns * P + k;
+    const int base = jq * Ns * P + k;
 #pragma unroll
     for (int r = 0; r < P; ++r) out[base + r * Ns] = o[r];
   }

@@ -21,7 +21,13 @@
 #include <cuda_fp16.h>
 #include <math.h>
 
+#include <algorithm>
+#include <climits>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cmath>
+#include <cub/cub.cuh>
 #include <vector>
 
 #include "common.cuh"
@@ -40,13 +46,38 @@ struct PhysicsState {
   float *d_comp = nullptr;     // Kahan compensation, [img_cap]
   size_t comp_cap = 0;
   // line tables
-  qpsdm_ttt_desc *d_desc_t = nullptr, *d_desc_q = nullptr;
-  float *d_ttt = nullptr, *d_qqq = nullptr;
-  size_t desc_cap = 0, ttt_cap = 0, qqq_cap = 0;
-  bool have_tables = false;
+  struct LineTab {
+    qpsdm_ttt_desc *dt = nullptr, *dq = nullptr;
+    float *ttt = nullptr, *qqq = nullptr;
+    size_t dt_cap = 0, dq_cap = 0, ttt_cap = 0, qqq_cap = 0;
+  };
+  std::vector<LineTab> tabs;  // one per line of the brick
+  int ntabs = 0;
+  int *d_any = nullptr;       // [max_batch] accepted by any line of the brick
+  // batched form: grouping scratch (sized for max_batch at create)
+  int form = QPSDM_FORM_PLAIN;
+  unsigned long long *d_key[2] = {};  // receiver keys, unsorted / sorted
+  int *d_val[2] = {};                 // trace indices, unsorted / sorted
+  unsigned long long *d_ukey = nullptr;
+  int *d_count = nullptr, *d_off = nullptr, *d_nruns = nullptr;
+  int *d_srcflag = nullptr, *d_sid = nullptr;  // source run flags / ids (1-based)
+  float2 *d_srcpos = nullptr;                  // [max_batch] source positions
+  int4 *d_mem = nullptr;                       // [max_batch] member info
+  int4 *d_grp = nullptr;                       // [max_batch] group records
+  float2 *d_grppos = nullptr;                  // [max_batch] receiver positions
+  int *d_tile_ctr = nullptr;
+  void *d_cub = nullptr;
+  size_t cub_bytes = 0;
+  int num_sms = 0;
+  int tile_z = 0, tile_x = 0, src_chunk = 16;
+  int variant = -1;          // batched kernel variant (autotuned)
+  float *d_tune = nullptr;   // scratch image of the autotuner
+  size_t tune_cap = 0;
+  float tune_ms[16] = {};    // autotuner timings per variant (ms)
 };
 
 static size_t dtype_bytes(int t) { return t == QPSDM_PANEL_FP32 ? 4 : 2; }
+static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p);
 
 // (-i ww_k) * A(pi f t*) * exp(-2 i f t* ln(f/fc)) / nfft for every bin.
 static void filter_table(const qpsdm_static_params &p, int nbins, float dtstar,
@@ -117,20 +148,49 @@ int physics_create(PhysicsState **out, const qpsdm_static_params &p, std::string
   if (cudaMalloc(&s->d_spec, sizeof(float2) * nk * p.max_batch) != cudaSuccess) return bad("spectra");
   const size_t pb = dtype_bytes(p.panel_dtype) * (size_t)p.nbins * p.nffti * p.max_batch;
   if (cudaMalloc(&s->d_panels, pb) != cudaSuccess) return bad("panels");
+  if (cudaMalloc(&s->d_any, sizeof(int) * p.max_batch) != cudaSuccess) return bad("flags");
+  s->form = p.form;
+  if (p.form == QPSDM_FORM_BATCHED) {
+    if (batched_alloc(s, p)) return bad("batched scratch");
+  } else if (p.form != QPSDM_FORM_PLAIN) {
+    if (err) *err = "unknown physics form";
+    physics_destroy(s);
+    return QPSDM_EINVAL;
+  }
   *out = s;
   return QPSDM_OK;
 }
 
 void physics_destroy(PhysicsState *s) {
   if (!s) return;
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(s->d_key[i]);
+    cudaFree(s->d_val[i]);
+  }
+  cudaFree(s->d_ukey);
+  cudaFree(s->d_count);
+  cudaFree(s->d_off);
+  cudaFree(s->d_nruns);
+  cudaFree(s->d_srcflag);
+  cudaFree(s->d_sid);
+  cudaFree(s->d_srcpos);
+  cudaFree(s->d_mem);
+  cudaFree(s->d_grp);
+  cudaFree(s->d_grppos);
+  cudaFree(s->d_tile_ctr);
+  cudaFree(s->d_cub);
   cudaFree(s->d_filter);
   cudaFree(s->d_spec);
   cudaFree(s->d_panels);
   cudaFree(s->d_comp);
-  cudaFree(s->d_desc_t);
-  cudaFree(s->d_desc_q);
-  cudaFree(s->d_ttt);
-  cudaFree(s->d_qqq);
+  for (auto &t : s->tabs) {
+    cudaFree(t.dt);
+    cudaFree(t.dq);
+    cudaFree(t.ttt);
+    cudaFree(t.qqq);
+  }
+  cudaFree(s->d_any);
+  cudaFree(s->d_tune);
   delete s;
 }
 
@@ -145,8 +205,7 @@ static bool grow_dev(T **p, size_t *cap, size_t need) {
   return true;
 }
 
-int physics_set_line(PhysicsState *s, const qpsdm_static_params &p,
-                     const qpsdm_line_params &l, cudaStream_t st, std::string *err) {
+static int check_tables(const qpsdm_line_params &l, std::string *err) {
   if (!l.ttt_desc || !l.qqq_desc || !l.ttt || !l.qqq || l.nxg <= 0 || l.nzg <= 0 ||
       l.nxi1 <= 0 || l.nzi1 <= 0) {
     if (err) *err = "physics mode needs ttt and qqq tables";
@@ -170,33 +229,51 @@ int physics_set_line(PhysicsState *s, const qpsdm_static_params &p,
       }
     }
   }
-  size_t dc = s->desc_cap, dq = s->desc_cap;
-  if (!grow_dev(&s->d_desc_t, &dc, ncell) || !grow_dev(&s->d_desc_q, &dq, ncell) ||
-      !grow_dev(&s->d_ttt, &s->ttt_cap, (size_t)l.ttt_len) ||
-      !grow_dev(&s->d_qqq, &s->qqq_cap, (size_t)l.qqq_len)) {
-    if (err) *err = "table allocation failed";
-    return QPSDM_ENOMEM;
+  return QPSDM_OK;
+}
+
+int physics_set_lines(PhysicsState *s, const qpsdm_static_params &p,
+                      const qpsdm_line_params *lines, int nlines, cudaStream_t st,
+                      std::string *err) {
+  (void)p;
+  for (int il = 0; il < nlines; ++il) {
+    int rc = check_tables(lines[il], err);
+    if (rc) return rc;
   }
-  s->desc_cap = dc < dq ? dc : dq;
-  cudaMemcpyAsync(s->d_desc_t, l.ttt_desc, sizeof(qpsdm_ttt_desc) * ncell,
-                  cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(s->d_desc_q, l.qqq_desc, sizeof(qpsdm_ttt_desc) * ncell,
-                  cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(s->d_ttt, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(s->d_qqq, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyHostToDevice, st);
+  if ((int)s->tabs.size() < nlines) s->tabs.resize(nlines);
+  for (int il = 0; il < nlines; ++il) {
+    const qpsdm_line_params &l = lines[il];
+    PhysicsState::LineTab &t = s->tabs[il];
+    const size_t ncell = (size_t)l.nxg * l.nzg;
+    if (!grow_dev(&t.dt, &t.dt_cap, ncell) || !grow_dev(&t.dq, &t.dq_cap, ncell) ||
+        !grow_dev(&t.ttt, &t.ttt_cap, (size_t)l.ttt_len) ||
+        !grow_dev(&t.qqq, &t.qqq_cap, (size_t)l.qqq_len)) {
+      if (err) *err = "table allocation failed";
+      return QPSDM_ENOMEM;
+    }
+    cudaMemcpyAsync(t.dt, l.ttt_desc, sizeof(qpsdm_ttt_desc) * ncell, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(t.dq, l.qqq_desc, sizeof(qpsdm_ttt_desc) * ncell, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(t.ttt, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(t.qqq, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyHostToDevice, st);
+  }
   if (cudaStreamSynchronize(st) != cudaSuccess) {
     if (err) *err = "table upload failed";
     return QPSDM_ECUDA;
   }
-  s->have_tables = true;
-  (void)p;
+  s->ntabs = nlines;
   return QPSDM_OK;
 }
 
 int physics_begin_offset(PhysicsState *s, const qpsdm_static_params &p,
-                         const qpsdm_offset_params &o, cudaStream_t st, std::string *err) {
+                         const qpsdm_offset_params &o, int nlines, cudaStream_t st,
+                         std::string *err) {
+  if (s->form == QPSDM_FORM_BATCHED && s->variant < 0 &&
+      !grow_dev(&s->d_tune, &s->tune_cap, (size_t)(o.ixend - o.ixstart) * p.nzi)) {
+    if (err) *err = "autotuner scratch allocation failed";
+    return QPSDM_ENOMEM;
+  }
   if (p.kahan) {
-    const size_t n = (size_t)(o.ixend - o.ixstart) * p.nzi;
+    const size_t n = (size_t)(o.ixend - o.ixstart) * p.nzi * nlines;
     if (!grow_dev(&s->d_comp, &s->comp_cap, n)) {
       if (err) *err = "compensation buffer allocation failed";
       return QPSDM_ENOMEM;
@@ -221,11 +298,12 @@ __device__ __forceinline__ float phys_tapered(float v, int j, int n, const float
 }
 
 __global__ void __launch_bounds__(256) k_phys_fwd(const uint8_t *__restrict__ rec, int rec_bytes,
-                                                  int be, const int *__restrict__ ints, int ntl,
+                                                  int be, const int *__restrict__ status,
+                                                  int sstride, int ntl,
                                                   float dt, const float *__restrict__ tap,
                                                   FftPlan p, float2 *__restrict__ spec) {
   const int itr = blockIdx.x;
-  if (ints[(size_t)itr * kGateInts] != kAccepted) return;
+  if (status[(size_t)itr * sstride] != kAccepted) return;
   extern __shared__ float2 sm[];
   float2 *b0 = sm, *b1 = sm + p.m, *twm = sm + 2 * p.m, *twn = sm + 3 * p.m;
   for (int i = threadIdx.x; i < p.m; i += blockDim.x) twm[i] = p.tw_m[i];
@@ -263,12 +341,12 @@ __device__ __forceinline__ void store_sample<__half>(__half *d, float v) { *d = 
 
 // One CTA per (trace, t* bin): filtered, zero-padded spectrum -> c2r nffti.
 template <typename T>
-__global__ void __launch_bounds__(256) k_phys_panels(const int *__restrict__ ints,
+__global__ void __launch_bounds__(256) k_phys_panels(const int *__restrict__ status, int sstride,
                                                      const float2 *__restrict__ spec, int nk,
                                                      const float2 *__restrict__ filt, FftPlan p,
                                                      int nbins, T *__restrict__ panels) {
   const int itr = blockIdx.x, b = blockIdx.y;
-  if (ints[(size_t)itr * kGateInts] != kAccepted) return;
+  if (status[(size_t)itr * sstride] != kAccepted) return;
   extern __shared__ float2 sm[];
   float2 *b0 = sm, *b1 = sm + p.m, *twm = sm + 2 * p.m, *twn = sm + 3 * p.m;
   for (int i = threadIdx.x; i < p.m; i += blockDim.x) twm[i] = p.tw_m[i];
@@ -344,19 +422,101 @@ __device__ __forceinline__ bool table_node(const qpsdm_ttt_desc &d, const float 
 
 struct PointCells {
   bool ok;
+  bool same;  // all four descriptors share one surface grid
   int ixl, izlA, izlB;
+  int cA, cB;          // cells of the two depth nodes
+  int nxs, nys;        // shared surface grid (fast path)
   float c2, xc;
-  qpsdm_ttt_desc tA, tB, qA, qB;
+  float rdx, rdy, hx, hy;  // 1/dxs, 1/dys, (nxs-1)/2, (nys-1)/2 of the shared grid
+  int64_t tA, tB, qA, qB;  // data offsets (idx) of the four blocks
 };
 
-__device__ __forceinline__ bool lookup_tq(const PointCells &pc, const float *__restrict__ ttt,
+__device__ __forceinline__ bool same_grid(const qpsdm_ttt_desc &a, const qpsdm_ttt_desc &b) {
+  return a.nxs == b.nxs && a.nys == b.nys && a.dxs == b.dxs && a.dys == b.dys;
+}
+
+// Cell, depth node and descriptors of image point (ixi, z), src/q-psdm.cu:2343-2349.
+__device__ __forceinline__ void setup_cells(PointCells &pc, int ixi, float z,
+                                            const PhysImageArgs &a,
+                                            const qpsdm_ttt_desc *__restrict__ dt,
+                                            const qpsdm_ttt_desc *__restrict__ dq) {
+  pc.ok = false;
+  pc.same = false;
+  if (ixi < a.tcdp1 || ixi > a.tcdp2) return;
+  const int lx = ixi - a.tcdp1;
+  const int ixg = lx / a.nxi1;
+  pc.ixl = lx - ixg * a.nxi1;
+  const float fz = z / a.dzii;
+  const int izn = (int)fz;
+  pc.c2 = fz - (float)izn;
+  int izgA = izn / a.nzi1, izgB = (izn + 1) / a.nzi1;
+  pc.izlA = izn - izgA * a.nzi1;
+  pc.izlB = izn + 1 - izgB * a.nzi1;
+  if (izgB >= a.nzg) {  // deepest node: no lower neighbour
+    izgB = izgA;
+    pc.izlB = pc.izlA;
+    pc.c2 = 0.0f;
+  }
+  if (ixg >= a.nxg || izgA >= a.nzg) return;
+  pc.ok = true;
+  pc.cA = ixg * a.nzg + izgA;
+  pc.cB = ixg * a.nzg + izgB;
+  const qpsdm_ttt_desc tA = dt[pc.cA], tB = dt[pc.cB], qA = dq[pc.cA], qB = dq[pc.cB];
+  pc.tA = tA.idx;
+  pc.tB = tB.idx;
+  pc.qA = qA.idx;
+  pc.qB = qB.idx;
+  pc.xc = (a.tcdp1 + ixg * a.nxi1 + 0.5f * (a.nxi1 - 1)) * a.dxi;
+  pc.same = same_grid(tA, tB) && same_grid(tA, qA) && same_grid(tA, qB);
+  pc.nxs = tA.nxs;
+  pc.nys = tA.nys;
+  pc.rdx = 1.0f / (float)tA.dxs;
+  pc.rdy = 1.0f / (float)tA.dys;
+  pc.hx = 0.5f * (tA.nxs - 1);
+  pc.hy = 0.5f * (tA.nys - 1);
+}
+
+// Bilinear value of a 2 x 2 node block starting at tab + base.
+__device__ __forceinline__ float bilin(const float *__restrict__ tab, int64_t base, int64_t sx,
+                                       int64_t sy, float wx, float wy) {
+  const float v00 = __ldg(tab + base), v01 = __ldg(tab + base + sx);
+  const float v10 = __ldg(tab + base + sy), v11 = __ldg(tab + base + sy + sx);
+  const float a = v00 + wx * (v01 - v00), b = v10 + wx * (v11 - v10);
+  return a + wy * (b - a);
+}
+
+__device__ __forceinline__ bool lookup_tq(const PointCells &pc,
+                                          const qpsdm_ttt_desc *__restrict__ dt,
+                                          const float *__restrict__ ttt,
+                                          const qpsdm_ttt_desc *__restrict__ dq,
                                           const float *__restrict__ qqq, int nxi1, int nzi1,
                                           float px, float py, float &t, float &q) {
+  if (pc.same) {  // one set of surface weights for t and t*, both depth nodes
+    const int nxs = pc.nxs, nys = pc.nys;
+    const float fx = (px - pc.xc) * pc.rdx + pc.hx;
+    const float fy = py * pc.rdy + pc.hy;
+    if (!(fx >= 0.0f && fx <= (float)(nxs - 1) && fy >= 0.0f && fy <= (float)(nys - 1)))
+      return false;
+    const int ix = min((int)fx, max(nxs - 2, 0));
+    const int iy = min((int)fy, max(nys - 2, 0));
+    const float wx = nxs > 1 ? fx - ix : 0.0f, wy = nys > 1 ? fy - iy : 0.0f;
+    const int64_t plane = (int64_t)nxi1 * nzi1;
+    const int64_t sx = nxs > 1 ? plane : 0, sy = nys > 1 ? (int64_t)nxs * plane : 0;
+    const int64_t off = (int64_t)(iy * nxs + ix) * plane + (int64_t)pc.ixl * nzi1;
+    const float ta = bilin(ttt, pc.tA + off + pc.izlA, sx, sy, wx, wy);
+    const float tb = bilin(ttt, pc.tB + off + pc.izlB, sx, sy, wx, wy);
+    const float qa = bilin(qqq, pc.qA + off + pc.izlA, sx, sy, wx, wy);
+    const float qb = bilin(qqq, pc.qB + off + pc.izlB, sx, sy, wx, wy);
+    t = ta + pc.c2 * (tb - ta);
+    q = qa + pc.c2 * (qb - qa);
+    return true;
+  }
+  // cells with different surface grids: one lookup per descriptor
   float ta, tb, qa, qb;
-  if (!table_node(pc.tA, ttt, px, py, pc.xc, pc.ixl, pc.izlA, nxi1, nzi1, ta)) return false;
-  if (!table_node(pc.tB, ttt, px, py, pc.xc, pc.ixl, pc.izlB, nxi1, nzi1, tb)) return false;
-  if (!table_node(pc.qA, qqq, px, py, pc.xc, pc.ixl, pc.izlA, nxi1, nzi1, qa)) return false;
-  if (!table_node(pc.qB, qqq, px, py, pc.xc, pc.ixl, pc.izlB, nxi1, nzi1, qb)) return false;
+  if (!table_node(dt[pc.cA], ttt, px, py, pc.xc, pc.ixl, pc.izlA, nxi1, nzi1, ta)) return false;
+  if (!table_node(dt[pc.cB], ttt, px, py, pc.xc, pc.ixl, pc.izlB, nxi1, nzi1, tb)) return false;
+  if (!table_node(dq[pc.cA], qqq, px, py, pc.xc, pc.ixl, pc.izlA, nxi1, nzi1, qa)) return false;
+  if (!table_node(dq[pc.cB], qqq, px, py, pc.xc, pc.ixl, pc.izlB, nxi1, nzi1, qb)) return false;
   t = ta + pc.c2 * (tb - ta);
   q = qa + pc.c2 * (qb - qa);
   return true;
@@ -395,30 +555,7 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
     tany2 = dips[3 * a.nxz + k];
     acc = img[(size_t)ixb * a.nzi + izi];
     if (comp) cmp = comp[(size_t)ixb * a.nzi + izi];
-    const int lx = ixi - a.tcdp1;
-    if (ixi >= a.tcdp1 && ixi <= a.tcdp2) {
-      const int ixg = lx / a.nxi1;
-      pc.ixl = lx - ixg * a.nxi1;
-      const float fz = z / a.dzii;
-      const int izn = (int)fz;
-      pc.c2 = fz - (float)izn;
-      int izgA = izn / a.nzi1, izgB = (izn + 1) / a.nzi1;
-      pc.izlA = izn - izgA * a.nzi1;
-      pc.izlB = izn + 1 - izgB * a.nzi1;
-      if (izgB >= a.nzg) {  // deepest node: no lower neighbour
-        izgB = izgA;
-        pc.izlB = pc.izlA;
-        pc.c2 = 0.0f;
-      }
-      if (ixg < a.nxg && izgA < a.nzg) {
-        pc.ok = true;
-        pc.tA = dt[ixg * a.nzg + izgA];
-        pc.tB = dt[ixg * a.nzg + izgB];
-        pc.qA = dq[ixg * a.nzg + izgA];
-        pc.qB = dq[ixg * a.nzg + izgB];
-        pc.xc = (a.tcdp1 + ixg * a.nxi1 + 0.5f * (a.nxi1 - 1)) * a.dxi;
-      }
-    }
+    setup_cells(pc, ixi, z, a, dt, dq);
   }
   const float tz = a.taperzone;
   const float tanx1c = tanx1 - tz * (1.0f + tanx1 * tanx1);
@@ -453,11 +590,11 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
       if (gm.x != last_sx || gm.y != last_sy) {
         last_sx = gm.x;
         last_sy = gm.y;
-        s_ok = lookup_tq(pc, ttt, qqq, a.nxi1, a.nzi1, gm.x, gm.y, ts, qs);
+        s_ok = lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, gm.x, gm.y, ts, qs);
       }
       if (!s_ok) continue;
       float tg, qg;
-      if (!lookup_tq(pc, ttt, qqq, a.nxi1, a.nzi1, gm.z, gm.w, tg, qg)) continue;
+      if (!lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, gm.z, gm.w, tg, qg)) continue;
       // ray directions and dip taper (src/q-psdm.cu:2303-2340)
       const float dsx = gm.x - x, dgx = gm.z - x;
       const float ds = sqrtf(dsx * dsx + gm.y * gm.y + z2);
@@ -511,48 +648,504 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
   }
 }
 
-int physics_process(PhysicsState *s, const qpsdm_static_params &p,
-                    const qpsdm_line_params &l, const qpsdm_offset_params &o,
-                    const PhysicsBatch &b, cudaStream_t st, std::string *err) {
-  if (!s->have_tables) {
-    if (err) *err = "physics mode: set_line without tables";
-    return QPSDM_ESTATE;
+// ---------------------------------------------------------------------------
+// batched form
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kNoKey = ~0ull;
+
+// Receiver keys (accepted traces; position bits of the gate's relative
+// coordinates), trace indices, and source-run flags from the raw headers.
+__global__ void k_batch_keys(const uint8_t *__restrict__ rec, int rec_bytes, int be, int ntr,
+                             const int *__restrict__ ints, const float *__restrict__ geom,
+                             unsigned long long *__restrict__ key, int *__restrict__ val,
+                             int *__restrict__ srcflag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ntr) return;
+  const uint8_t *r = rec + (size_t)i * rec_bytes;
+  int flag = 1;
+  if (i > 0) {
+    const uint8_t *q = r - rec_bytes;
+    flag = su_i32(r, kOffSx, be) != su_i32(q, kOffSx, be) ||
+           su_i32(r, kOffSy, be) != su_i32(q, kOffSy, be);
   }
-  const int ntr = b.ntr;
-  // 1. forward spectra
+  srcflag[i] = flag;
+  const bool ok = ints[(size_t)i * kGateInts] == kAccepted;
+  const float gx = geom[(size_t)i * kGateF + 2], gy = geom[(size_t)i * kGateF + 3];
+  key[i] = ok ? ((unsigned long long)__float_as_uint(gy) << 32) | __float_as_uint(gx) : kNoKey;
+  val[i] = i;
+}
+
+// Group records: [2g] = (first sorted position, end, min ixi1, max ixi2),
+// [2g+1] = (min source, max source); receiver position per group.
+__global__ void k_batch_groups(const unsigned long long *__restrict__ ukey,
+                               const int *__restrict__ count, const int *__restrict__ off,
+                               const int *__restrict__ nruns, const int *__restrict__ sval,
+                               const int *__restrict__ ints, const int *__restrict__ sid,
+                               int4 *__restrict__ grp, float2 *__restrict__ grppos, int ntr) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ntr || g >= *nruns) return;
+  const unsigned long long k = ukey[g];
+  const int start = off[g], n = count[g];
+  if (k == kNoKey) {
+    grp[2 * g] = make_int4(start, start, 1, 0);
+    grp[2 * g + 1] = make_int4(1, 0, 0, 0);
+    return;
+  }
+  int c0 = INT_MAX, c1 = INT_MIN, s0 = INT_MAX, s1 = INT_MIN;
+  for (int p = start; p < start + n; ++p) {
+    const int j = sval[p];
+    c0 = min(c0, ints[(size_t)j * kGateInts + 4]);
+    c1 = max(c1, ints[(size_t)j * kGateInts + 5]);
+    const int sj = sid[j] - 1;
+    s0 = min(s0, sj);
+    s1 = max(s1, sj);
+  }
+  grp[2 * g] = make_int4(start, start + n, c0, c1);
+  grp[2 * g + 1] = make_int4(s0, s1, 0, 0);
+  grppos[g] = make_float2(__uint_as_float((unsigned)(k & 0xffffffffu)),
+                          __uint_as_float((unsigned)(k >> 32)));
+}
+
+// Member info per sorted position (trace, source, column range) and the
+// position of every source run (the gate's double-precision arithmetic).
+__global__ void k_batch_members(const uint8_t *__restrict__ rec, int rec_bytes, int be, int ntr,
+                                const int *__restrict__ sval, const int *__restrict__ ints,
+                                const int *__restrict__ sid, const int *__restrict__ srcflag,
+                                double scaled, double fxi, double cyi, int4 *__restrict__ mem,
+                                float2 *__restrict__ srcpos) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ntr) return;
+  const int j = sval[p];
+  const int *q = ints + (size_t)j * kGateInts;
+  mem[p] = q[0] == kAccepted ? make_int4(j, sid[j] - 1, q[4], q[5]) : make_int4(j, -1, 1, 0);
+  if (srcflag[p]) {  // p as a trace index: first trace of a source run
+    const uint8_t *r = rec + (size_t)p * rec_bytes;
+    const double sx = __dmul_rn((double)su_i32(r, kOffSx, be), scaled);
+    const double sy = __dmul_rn((double)su_i32(r, kOffSy, be), scaled);
+    srcpos[sid[p] - 1] = make_float2(__double2float_rn(__dsub_rn(sx, fxi)),
+                                     __double2float_rn(__dsub_rn(sy, cyi)));
+  }
+}
+
+// Source terms kept per (source, point) in shared memory.
+enum { kMapT = 0, kMapQ, kMapCS, kMapAX, kMapAY, kMapAZ, kMapN };
+
+template <int TZ, int TX, int MB, typename T>
+__global__ void __launch_bounds__(TZ *TX, MB)
+    k_image_batched(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
+                    const float *__restrict__ dips, const int4 *__restrict__ grp,
+                    const float2 *__restrict__ grppos, const int *__restrict__ nruns,
+                    const int4 *__restrict__ mem, const float2 *__restrict__ srcpos,
+                    const int *__restrict__ nsrc_ptr, const qpsdm_ttt_desc *__restrict__ dt,
+                    const float *__restrict__ ttt, const qpsdm_ttt_desc *__restrict__ dq,
+                    const float *__restrict__ qqq, const T *__restrict__ panels,
+                    int *__restrict__ tile_ctr, int ntz, int ntx, int sc,
+                    unsigned long long *npt) {
+  constexpr int NT = TZ * TX;
+  extern __shared__ float smap[];  // [kMapN][sc][NT]
+  __shared__ int s_tile;
+  __shared__ unsigned long long s_cnt;
+  const int tid = threadIdx.x;
+  const int lz = tid % TZ, lx = tid / TZ;
+  const int ngroups = *nruns, nsrc = *nsrc_ptr;
+  const float inv_dt1 = 1.0f / a.dt1, inv_dts = 1.0f / a.dtstar;
+  const size_t pstride = (size_t)a.nbins * a.nt;
+  if (tid == 0) s_cnt = 0;
+  unsigned cnt = 0;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1);
+    __syncthreads();
+    const int tile = s_tile;
+    if (tile >= ntz * ntx) break;
+    const int izi = (tile % ntz) * TZ + lz;
+    const int ixb = (tile / ntz) * TX + lx;
+    const bool live = izi < a.nzi && ixb < a.nxb;
+    const int ixi = ixb + a.ixstart;
+    PointCells pc;
+    pc.ok = false;
+    float tanx1 = 0.f, tanx2 = 0.f, tany1 = 0.f, tany2 = 0.f, acc = 0.f, cmp = 0.f;
+    const float z = izi * a.dzi;
+    if (live) {
+      const size_t k = (size_t)ixi * a.nzi + izi;
+      tanx1 = dips[k];
+      tanx2 = dips[a.nxz + k];
+      tany1 = dips[2 * a.nxz + k];
+      tany2 = dips[3 * a.nxz + k];
+      acc = img[(size_t)ixb * a.nzi + izi];
+      if (comp) cmp = comp[(size_t)ixb * a.nzi + izi];
+      setup_cells(pc, ixi, z, a, dt, dq);
+    }
+    const bool act = live && pc.ok;
+    const float tz = a.taperzone;
+    const float tanx1c = tanx1 - tz * (1.0f + tanx1 * tanx1);
+    const float tanx2c = tanx2 + tz * (1.0f + tanx2 * tanx2);
+    const float tany1c = tany1 - tz * (1.0f + tany1 * tany1);
+    const float tany2c = tany2 + tz * (1.0f + tany2 * tany2);
+    const float z2 = z * z;
+    const float x = ixi * a.dxi;
+
+    for (int s0 = 0; s0 < nsrc && act; s0 += sc) {
+      const int ns = min(sc, nsrc - s0);
+      // source terms of this chunk for this thread's point
+      for (int s = 0; s < ns; ++s) {
+        const float2 sp = srcpos[s0 + s];
+        float ts, qs;
+        float *m = smap + (size_t)s * NT + tid;
+        if (!lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, sp.x, sp.y, ts, qs)) {
+          m[kMapT * sc * NT] = NAN;
+          continue;
+        }
+        const float dsx = sp.x - x;
+        const float ds = sqrtf(dsx * dsx + sp.y * sp.y + z2);
+        const float rds = __fdividef(1.0f, ds);
+        m[kMapT * sc * NT] = ts;
+        m[kMapQ * sc * NT] = qs;
+        m[kMapCS * sc * NT] = __fdividef(ds * ds * ds, ts);  // source factor of (ds/dg)^3 tg/ts
+        m[kMapAX * sc * NT] = dsx * rds;
+        m[kMapAY * sc * NT] = sp.y * rds;
+        m[kMapAZ * sc * NT] = z * rds;
+      }
+      for (int g = 0; g < ngroups; ++g) {
+        const int4 gr = __ldg(grp + 2 * g);
+        if (gr.x >= gr.y || ixi < gr.z || ixi > gr.w) continue;
+        const int4 gs = __ldg(grp + 2 * g + 1);
+        if (gs.y < s0 || gs.x >= s0 + ns) continue;
+        // receiver terms, once per receiver position
+        const float2 gp = __ldg(grppos + g);
+        float tg, qg;
+        const bool rok = lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
+        const float dgx = gp.x - x;
+        const float dg = sqrtf(dgx * dgx + gp.y * gp.y + z2);
+        const float rdg = __fdividef(1.0f, dg);
+        const float agx = dgx * rdg, agy = gp.y * rdg, agz = z * rdg;
+        const float gfac = tg * rdg * rdg * rdg;  // receiver factor of (ds/dg)^3 tg/ts
+        // Members in blocks of U: first every member's time/t* pick and
+        // weight, then all panel gathers, then the sums (in member order), so
+        // that U members' loads are in flight together.
+        constexpr int U = 4;
+        for (int p0 = gr.x; p0 < gr.y; p0 += U) {
+          const T *pp[U];
+          float fwt[U], fwb[U], fac[U];
+          bool on[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            on[u] = false;
+            pp[u] = panels;
+            fwt[u] = fwb[u] = fac[u] = 0.0f;
+            const int p = p0 + u;
+            if (p >= gr.y) continue;
+            const int4 mi = __ldg(mem + p);
+            const int sl = mi.y - s0;
+            if (sl < 0 || sl >= ns || ixi < mi.z || ixi > mi.w) continue;
+            ++cnt;
+            if (!rok) continue;
+            const float *m = smap + (size_t)sl * NT + tid;
+            const float ts = m[kMapT * sc * NT];
+            if (isnan(ts)) continue;
+            const float ux = m[kMapAX * sc * NT] + agx;
+            const float uy = m[kMapAY * sc * NT] + agy;
+            const float uz = m[kMapAZ * sc * NT] + agz;
+            const float ruz = __fdividef(1.0f, uz);
+            const float tanx = ux * ruz, tany = uy * ruz;
+            if (!(tanx > tanx1c && tanx < tanx2c && tany > tany1c && tany < tany2c)) continue;
+            float w = 1.0f;
+            if (tanx < tanx1) w *= (tanx - tanx1c) / (tanx1 - tanx1c);
+            if (tanx > tanx2) w *= (tanx2c - tanx) / (tanx2c - tanx2);
+            if (tany < tany1) w *= (tany - tany1c) / (tany1 - tany1c);
+            if (tany > tany2) w *= (tany2c - tany) / (tany2c - tany2);
+            const float t = ts + tg;
+            const float ft = t * inv_dt1;
+            const int it1 = (int)ft;
+            if (!(it1 > 0 && it1 + 1 < a.nt)) continue;
+            const float fb =
+                fminf(fmaxf((m[kMapQ * sc * NT] + qg) * inv_dts, 0.0f), (float)(a.nbins - 1));
+            const int b0 = min((int)fb, a.nbins - 2);
+            fwt[u] = ft - (float)it1;
+            fwb[u] = fb - (float)b0;
+            pp[u] = panels + (size_t)mi.x * pstride + (size_t)b0 * a.nt + it1;
+            const float v = t > 0.1f ? __fdividef(100.0f, t * t) : 10000.0f;
+            const float r = m[kMapCS * sc * NT] * gfac;
+            fac[u] = w * (r + __fdividef(1.0f, r)) * v;
+            on[u] = true;
+          }
+          float smp[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            smp[u] = 0.0f;
+            if (on[u]) {
+              const T *q = pp[u];
+              const float p00 = ld_sample<T>(q), p01 = ld_sample<T>(q + 1);
+              const float p10 = ld_sample<T>(q + a.nt), p11 = ld_sample<T>(q + a.nt + 1);
+              const float s0v = p00 + fwt[u] * (p01 - p00), s1v = p10 + fwt[u] * (p11 - p10);
+              smp[u] = s0v + fwb[u] * (s1v - s0v);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (!on[u]) continue;
+            const float val = fac[u] * smp[u];
+            if (comp) {
+              const float y = val - cmp;
+              const float tt = acc + y;
+              cmp = (tt - acc) - y;
+              acc = tt;
+            } else {
+              acc += val;
+            }
+          }
+        }
+      }
+    }
+    if (live) {
+      img[(size_t)ixb * a.nzi + izi] = acc;
+      if (comp) comp[(size_t)ixb * a.nzi + izi] = cmp;
+    }
+  }
+  if (npt) {
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    if ((tid & 31) == 0 && cnt) atomicAdd(&s_cnt, (unsigned long long)cnt);
+    __syncthreads();
+    if (tid == 0 && s_cnt) atomicAdd(npt, s_cnt);
+  }
+}
+
+static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p) {
+  const int n = p.max_batch;
+  bool ok = true;
+  for (int i = 0; i < 2; ++i) {
+    ok &= cudaMalloc(&s->d_key[i], sizeof(unsigned long long) * n) == cudaSuccess;
+    ok &= cudaMalloc(&s->d_val[i], sizeof(int) * n) == cudaSuccess;
+  }
+  ok &= cudaMalloc(&s->d_ukey, sizeof(unsigned long long) * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_count, sizeof(int) * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_off, sizeof(int) * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_nruns, sizeof(int)) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_srcflag, sizeof(int) * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_sid, sizeof(int) * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_srcpos, sizeof(float2) * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_mem, sizeof(int4) * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_grp, sizeof(int4) * 2 * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_grppos, sizeof(float2) * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_tile_ctr, sizeof(int)) == cudaSuccess;
+  if (!ok) return QPSDM_ENOMEM;
+  size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, b1, s->d_key[0], s->d_key[1], s->d_val[0],
+                                  s->d_val[1], n);
+  cub::DeviceRunLengthEncode::Encode(nullptr, b2, s->d_key[1], s->d_ukey, s->d_count,
+                                     s->d_nruns, n);
+  cub::DeviceScan::ExclusiveSum(nullptr, b3, s->d_count, s->d_off, n);
+  cub::DeviceScan::InclusiveSum(nullptr, b4, s->d_srcflag, s->d_sid, n);
+  s->cub_bytes = std::max(std::max(b1, b2), std::max(b3, b4));
+  if (cudaMalloc(&s->d_cub, s->cub_bytes) != cudaSuccess) return QPSDM_ENOMEM;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (p.tile_z > 0) s->tile_z = p.tile_z;
+  if (p.tile_x > 0) s->tile_x = p.tile_x;
+  return QPSDM_OK;
+}
+
+// One line of the brick as the image kernels see it.
+struct LineView {
+  const int *ints;
+  const float *geom;
+  const float *dips;
+  float *img;
+  float *comp;
+  const PhysicsState::LineTab *tab;
+  const qpsdm_line_params *l;
+};
+
+// Launch variants of the batched kernel: image tile (depth x cdps, one
+// thread per point, a warp along depth) and the minimum resident blocks per SM
+// the register allocation is held to.  The autotuner times them all on the
+// first batch and keeps the fastest.
+struct BatchedVariant {
+  int tz, tx, mb;
+};
+static const BatchedVariant kVariants[] = {
+    {32, 8, 2}, {32, 8, 3}, {32, 4, 4}, {32, 4, 6}, {64, 4, 2}, {64, 4, 3}, {128, 2, 2},
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+template <int TZ, int TX, int MB, typename T>
+static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
+                               const LineView &v, float *img, float *comp,
+                               unsigned long long *npt, cudaStream_t st) {
+  const int ntz = (a.nzi + TZ - 1) / TZ, ntx = (a.nxb + TX - 1) / TX;
+  const size_t smem = sizeof(float) * kMapN * (size_t)s->src_chunk * TZ * TX;
+  auto kern = k_image_batched<TZ, TX, MB, T>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return QPSDM_ECUDA;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TZ * TX, smem);
+  const int grid = std::max(1, std::min(ntz * ntx, std::max(per_sm, 1) * s->num_sms));
+  cudaMemsetAsync(s->d_tile_ctr, 0, sizeof(int), st);
+  kern<<<grid, TZ * TX, smem, st>>>(img, comp, a, v.dips, s->d_grp, s->d_grppos, s->d_nruns,
+                                    s->d_mem, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
+                                    v.tab->ttt, v.tab->dq, v.tab->qqq, (const T *)s->d_panels,
+                                    s->d_tile_ctr, ntz, ntx, s->src_chunk, npt);
+  return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
+}
+
+template <typename T>
+static int launch_variant(int vi, PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
+                          const LineView &v, float *img, float *comp, unsigned long long *npt,
+                          cudaStream_t st) {
+  switch (vi) {
+    case 0: return launch_batched_tile<32, 8, 2, T>(s, a, b, v, img, comp, npt, st);
+    case 1: return launch_batched_tile<32, 8, 3, T>(s, a, b, v, img, comp, npt, st);
+    case 2: return launch_batched_tile<32, 4, 4, T>(s, a, b, v, img, comp, npt, st);
+    case 3: return launch_batched_tile<32, 4, 6, T>(s, a, b, v, img, comp, npt, st);
+    case 4: return launch_batched_tile<64, 4, 2, T>(s, a, b, v, img, comp, npt, st);
+    case 5: return launch_batched_tile<64, 4, 3, T>(s, a, b, v, img, comp, npt, st);
+    default: return launch_batched_tile<128, 2, 2, T>(s, a, b, v, img, comp, npt, st);
+  }
+}
+
+// Tuning results shared by the engines of a process:
+// (device, nzi, nxb, dtype, nbins) -> variant.
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int, int, int>, int> g_tune;
+
+// Picks the variant for this image shape: an explicit tile from the static
+// parameters, a cached result, or a timing of every variant on this batch
+// into a scratch image (synchronous; happens on the first batch only).
+template <typename T>
+static int choose_variant(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
+                          const LineView &v, cudaStream_t st) {
+  if (s->variant >= 0) return s->variant;
+  if (s->tile_z > 0 && s->tile_x > 0) {
+    for (int i = 0; i < kNumVariants; ++i)
+      if (kVariants[i].tz == s->tile_z && kVariants[i].tx == s->tile_x) return s->variant = i;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, a.nzi, a.nxb, s->dtype, s->nbins);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return s->variant = it->second;
+  }
+  float *scratch = s->d_tune;
+  const size_t n = (size_t)a.nxb * a.nzi;
+  if (!scratch || s->tune_cap < n) return s->variant = 2;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = 2;
+  float best_ms = 1e30f;
+  for (int i = 0; i < kNumVariants; ++i) {
+    cudaMemsetAsync(scratch, 0, sizeof(float) * n, st);
+    cudaEventRecord(e0, st);
+    const int rc = launch_variant<T>(i, s, a, b, v, scratch, nullptr, nullptr, st);
+    cudaEventRecord(e1, st);
+    if (rc || cudaEventSynchronize(e1) != cudaSuccess) continue;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    s->tune_ms[i] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+  return s->variant = best;
+}
+
+template <typename T>
+static int launch_batched_image(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
+                                const LineView &v, cudaStream_t st) {
+  const int vi = choose_variant<T>(s, a, b, v, st);
+  return launch_variant<T>(vi, s, a, b, v, v.img, v.comp, b.d_npt, st);
+}
+
+// Grouping of one batch (all on the stream, nothing read back).
+static int batched_group(PhysicsState *s, const qpsdm_static_params &p, const LineView &v,
+                         const PhysicsBatch &b, cudaStream_t st) {
+  const qpsdm_line_params &l = *v.l;
+  const int n = b.ntr, blk = 256, grd = (n + blk - 1) / blk;
+  k_batch_keys<<<grd, blk, 0, st>>>(b.d_rec, b.rec_bytes, b.big_endian, n, v.ints, v.geom,
+                                    s->d_key[0], s->d_val[0], s->d_srcflag);
+  size_t tb = s->cub_bytes;
+  if (cub::DeviceScan::InclusiveSum(s->d_cub, tb, s->d_srcflag, s->d_sid, n, st) != cudaSuccess)
+    return QPSDM_ECUDA;
+  tb = s->cub_bytes;
+  if (cub::DeviceRadixSort::SortPairs(s->d_cub, tb, s->d_key[0], s->d_key[1], s->d_val[0],
+                                      s->d_val[1], n, 0, 64, st) != cudaSuccess)
+    return QPSDM_ECUDA;
+  cudaMemsetAsync(s->d_count, 0, sizeof(int) * n, st);
+  tb = s->cub_bytes;
+  if (cub::DeviceRunLengthEncode::Encode(s->d_cub, tb, s->d_key[1], s->d_ukey, s->d_count,
+                                         s->d_nruns, n, st) != cudaSuccess)
+    return QPSDM_ECUDA;
+  tb = s->cub_bytes;
+  if (cub::DeviceScan::ExclusiveSum(s->d_cub, tb, s->d_count, s->d_off, n, st) != cudaSuccess)
+    return QPSDM_ECUDA;
+  k_batch_groups<<<grd, blk, 0, st>>>(s->d_ukey, s->d_count, s->d_off, s->d_nruns, s->d_val[1],
+                                      v.ints, s->d_sid, s->d_grp, s->d_grppos, n);
+  k_batch_members<<<grd, blk, 0, st>>>(b.d_rec, b.rec_bytes, b.big_endian, n, s->d_val[1],
+                                       v.ints, s->d_sid, s->d_srcflag, p.scaled, l.fxi, l.cyi,
+                                       s->d_mem, s->d_srcpos);
+  return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
+}
+
+// Any line of the brick accepted the trace: its panels are needed.
+__global__ void k_any_line(const int *__restrict__ ints, size_t ints_ls, int nlines, int ntr,
+                           int *__restrict__ any) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ntr) return;
+  int a = 0;
+  for (int il = 0; il < nlines; ++il)
+    a |= ints[il * ints_ls + (size_t)i * kGateInts] == kAccepted;
+  any[i] = a ? kAccepted : 0;
+}
+
+// Forward spectra and t*-binned panels of the traces whose status is kAccepted.
+static int run_panels(PhysicsState *s, const qpsdm_static_params &p, const PhysicsBatch &b,
+                      const int *status, int sstride, cudaStream_t st, std::string *err) {
   FftPlan pf, pi;
   int rc = fft_plan(p.nfft, &pf, err);
   if (rc) return rc;
   rc = fft_plan(p.nffti, &pi, err);
   if (rc) return rc;
+  const int ntr = b.ntr;
   size_t sm = fft_smem_bytes(pf.m);
   if ((rc = fft_set_smem_attr((const void *)k_phys_fwd, sm))) return rc;
-  b.prof->begin(QPSDM_K_PRE, st);
-  k_phys_fwd<<<ntr, 256, sm, st>>>(b.d_rec, b.rec_bytes, b.big_endian, b.d_ints, p.ntl, p.dt,
-                                   b.d_taper200, pf, s->d_spec);
-  // 2. t*-binned panels
+  k_phys_fwd<<<ntr, 256, sm, st>>>(b.d_rec, b.rec_bytes, b.big_endian, status, sstride, p.ntl,
+                                   p.dt, b.d_taper200, pf, s->d_spec);
   const int nk = p.nfft / 2 + 1;
   sm = fft_smem_bytes(pi.m);
   dim3 gp(ntr, s->nbins);
   switch (s->dtype) {
     case QPSDM_PANEL_FP32:
       if ((rc = fft_set_smem_attr((const void *)k_phys_panels<float>, sm))) return rc;
-      k_phys_panels<float><<<gp, 256, sm, st>>>(b.d_ints, s->d_spec, nk, s->d_filter, pi,
+      k_phys_panels<float><<<gp, 256, sm, st>>>(status, sstride, s->d_spec, nk, s->d_filter, pi,
                                                 s->nbins, (float *)s->d_panels);
       break;
     case QPSDM_PANEL_BF16:
       if ((rc = fft_set_smem_attr((const void *)k_phys_panels<__nv_bfloat16>, sm))) return rc;
-      k_phys_panels<__nv_bfloat16><<<gp, 256, sm, st>>>(b.d_ints, s->d_spec, nk, s->d_filter,
-                                                        pi, s->nbins,
+      k_phys_panels<__nv_bfloat16><<<gp, 256, sm, st>>>(status, sstride, s->d_spec, nk,
+                                                        s->d_filter, pi, s->nbins,
                                                         (__nv_bfloat16 *)s->d_panels);
       break;
     default:
       if ((rc = fft_set_smem_attr((const void *)k_phys_panels<__half>, sm))) return rc;
-      k_phys_panels<__half><<<gp, 256, sm, st>>>(b.d_ints, s->d_spec, nk, s->d_filter, pi,
-                                                 s->nbins, (__half *)s->d_panels);
+      k_phys_panels<__half><<<gp, 256, sm, st>>>(status, sstride, s->d_spec, nk, s->d_filter,
+                                                 pi, s->nbins, (__half *)s->d_panels);
   }
-  b.prof->end(st);
-  // 3. image
+  return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
+}
+
+static PhysImageArgs image_args(const PhysicsState *s, const qpsdm_static_params &p,
+                                const qpsdm_line_params &l, const qpsdm_offset_params &o,
+                                size_t nxz) {
   PhysImageArgs a{};
   a.nzi = p.nzi;
   a.nxb = o.ixend - o.ixstart;
@@ -571,34 +1164,105 @@ int physics_process(PhysicsState *s, const qpsdm_static_params &p,
   a.nzg = l.nzg;
   a.nxi1 = l.nxi1;
   a.nzi1 = l.nzi1;
-  a.nxz = b.nxz;
-  float *comp = p.kahan ? s->d_comp : nullptr;
+  a.nxz = nxz;
+  return a;
+}
+
+template <typename T>
+static void launch_plain(const PhysImageArgs &a, const PhysicsBatch &b, const LineView &v,
+                         const T *panels, cudaStream_t st) {
   dim3 block(kPhysBz, kPhysBx);
   dim3 grid((a.nzi + kPhysBz - 1) / kPhysBz, (a.nxb + kPhysBx - 1) / kPhysBx);
-  b.prof->begin(QPSDM_K_IMAGE, st);
-  switch (s->dtype) {
-    case QPSDM_PANEL_FP32:
-      k_image_plain<float><<<grid, block, 0, st>>>(b.d_img, comp, a, b.d_dips, b.d_ints,
-                                                   b.d_geom, ntr, s->d_desc_t, s->d_ttt,
-                                                   s->d_desc_q, s->d_qqq,
-                                                   (const float *)s->d_panels, b.d_npt);
-      break;
-    case QPSDM_PANEL_BF16:
-      k_image_plain<__nv_bfloat16><<<grid, block, 0, st>>>(
-          b.d_img, comp, a, b.d_dips, b.d_ints, b.d_geom, ntr, s->d_desc_t, s->d_ttt,
-          s->d_desc_q, s->d_qqq, (const __nv_bfloat16 *)s->d_panels, b.d_npt);
-      break;
-    default:
-      k_image_plain<__half><<<grid, block, 0, st>>>(
-          b.d_img, comp, a, b.d_dips, b.d_ints, b.d_geom, ntr, s->d_desc_t, s->d_ttt,
-          s->d_desc_q, s->d_qqq, (const __half *)s->d_panels, b.d_npt);
+  k_image_plain<T><<<grid, block, 0, st>>>(v.img, v.comp, a, v.dips, v.ints, v.geom, b.ntr,
+                                           v.tab->dt, v.tab->ttt, v.tab->dq, v.tab->qqq,
+                                           panels, b.d_npt);
+}
+
+int physics_process(PhysicsState *s, const qpsdm_static_params &p,
+                    const qpsdm_line_params *lines, const qpsdm_offset_params &o,
+                    const PhysicsBatch &b, cudaStream_t st, std::string *err) {
+  if (s->ntabs < b.nlines) {
+    if (err) *err = "physics mode: set_line without tables";
+    return QPSDM_ESTATE;
   }
+  const size_t nimg = (size_t)(o.ixend - o.ixstart) * p.nzi;
+  auto view = [&](int il) {
+    LineView v;
+    v.ints = b.d_ints + il * b.ints_ls;
+    v.geom = b.d_geom + il * b.geom_ls;
+    v.dips = b.d_dips + (size_t)il * 4 * b.nxz;
+    v.img = b.d_img + il * b.img_ls;
+    v.comp = p.kahan ? s->d_comp + il * nimg : nullptr;
+    v.tab = &s->tabs[il];
+    v.l = &lines[il];
+    return v;
+  };
+  int rc = QPSDM_OK;
+  if (s->form == QPSDM_FORM_PLAIN) {
+    // as the reference: each line preprocesses its accepted traces again
+    for (int il = 0; il < b.nlines && !rc; ++il) {
+      const LineView v = view(il);
+      b.prof->begin(QPSDM_K_PRE, st);
+      rc = run_panels(s, p, b, v.ints, kGateInts, st, err);
+      b.prof->end(st);
+      if (rc) break;
+      const PhysImageArgs a = image_args(s, p, lines[il], o, b.nxz);
+      b.prof->begin(QPSDM_K_IMAGE, st);
+      if (s->dtype == QPSDM_PANEL_FP32)
+        launch_plain<float>(a, b, v, (const float *)s->d_panels, st);
+      else if (s->dtype == QPSDM_PANEL_BF16)
+        launch_plain<__nv_bfloat16>(a, b, v, (const __nv_bfloat16 *)s->d_panels, st);
+      else
+        launch_plain<__half>(a, b, v, (const __half *)s->d_panels, st);
+      b.prof->end(st);
+      if (cudaGetLastError() != cudaSuccess) rc = QPSDM_ECUDA;
+    }
+    if (rc && err && err->empty()) *err = "physics launch failed";
+    return rc;
+  }
+  // batched: panels once for every trace any line accepted, shared by the brick
+  b.prof->begin(QPSDM_K_PRE, st);
+  k_any_line<<<(b.ntr + 255) / 256, 256, 0, st>>>(b.d_ints, b.ints_ls, b.nlines, b.ntr,
+                                                  s->d_any);
+  rc = run_panels(s, p, b, s->d_any, 1, st, err);
   b.prof->end(st);
-  if (cudaGetLastError() != cudaSuccess) {
-    if (err) *err = "physics launch failed";
-    return QPSDM_ECUDA;
+  if (rc) return rc;
+  for (int il = 0; il < b.nlines; ++il) {
+    const LineView v = view(il);
+    b.prof->begin(QPSDM_K_OTHER, st);
+    rc = batched_group(s, p, v, b, st);
+    b.prof->end(st);
+    if (rc) {
+      if (err) *err = "batched grouping failed";
+      return rc;
+    }
+    const PhysImageArgs a = image_args(s, p, lines[il], o, b.nxz);
+    b.prof->begin(QPSDM_K_IMAGE, st);
+    if (s->dtype == QPSDM_PANEL_FP32)
+      rc = launch_batched_image<float>(s, a, b, v, st);
+    else if (s->dtype == QPSDM_PANEL_BF16)
+      rc = launch_batched_image<__nv_bfloat16>(s, a, b, v, st);
+    else
+      rc = launch_batched_image<__half>(s, a, b, v, st);
+    b.prof->end(st);
+    if (rc) {
+      if (err) *err = "batched image launch failed";
+      return rc;
+    }
   }
   return QPSDM_OK;
+}
+
+int physics_tuning(const PhysicsState *s, int *variant, int *tz, int *tx, int *mb,
+                   float *times, int ntimes) {
+  if (!s) return QPSDM_ESTATE;
+  const int v = s->variant;
+  if (variant) *variant = v;
+  if (tz) *tz = v >= 0 ? kVariants[v].tz : 0;
+  if (tx) *tx = v >= 0 ? kVariants[v].tx : 0;
+  if (mb) *mb = v >= 0 ? kVariants[v].mb : 0;
+  for (int i = 0; times && i < ntimes && i < kNumVariants; ++i) times[i] = s->tune_ms[i];
+  return kNumVariants;
 }
 
 int physics_finalize_image(PhysicsState *s, float *d_img, size_t n, cudaStream_t st,

@@ -13,15 +13,20 @@ namespace qpsdm {
 
 struct PhysicsState;
 
+// One batch of records imaged into every line of the brick.  Per-line arrays
+// are laid out line after line with the given strides (elements).
 struct PhysicsBatch {
   const uint8_t *d_rec;
-  int rec_bytes, ntr, big_endian;
+  int rec_bytes, ntr, big_endian, nlines;
   int *d_ints;
+  size_t ints_ls;
   float *d_geom;
+  size_t geom_ls;
   const float *d_taper200;
-  const float *d_dips;
+  const float *d_dips;  // line stride 4 * nxz
   size_t nxz;
   float *d_img;
+  size_t img_ls;
   unsigned long long *d_npt;
   unsigned *d_err;
   KernelProfiler *prof;
@@ -29,13 +34,17 @@ struct PhysicsBatch {
 
 int physics_create(PhysicsState **out, const qpsdm_static_params &p, std::string *err);
 void physics_destroy(PhysicsState *s);
-int physics_set_line(PhysicsState *s, const qpsdm_static_params &p,
-                     const qpsdm_line_params &l, cudaStream_t st, std::string *err);
+int physics_set_lines(PhysicsState *s, const qpsdm_static_params &p,
+                      const qpsdm_line_params *lines, int nlines, cudaStream_t st,
+                      std::string *err);
 int physics_begin_offset(PhysicsState *s, const qpsdm_static_params &p,
-                         const qpsdm_offset_params &o, cudaStream_t st, std::string *err);
+                         const qpsdm_offset_params &o, int nlines, cudaStream_t st,
+                         std::string *err);
 int physics_process(PhysicsState *s, const qpsdm_static_params &p,
-                    const qpsdm_line_params &l, const qpsdm_offset_params &o,
+                    const qpsdm_line_params *lines, const qpsdm_offset_params &o,
                     const PhysicsBatch &b, cudaStream_t st, std::string *err);
+int physics_tuning(const PhysicsState *s, int *variant, int *tz, int *tx, int *mb,
+                   float *times, int ntimes);
 int physics_finalize_image(PhysicsState *s, float *d_img, size_t n, cudaStream_t st,
                            std::string *err);
 

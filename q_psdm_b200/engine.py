@@ -40,7 +40,8 @@ def static_params(*, nxi, nzi, ntl, dt, dxi, dyi, dzi, fci=1, scaled=1.0,
                   fxv, fyv, nxv, nyv, fc=40.0, f1=1.0, f3=130.0, f4=140.0,
                   threshold=600.0, contract=3.0, taperzone=8.0, dzii=48.0,
                   mode=_lib.MODE_COMPAT, panel_dtype=_lib.PANEL_FP32, nbins=16,
-                  dtstar=0.002, max_batch=4096, kahan=0) -> StaticParams:
+                  dtstar=0.002, max_batch=4096, kahan=0, form=0, use_graph=0,
+                  tile_z=0, tile_x=0) -> StaticParams:
     """Build line-independent parameters the way main()/qpsdm() do.
 
     The velocity-grid bounding box is padded by 2 km in x and 1 km in y
@@ -58,6 +59,7 @@ def static_params(*, nxi, nzi, ntl, dt, dxi, dyi, dzi, fci=1, scaled=1.0,
     p.dzii = dzii
     p.mode, p.panel_dtype, p.nbins, p.dtstar = mode, panel_dtype, nbins, dtstar
     p.max_batch, p.kahan = max_batch, kahan
+    p.form, p.use_graph, p.tile_z, p.tile_x = form, use_graph, tile_z, tile_x
     check(lib().qpsdm_static_params_init(C.byref(p)), what="static_params_init")
     return p
 
@@ -145,7 +147,20 @@ class Engine:
         """dips: (dipx1, dipx2, dipy1, dipy2), each [nxi, nzi] float32.
         tables: None or dict(nxg, nzg, nxi1, nzi1, cdp1, cdp2, ttt_desc,
         ttt, qqq_desc, qqq) in the reference layout."""
+        self.set_lines([dict(fxi=fxi, cyi=cyi, dips=dips, nf3=nf3, q=q, tables=tables,
+                             ttt_cdp1=ttt_cdp1, ttt_cdp2=ttt_cdp2)])
+
+    def set_lines(self, lines) -> None:
+        """An image brick: a list of set_line keyword dicts, one per line."""
         keep = []
+        arr = (LineParams * len(lines))()
+        for i, ln in enumerate(lines):
+            arr[i] = self._line_params(keep, **ln)
+        self._ck(lib().qpsdm_set_lines(self.h, arr, len(lines)), "set_lines")
+        self.nlines = len(lines)
+
+    def _line_params(self, keep, *, fxi, cyi, dips, nf3=None, q=None, tables=None,
+                     ttt_cdp1=None, ttt_cdp2=None) -> LineParams:
         def fptr(a, dt=np.float32):
             if a is None:
                 return None
@@ -172,7 +187,7 @@ class Engine:
         else:
             lp.ttt_cdp1 = self.p.fci if ttt_cdp1 is None else ttt_cdp1
             lp.ttt_cdp2 = self.p.fci + self.p.nxi - 1 if ttt_cdp2 is None else ttt_cdp2
-        self._ck(lib().qpsdm_set_line(self.h, C.byref(lp)), "set_line")
+        return lp
 
     def begin_offset(self, o: OffsetParams) -> None:
         self._ck(lib().qpsdm_begin_offset(self.h, C.byref(o)), "begin_offset")
@@ -197,11 +212,13 @@ class Engine:
         self._ck(lib().qpsdm_fence(self.h), "fence")
 
     def get_image(self, apply_nsb_scale: bool = True) -> np.ndarray:
+        """[nxb, nzi] for one line, [nlines, nxb, nzi] for a brick."""
         nxb = self.off.ixend - self.off.ixstart
-        img = np.zeros((nxb, self.p.nzi), np.float32)
+        nl = getattr(self, "nlines", 1)
+        img = np.zeros((nl, nxb, self.p.nzi), np.float32)
         self._ck(lib().qpsdm_get_image(self.h, img.ctypes.data, int(apply_nsb_scale)),
                  "get_image")
-        return img
+        return img[0] if nl == 1 else img
 
     def set_stream(self, stream_handle: int | None) -> None:
         """Run engine kernels on a caller stream (e.g. torch's
@@ -217,6 +234,17 @@ class Engine:
         ms, n = C.c_double(), C.c_int64()
         self._ck(lib().qpsdm_profile_get(self.h, cls, C.byref(ms), C.byref(n)), "profile_get")
         return ms.value, n.value
+
+    def tuning(self) -> dict:
+        """The batched form's autotuned image-kernel variant and timings."""
+        v, tz, tx, mb = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        ms = np.zeros(16, np.float32)
+        n = lib().qpsdm_tuning_info(self.h, C.byref(v), C.byref(tz), C.byref(tx),
+                                    C.byref(mb), ms.ctypes.data, ms.size)
+        if n < 0:
+            raise QpsdmError(-n, "tuning_info")
+        return {"variant": v.value, "tile": [tz.value, tx.value], "min_blocks": mb.value,
+                "variant_ms": [float(x) for x in ms[:n]]}
 
     def image_device_ptr(self) -> int:
         p = C.c_void_p()

@@ -22,8 +22,13 @@ NBINS, DTSTAR = 16, 0.0015
 
 
 def make_case(nshots: int = 2, seed: int = 3, shots=None, line: int = 64,
-              half_x: int = 40, half_y: int = 30, ixstart: int = 0, ixend: int = 128):
+              half_x: int = 40, half_y: int = 30, ixstart: int = 0, ixend: int = 128,
+              rstep: int = 1):
+    """rstep > 1 keeps every rstep-th receiver of the spread (smaller cases
+    with many shots)."""
     sv = synth.config1(seed)
+    if rstep > 1:
+        sv.receivers = sv.receivers[::rstep].copy()
     shots = list(range(5, 5 + nshots)) if shots is None else list(shots)
     sx, sy, gx, gy = synth.trace_geometry(sv, shots)
     hdr = np.stack([sx, sy, gx, gy], axis=1).astype(np.int32)
@@ -75,7 +80,7 @@ def oracle_run(case, nbins=NBINS, dtstar=DTSTAR):
 
 
 def engine(case, *, panel_dtype=0, kahan=0, nbins=NBINS, dtstar=DTSTAR, max_batch=4096,
-           device=0):
+           device=0, form=0, tile=(0, 0), use_graph=0):
     from q_psdm_b200 import engine as E
     sv = case["sv"]
     p = E.static_params(nxi=sv.nxi, nzi=sv.nzi, ntl=NTL, dt=float(DT), dxi=sv.dxi, dyi=sv.dyi,
@@ -83,7 +88,8 @@ def engine(case, *, panel_dtype=0, kahan=0, nbins=NBINS, dtstar=DTSTAR, max_batc
                         nxv=sv.nxi, nyv=sv.nyi, fc=case["fc"], f1=F1, f3=F3, f4=F4,
                         threshold=THRESHOLD, contract=CONTRACT, taperzone=TAPERZONE,
                         dzii=case["tab"].dzii, mode=1, panel_dtype=panel_dtype,
-                        nbins=nbins, dtstar=dtstar, max_batch=max_batch, kahan=kahan)
+                        nbins=nbins, dtstar=dtstar, max_batch=max_batch, kahan=kahan,
+                        form=form, tile_z=tile[0], tile_x=tile[1], use_graph=use_graph)
     eng = E.Engine(p, device=device)
     d = case["dips"].reshape(4, sv.nxi, sv.nzi)
     eng.set_line(fxi=case["fxi"], cyi=case["cyi"], dips=d, tables=case["tab"].as_engine_dict())

@@ -108,3 +108,32 @@ def test_nsb_scale_and_errors(cuda):
             eng.submit(bad)  # ns != ntl
     finally:
         eng.close()
+
+
+def test_compat_brick_bit_exact(cuda):
+    from q_psdm_b200 import engine as E
+    from tests.compat_case import DT, NTL
+    c = make_case("small")
+    refs = []
+    for L in (60, 64):
+        cc = dict(c, cyi=c["sv"].line_y(L))
+        cc["ref_args"] = dict(c["ref_args"], cyi=cc["cyi"])
+        refs.append(oracle_run(cc)[2])
+    eng, _, *_ = engine_run(c)
+    try:
+        sv = c["sv"]
+        d = c["dips"].reshape(4, sv.nxi, sv.nzi)
+        eng.set_lines([dict(fxi=c["fxi"], cyi=sv.line_y(L), dips=d, ttt_cdp1=c["tcdp"][0],
+                            ttt_cdp2=c["tcdp"][1]) for L in (60, 64)])
+        az = c["az"]
+        o = E.offset_params(eng.p, c["ixstart"], c["ixend"], aznx1=az[0], aznx2=az[1],
+                            azny1=az[2], azny2=az[3])
+        eng.begin_offset(o)
+        h = c["hdr"]
+        rec = E.encode_su(h[:, 0], h[:, 1], h[:, 2], h[:, 3], c["traces"],
+                          dt_us=int(round(float(DT) * 1e6)), scalco=sv.scalco)
+        eng.submit(rec)
+        img = eng.get_image(False)
+    finally:
+        eng.close()
+    assert np.array_equal(img[0], refs[0]) and np.array_equal(img[1], refs[1])

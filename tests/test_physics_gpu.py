@@ -77,3 +77,64 @@ def test_missing_tables_rejected(cuda, case):
                          dips=case["dips"].reshape(4, sv.nxi, sv.nzi), tables=bad)
     finally:
         eng.close()
+
+
+# ---- batched form ---------------------------------------------------------
+@pytest.mark.parametrize("dtype,tol", [(0, 5e-5), (1, 1e-3)])
+@pytest.mark.parametrize("tile", [(32, 8), (64, 4), (128, 2), (32, 4)])
+def test_batched_matches_fp64(cuda, case, dtype, tol, tile):
+    eng, p, o = engine(case, panel_dtype=dtype, form=1, tile=tile)
+    try:
+        eng.submit(records(case))
+        img = eng.get_image(False)
+        _, npt = eng.counters()
+    finally:
+        eng.close()
+    assert npt == case["o_npt"]
+    assert nrmse(img, case["o_img"]) <= tol
+
+
+def test_batched_many_shots_and_splits(cuda):
+    # 11 shots exceed one source chunk of the batched kernel; irregular split
+    c = make_case(shots=range(2, 13), rstep=8, half_x=50, half_y=40)
+    ref, npt, _ = oracle_run(c)
+    rec = records(c)
+    eng, p, o = engine(c, form=1, max_batch=1000, kahan=1)
+    try:
+        eng.submit(rec[:333])
+        eng.submit(rec[333:])
+        img = eng.get_image(False)
+        _, n = eng.counters()
+    finally:
+        eng.close()
+    assert n == npt
+    assert nrmse(img, ref) <= 5e-5
+
+
+# ---- image bricks (several lines per submit) ------------------------------
+@pytest.mark.parametrize("form,dtype,tol", [(0, 0, 5e-5), (1, 0, 5e-5), (1, 1, 1e-3)])
+def test_brick_equals_single_lines(cuda, form, dtype, tol):
+    base = make_case(nshots=2, rstep=2, half_y=40)
+    lines = [58, 64, 70]
+    refs, npt_ref = [], 0
+    for L in lines:
+        c = dict(base, line=L, cyi=base["sv"].line_y(L))
+        img, npt, _ = oracle_run(c)
+        refs.append(img)
+        npt_ref += npt
+    eng, p, o = engine(base, panel_dtype=dtype, form=form)
+    try:
+        sv = base["sv"]
+        d = base["dips"].reshape(4, sv.nxi, sv.nzi)
+        eng.set_lines([dict(fxi=base["fxi"], cyi=sv.line_y(L), dips=d,
+                            tables=base["tab"].as_engine_dict()) for L in lines])
+        eng.begin_offset(o)
+        eng.submit(records(base))
+        img = eng.get_image(False)
+        _, npt = eng.counters()
+    finally:
+        eng.close()
+    assert img.shape == (3, base["nxb"], sv.nzi)
+    assert npt == npt_ref
+    for k in range(3):
+        assert nrmse(img[k], refs[k]) <= tol, k
