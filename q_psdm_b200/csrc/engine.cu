@@ -15,7 +15,9 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -64,6 +66,14 @@ struct qpsdm_engine {
   // physics state (physics.cu)
   PhysicsState *phys = nullptr;
   KernelProfiler prof;
+  // CUDA graphs of whole batches, keyed by (record buffer, ntr, big_endian)
+  struct GraphRec {
+    cudaGraphExec_t exec;
+    int64_t launches[4];
+  };
+  std::map<std::tuple<const void *, int, int>, GraphRec> graphs;
+  int64_t batches_run = 0;
+  int64_t graph_replays = 0;
 };
 
 namespace {
@@ -107,6 +117,8 @@ int grow(qpsdm_engine *e, T **ptr, size_t *cap, size_t need) {
   *cap = need;
   return QPSDM_OK;
 }
+
+void clear_graphs(qpsdm_engine *e);
 
 // Taper factors of fetch_and_taper (src/psdmpkg.cc:221-228), computed on the
 // host with the same float/double mix so the device multiplies by the same
@@ -192,6 +204,7 @@ extern "C" int qpsdm_engine_destroy(qpsdm_engine *e) {
   DeviceGuard g(e->device);
   if (e->s_comp) cudaStreamSynchronize(e->s_comp);
   if (e->s_copy) cudaStreamSynchronize(e->s_copy);
+  clear_graphs(e);
   if (e->phys) physics_destroy(e->phys);
   for (int i = 0; i < 2; ++i) {
     if (e->ev_stage_free[i]) cudaEventDestroy(e->ev_stage_free[i]);
@@ -249,6 +262,7 @@ extern "C" int qpsdm_set_lines(qpsdm_engine *e, const qpsdm_line_params *l, int 
     if (rc) return rc;
   }
   e->lines.assign(l, l + nlines);
+  clear_graphs(e);
   e->line_set = true;
   e->offset_set = false;
   return QPSDM_OK;
@@ -291,6 +305,7 @@ extern "C" int qpsdm_begin_offset(qpsdm_engine *e, const qpsdm_offset_params *o)
     if (rc) return rc;
   }
   e->off = *o;
+  clear_graphs(e);
   e->offset_set = true;
   e->traces_accepted = 0;
   return QPSDM_OK;
@@ -395,6 +410,54 @@ int process_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
   return physics_process(e->phys, e->p, e->lines.data(), e->off, b, e->s_comp, &e->err);
 }
 
+void clear_graphs(qpsdm_engine *e) {
+  for (auto &kv : e->graphs) cudaGraphExecDestroy(kv.second.exec);
+  e->graphs.clear();
+}
+
+// One batch: replayed from a CUDA graph when use_graph is set and this
+// (buffer, size) was seen before; captured on its second occurrence (the
+// first runs eagerly so that plans, attributes and the autotuner settle).
+int run_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
+  const bool graphs = e->p.use_graph != 0;
+  if (!graphs || e->batches_run == 0) {
+    ++e->batches_run;
+    return process_batch(e, d_rec, ntr, be);
+  }
+  const auto key = std::make_tuple((const void *)d_rec, ntr, be);
+  auto it = e->graphs.find(key);
+  if (it != e->graphs.end()) {
+    CK(cudaGraphLaunch(it->second.exec, e->s_comp));
+    for (int c = 0; c < 4; ++c) e->prof.launches[c] += it->second.launches[c];
+    ++e->graph_replays;
+    ++e->batches_run;
+    return QPSDM_OK;
+  }
+  int64_t before[4];
+  for (int c = 0; c < 4; ++c) before[c] = e->prof.launches[c];
+  const bool prof_on = e->prof.on;
+  e->prof.on = false;  // no timing events inside the graph
+  CK(cudaStreamBeginCapture(e->s_comp, cudaStreamCaptureModeThreadLocal));
+  const int rc = process_batch(e, d_rec, ntr, be);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(e->s_comp, &g);
+  e->prof.on = prof_on;
+  if (rc || ce != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return rc ? rc : cuda_fail(e, ce, "cudaStreamEndCapture");
+  }
+  qpsdm_engine::GraphRec gr{};
+  const cudaError_t ie = cudaGraphInstantiate(&gr.exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) return cuda_fail(e, ie, "cudaGraphInstantiate");
+  for (int c = 0; c < 4; ++c) gr.launches[c] = e->prof.launches[c] - before[c];
+  e->graphs[key] = gr;
+  CK(cudaGraphLaunch(gr.exec, e->s_comp));
+  ++e->batches_run;
+  return QPSDM_OK;
+}
+
 }  // namespace
 
 extern "C" int qpsdm_submit_traces_device(qpsdm_engine *e, const void *d_records,
@@ -406,7 +469,7 @@ extern "C" int qpsdm_submit_traces_device(qpsdm_engine *e, const void *d_records
   if (ntr < 0 || ntr > e->p.max_batch) return fail(e, QPSDM_EINVAL, "ntr outside [0, max_batch]");
   if (ntr == 0) return QPSDM_OK;
   DeviceGuard g(e->device);
-  return process_batch(e, (const uint8_t *)d_records, ntr, be);
+  return run_batch(e, (const uint8_t *)d_records, ntr, be);
 }
 
 extern "C" int qpsdm_submit_traces(qpsdm_engine *e, const void *records, int ntr,
@@ -438,7 +501,7 @@ extern "C" int qpsdm_submit_traces(qpsdm_engine *e, const void *records, int ntr
     if (pinned) CK(cudaEventSynchronize(e->ev_stage_free[s]));
     CK(cudaEventRecord(e->ev_rec_ready[s], e->s_copy));
     CK(cudaStreamWaitEvent(e->s_comp, e->ev_rec_ready[s], 0));
-    int rc = process_batch(e, e->d_rec[s], n, be);
+    int rc = run_batch(e, e->d_rec[s], n, be);
     if (rc) return rc;
     CK(cudaEventRecord(e->ev_rec_free[s], e->s_comp));
     e->slot ^= 1;
