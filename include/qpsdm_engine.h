@@ -243,6 +243,55 @@ int qpsdm_spectra_device_ptr(qpsdm_engine *e, float **d_re, float **d_im);
  * (sx, sy, gx, gy relative to fxi, cyi).  Device pointers. */
 int qpsdm_gate_device_ptr(qpsdm_engine *e, int **d_ints, float **d_geom);
 
+/* ---- table generation (the files get_ttt_all reads) -----------------------*/
+
+/* Gridded model: velocity (m/s) and 1/Q on [nz][ny][nx] nodes of spacing h
+ * with origin (ox, oy) at the surface; (v0, kz) is the linear-gradient
+ * background used to start each source analytically. */
+typedef struct {
+  int nx, ny, nz;
+  float h, ox, oy;
+  float v0, kz;
+} qpsdm_eik_model;
+
+/* Local grid of every source of a batch: nx x ny x nz nodes of spacing h. */
+typedef struct {
+  int nx, ny, nz;
+  float h;
+} qpsdm_eik_grid;
+
+/* Traveltime T and t* of nsrc surface sources on their local grids
+ * (d_T, d_tstar: [nsrc][nz][ny][nx]).  d_src: nsrc x (sx, sy, ox, oy) floats,
+ * source position and local-grid origin in model coordinates.  d_work:
+ * 2 * nsrc * nx*ny*nz + 1 floats of scratch.  First-order Godunov upwind
+ * updates relaxed until nothing changes (at most max_iter sweeps), the
+ * analytic background held inside init_radius of the source.  The
+ * generator of the L<line>.ttt / .qqq data read by get_ttt_all
+ * (src/q-psdm.cu:2382-2627); no counterpart of its own in the reference. */
+int qpsdm_eikonal_solve(const float *d_vel, const float *d_invq,
+                        const qpsdm_eik_model *model, const float *d_src, int nsrc,
+                        const qpsdm_eik_grid *grid, float init_radius, int max_iter,
+                        float *d_work, float *d_T, float *d_tstar, void *stream);
+
+/* Geometry of the line table being filled (reference layout). */
+typedef struct {
+  int nxi1, nzi1, nzg;
+  float dxi, dzii;
+  float x_cdp1; /* model x of the table's first cdp */
+  float line_y; /* model y of the image line */
+} qpsdm_eik_fill_geom;
+
+/* Writes every table entry whose source is in this solved batch
+ * (sources s0 .. s0+ns-1, d_src of the batch) by trilinear sampling of the
+ * grids: entries of cell c are block c of the descriptors (d_cell_base:
+ * ncell+1 prefix sums of block sizes), node_src maps (cell, surface node) to
+ * the global source number (d_node_base: ncell+1 prefix sums of nodes). */
+int qpsdm_eikonal_fill(const float *d_T, const float *d_tstar, const qpsdm_eik_grid *grid,
+                       const float *d_src, int s0, int ns, const qpsdm_ttt_desc *d_desc,
+                       const int64_t *d_cell_base, const int *d_node_base,
+                       const int *d_node_src, int ncell, const qpsdm_eik_fill_geom *fg,
+                       float *d_ttt, float *d_qqq, void *stream);
+
 /* ---- standalone kernels (device pointers) ---------------------------------*/
 
 /* Batched real-to-complex FFT, unnormalised, e^{-iwt} (the convention of

@@ -73,6 +73,20 @@ class OffsetParams(C.Structure):
     ]
 
 
+class EikModel(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("h", C.c_float),
+                ("ox", C.c_float), ("oy", C.c_float), ("v0", C.c_float), ("kz", C.c_float)]
+
+
+class EikGrid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("h", C.c_float)]
+
+
+class EikFillGeom(C.Structure):
+    _fields_ = [("nxi1", C.c_int), ("nzi1", C.c_int), ("nzg", C.c_int), ("dxi", C.c_float),
+                ("dzii", C.c_float), ("x_cdp1", C.c_float), ("line_y", C.c_float)]
+
+
 # (name, restype, argtypes) of every symbol include/qpsdm_engine.h declares.
 _P, _I, _F, _V = C.c_void_p, C.c_int, C.c_float, C.c_void_p
 SYMBOLS = [
@@ -102,6 +116,10 @@ SYMBOLS = [
     ("qpsdm_fft_r2c", _I, [_P, _I, _I, _P, _P]),
     ("qpsdm_fft_c2r", _I, [_P, _I, _I, _P, _P]),
     ("qpsdm_fft_r2c_noalloc", _I, [_P, _I, _I, _P, _P]),
+    ("qpsdm_eikonal_solve", _I, [_P, _P, C.POINTER(EikModel), _P, _I, C.POINTER(EikGrid),
+                                 _F, _I, _P, _P, _P, _P]),
+    ("qpsdm_eikonal_fill", _I, [_P, _P, C.POINTER(EikGrid), _P, _I, _I, _P, _P, _P, _P, _I,
+                                C.POINTER(EikFillGeom), _P, _P, _P]),
 ]
 FFT_NOALLOC_MAX_N = 8192
 ESIZE = 8

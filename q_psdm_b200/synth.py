@@ -189,3 +189,39 @@ def dip_fields(nxi: int, nzi: int, contract_rad: float):
     x1 = np.full((nxi, nzi), lo, np.float32)
     x2 = np.full((nxi, nzi), hi, np.float32)
     return x1, x2, x1.copy(), x2.copy()
+
+
+def config2_anomalies(seed: int = 0):
+    """Two seeded Gaussian velocity anomalies (+15 % and -15 %, 300 m radius)
+    inside the config-2 image volume: rows of (x, y, z, relative amplitude),
+    coordinates relative to the first image cdp and line."""
+    rng = np.random.default_rng([seed, 2])
+    xy = rng.uniform(1200.0, 3900.0, size=(2, 2))
+    z = rng.uniform(900.0, 2400.0, size=2)
+    return np.array([[xy[0, 0], xy[0, 1], z[0], 0.15], [xy[1, 0], xy[1, 1], z[1], -0.15]])
+
+
+Q_LAYERS = ((0.0, 200.0), (600.0, 120.0), (1300.0, 80.0), (2100.0, 50.0), (3000.0, 30.0))
+
+
+def config2_model(h: float = 40.0, seed: int = 0, anomalies: bool = True,
+                  layered_q: bool = True, xr=(-2800.0, 7900.0), yr=(-1400.0, 6600.0),
+                  zmax: float = 4200.0, v0: float = 1800.0, kz: float = 0.5, q: float = 80.0):
+    """Config-2 model on a grid: v(z) = v0 + kz z plus the two anomalies, and
+    the 5-layer Q model (Q 200/120/80/50/30 below 0/600/1300/2100/3000 m)."""
+    from .tables import GridModel
+    xs = np.arange(xr[0], xr[1] + h, h, dtype=np.float32)
+    ys = np.arange(yr[0], yr[1] + h, h, dtype=np.float32)
+    zs = np.arange(0.0, zmax + h, h, dtype=np.float32)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    v = v0 + kz * Z
+    if anomalies:
+        for ax, ay, az, amp in config2_anomalies(seed):
+            r2 = (X - ax) ** 2 + (Y - ay) ** 2 + (Z - az) ** 2
+            v = v * (1.0 + amp * np.exp(-r2 / (300.0 ** 2)))
+    iq = np.full(v.shape, 1.0 / q, np.float32)
+    if layered_q:
+        for ztop, qv in Q_LAYERS:
+            iq[Z >= ztop] = 1.0 / qv
+    return GridModel(v.astype(np.float32), iq.astype(np.float32), h, float(xs[0]),
+                     float(ys[0]), v0, kz)

@@ -178,3 +178,143 @@ def load_line(ttpath: str, line: int, line1: int, line2: int, torq: str = "t") -
     c2 = np.float32(1.0 * (line - lo) / (hi - lo))
     c1 = np.float32(1.0 - c2)
     return (a * c1 + b * c2).astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# tables from the eikonal / t* generator (GPU)
+# ---------------------------------------------------------------------------
+@dataclass
+class GridModel:
+    """Velocity (m/s) and 1/Q on [nz][ny][nx] nodes of spacing h, origin
+    (ox, oy) at the surface, coordinates relative to the first image cdp (x)
+    and the first image line (y).  (v0, kz) is the linear-gradient background
+    that starts every source analytically."""
+    vel: np.ndarray
+    invq: np.ndarray
+    h: float
+    ox: float
+    oy: float
+    v0: float
+    kz: float
+
+
+def _layout(nxi, nxi1, nzi1, nxs, nys, surf_dx, surf_dy, nzg=1):
+    ncdp = nxi
+    nxg = -(-ncdp // nxi1)
+    desc = np.zeros(nxg * nzg, DESC_DTYPE)
+    block = nys * nxs * nxi1 * nzi1
+    for k in range(nxg * nzg):
+        desc[k] = (k * block, nys, nxs, surf_dy, surf_dx)
+    return nxg, nzg, desc, block
+
+
+def eikonal_line_tables(model: GridModel, *, fci: int, nxi: int, dxi: float, zmax: float,
+                        line_y: float, dzii: float, nxi1: int = 16, surf_dx: int,
+                        surf_dy: int, half_x: float, half_y: float, h: float | None = None,
+                        batch: int = 128, init_radius: float | None = None,
+                        device: int = 0, background: GridModel | None = None,
+                        q_background: float | None = None) -> LineTables:
+    """Tables of the image line at model y = line_y, computed by the GPU
+    eikonal / t* generator (qpsdm_eikonal_solve + qpsdm_eikonal_fill) in the
+    reference layout; every distinct surface node of the cells' grids is one
+    source, solved on its own local grid.
+
+    With `background` (the linear-gradient model v0 + kz z of `model`, with
+    constant Q = q_background) the first-order scheme's systematic error is
+    cancelled: T = T_exact(bg) + T(model) - T(bg) and
+    t* = t*(model) * t*_exact(bg) / t*(bg), the background solved on the same
+    grids and its exact values from the linear-gradient formula."""
+    if background is not None:
+        kw = dict(fci=fci, nxi=nxi, dxi=dxi, zmax=zmax, line_y=line_y, dzii=dzii, nxi1=nxi1,
+                  surf_dx=surf_dx, surf_dy=surf_dy, half_x=half_x, half_y=half_y, h=h,
+                  batch=batch, init_radius=init_radius, device=device)
+        full = eikonal_line_tables(model, **kw)
+        bg = eikonal_line_tables(background, **kw)
+        v0, kz = background.v0, background.kz
+
+        def tfn(px, py, x, z):
+            r = np.hypot(px - x, py)
+            if kz < 1e-9:
+                return np.hypot(r, z) / v0
+            v = v0 + kz * z
+            return np.arccosh(np.maximum(1.0 + kz * kz * (r * r + z * z) / (2 * v0 * v), 1.0)) / kz
+
+        ana = build_line_tables(tfn, lambda *a: tfn(*a) / q_background, fci=fci, nxi=nxi,
+                                dxi=dxi, zmax=zmax, dzii=dzii, nxi1=nxi1, nzi1=full.nzi1,
+                                surf_dx=surf_dx, surf_dy=surf_dy, half_x=half_x, half_y=half_y)
+        full.ttt[:] = (ana.ttt.astype(np.float64) + full.ttt - bg.ttt).astype(np.float32)
+        ratio = np.where(bg.qqq > 0, ana.qqq / np.maximum(bg.qqq, 1e-12), 1.0)
+        full.qqq[:] = (full.qqq * ratio).astype(np.float32)
+        return full
+    import ctypes as C
+
+    import torch
+
+    from . import _lib
+    L = _lib.lib()
+    h = h or model.h
+    r0 = init_radius if init_radius is not None else 3.0 * h
+    nnodes = int(np.floor(zmax / dzii)) + 2
+    nxs = 2 * int(np.ceil(half_x / surf_dx)) + 1
+    nys = 2 * int(np.ceil(half_y / surf_dy)) + 1
+    nxg, nzg, desc, block = _layout(nxi, nxi1, nnodes, nxs, nys, surf_dx, surf_dy)
+    tab = LineTables(fci, fci + nxi - 1, dxi, 8.0, nxg, nzg, nxi1, nnodes, dzii, desc,
+                     np.zeros(nxg * nzg * block, np.float32),
+                     np.zeros(nxg * nzg * block, np.float32))
+    # distinct surface nodes -> sources
+    pos, node_src = {}, []
+    for c in range(nxg * nzg):
+        xs, ys = cell_surface_nodes(tab, c // nzg, c % nzg, fci)
+        for y in ys:
+            for x in xs:
+                key = (round(float(x), 3), round(float(line_y + y), 3))
+                if key not in pos:
+                    pos[key] = len(pos)
+                node_src.append(pos[key])
+    src_xy = np.array(list(pos.keys()), np.float32)
+    nsrc = len(src_xy)
+    node_base = np.arange(0, nxg * nzg + 1, dtype=np.int32) * (nys * nxs)
+    cell_base = np.arange(0, nxg * nzg + 1, dtype=np.int64) * block
+    # local grid of each source: the cells that use it and the line
+    gx = int(np.ceil((2 * (half_x + nxi1 * dxi) + 4 * h) / h)) + 1
+    gy = int(np.ceil((2 * half_y + 4 * h) / h)) + 1
+    gz = int(np.ceil(zmax / h)) + 3
+    grid = _lib.EikGrid(gx, gy, gz, h)
+    oy = line_y - half_y - 2 * h
+    mdl = _lib.EikModel(model.vel.shape[2], model.vel.shape[1], model.vel.shape[0], model.h,
+                        model.ox, model.oy, model.v0, model.kz)
+    fg = _lib.EikFillGeom(nxi1, nnodes, nzg, dxi, dzii, 0.0, line_y)
+    dev = torch.device("cuda", device)
+    d_vel = torch.from_numpy(np.ascontiguousarray(model.vel, np.float32)).to(dev)
+    d_iq = torch.from_numpy(np.ascontiguousarray(model.invq, np.float32)).to(dev)
+    d_desc = torch.from_numpy(desc.view(np.uint8).copy()).to(dev)
+    d_cb = torch.from_numpy(cell_base).to(dev)
+    d_nb = torch.from_numpy(node_base).to(dev)
+    d_ns = torch.from_numpy(np.array(node_src, np.int32)).to(dev)
+    d_ttt = torch.zeros(tab.ttt.size, dtype=torch.float32, device=dev)
+    d_qqq = torch.zeros(tab.qqq.size, dtype=torch.float32, device=dev)
+    n = gx * gy * gz
+    nb = min(batch, nsrc)
+    d_T = torch.empty(nb * n, dtype=torch.float32, device=dev)
+    d_S = torch.empty(nb * n, dtype=torch.float32, device=dev)
+    d_w = torch.empty(2 * nb * n + 1, dtype=torch.float32, device=dev)
+    for s0 in range(0, nsrc, nb):
+        ns = min(nb, nsrc - s0)
+        sp = np.zeros((ns, 4), np.float32)
+        sp[:, 0:2] = src_xy[s0:s0 + ns]
+        sp[:, 2] = sp[:, 0] - 0.5 * (gx - 1) * h
+        sp[:, 3] = oy
+        d_sp = torch.from_numpy(sp).to(dev)
+        rc = L.qpsdm_eikonal_solve(d_vel.data_ptr(), d_iq.data_ptr(), C.byref(mdl),
+                                   d_sp.data_ptr(), ns, C.byref(grid), r0, 4 * (gx + gy + gz),
+                                   d_w.data_ptr(), d_T.data_ptr(), d_S.data_ptr(), None)
+        _lib.check(rc, what="eikonal_solve")
+        rc = L.qpsdm_eikonal_fill(d_T.data_ptr(), d_S.data_ptr(), C.byref(grid), d_sp.data_ptr(),
+                                  s0, ns, d_desc.data_ptr(), d_cb.data_ptr(), d_nb.data_ptr(),
+                                  d_ns.data_ptr(), nxg * nzg, C.byref(fg), d_ttt.data_ptr(),
+                                  d_qqq.data_ptr(), None)
+        _lib.check(rc, what="eikonal_fill")
+    torch.cuda.synchronize(dev)
+    tab.ttt[:] = d_ttt.cpu().numpy()
+    tab.qqq[:] = d_qqq.cpu().numpy()
+    return tab
