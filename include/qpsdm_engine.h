@@ -320,6 +320,47 @@ int qpsdm_fft_c2r(const float *d_in, int n, int batch, float *d_out,
 int qpsdm_fft_r2c_noalloc(const float *d_in, int n, int batch, float *d_out,
                           void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Learned traveltime / t* surrogate (no counterpart in the reference, which
+ * reads precomputed tables only).
+ *
+ * A 5 -> 128 x 4 (SiLU) -> 2 multilayer perceptron: inputs (source x, source
+ * y, point x, point y, point z), outputs two table corrections.  BF16 weights
+ * and activations on the tcgen05 tensor cores, FP32 accumulation, FP32 master
+ * weights and Adam moments.  Inputs are normalised on the device as
+ * (raw - in_shift) * in_scale; the training loss is
+ *   sum_s sum_j out_weight[j] (y_j - t_j)^2 / n.
+ * The parameter vector (qpsdm_mlp_param_count() floats) is, in order:
+ * W1 [128][16] (input columns 5..15 are padding, kept at zero), b1 [128],
+ * W2 [128][128], b2, W3, b3, W4, b4, W5 [16][128] (rows 2..15 padding), b5 [16].
+ * Training kernels write per-CTA gradient slices that are summed in a fixed
+ * order: gradients and training are deterministic for a given launch size.
+ * Device pointers: d_x [n][5], d_t [n][2], d_y [n][2] floats.
+ * ------------------------------------------------------------------------- */
+typedef struct qpsdm_mlp qpsdm_mlp;
+int qpsdm_mlp_create(int device, qpsdm_mlp **out);
+int qpsdm_mlp_destroy(qpsdm_mlp *h);
+int qpsdm_mlp_param_count(void);
+/* Replace the parameters (host array) and reset the Adam state. */
+int qpsdm_mlp_set_params(qpsdm_mlp *h, const float *host_params);
+int qpsdm_mlp_get_params(qpsdm_mlp *h, float *host_params);
+int qpsdm_mlp_set_scaling(qpsdm_mlp *h, const float *in_shift,
+                          const float *in_scale, const float *out_weight);
+/* Loss and its gradient over all n samples (no update); host_grads
+ * (param_count floats) and loss may be NULL.  Synchronises the stream. */
+int qpsdm_mlp_gradients(qpsdm_mlp *h, const float *d_x, const float *d_t,
+                        int n, float *host_grads, float *loss, void *stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the n samples given; when
+ * loss is not NULL the loss before the step is returned (synchronises). */
+int qpsdm_mlp_train_step(qpsdm_mlp *h, const float *d_x, const float *d_t,
+                         int n, float lr, float *loss, void *stream);
+/* Inference, asynchronous on stream. */
+int qpsdm_mlp_forward(qpsdm_mlp *h, const float *d_x, int n, float *d_y,
+                      void *stream);
+/* Synchronise; QPSDM_ETIMEOUT if a tensor-core wait gave up in any kernel
+ * since the handle was created. */
+int qpsdm_mlp_status(qpsdm_mlp *h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,7 +17,7 @@ MODE_COMPAT, MODE_PHYSICS = 0, 1
 K_GATE, K_PRE, K_IMAGE, K_OTHER = 0, 1, 2, 3
 PANEL_FP32, PANEL_BF16, PANEL_FP16 = 0, 1, 2
 ERRORS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "ESTATE",
-          5: "ETIMEOUT", 6: "ENOTSUP", 7: "ENOKERNEL"}
+          5: "ETIMEOUT", 6: "ENOTSUP", 7: "ENOKERNEL", 8: "ESIZE"}
 
 
 class TttDesc(C.Structure):
@@ -120,6 +120,16 @@ SYMBOLS = [
                                  _F, _I, _P, _P, _P, _P]),
     ("qpsdm_eikonal_fill", _I, [_P, _P, C.POINTER(EikGrid), _P, _I, _I, _P, _P, _P, _P, _I,
                                 C.POINTER(EikFillGeom), _P, _P, _P]),
+    ("qpsdm_mlp_create", _I, [_I, C.POINTER(C.c_void_p)]),
+    ("qpsdm_mlp_destroy", _I, [_P]),
+    ("qpsdm_mlp_param_count", _I, []),
+    ("qpsdm_mlp_set_params", _I, [_P, _P]),
+    ("qpsdm_mlp_get_params", _I, [_P, _P]),
+    ("qpsdm_mlp_set_scaling", _I, [_P, _P, _P, _P]),
+    ("qpsdm_mlp_gradients", _I, [_P, _P, _P, _I, _P, C.POINTER(C.c_float), _P]),
+    ("qpsdm_mlp_train_step", _I, [_P, _P, _P, _I, _F, C.POINTER(C.c_float), _P]),
+    ("qpsdm_mlp_forward", _I, [_P, _P, _I, _P, _P]),
+    ("qpsdm_mlp_status", _I, [_P]),
 ]
 FFT_NOALLOC_MAX_N = 8192
 ESIZE = 8
