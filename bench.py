@@ -69,6 +69,15 @@ def parse():
     ap.add_argument("--form", default="batched", choices=list(FORMS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--only-surrogate", action="store_true",
+                    help="time only the surrogate network's kernels (for profiling)")
+    ap.add_argument("--shots", type=int, default=0,
+                    help="shot gathers per step of the chosen form (default: the form's own)")
+    ap.add_argument("--lines", type=int, default=0,
+                    help="image lines per step of the chosen form (default: the form's own)")
+    ap.add_argument("--tile", default="",
+                    help="batched kernel tile 'Z,X' instead of autotuning (for profiling)")
     return ap.parse_args()
 
 
@@ -81,9 +90,10 @@ class Workload:
     LINE0 = 252                      # first image line of the brick
     HALF_CDPS, HALF_LINES = 200, 100  # aperture: +-2 km in x, +-1 km in y
 
-    def __init__(self, rank: int = 0):
+    def __init__(self, rank: int = 0, tile=(0, 0)):
         from q_psdm_b200 import synth
         self.synth = synth
+        self.tile = tile
         self.sv = synth.config2(seed=11)
         self.rank = rank
         ly = self.sv.line_y(self.LINE0 + 4)
@@ -122,13 +132,14 @@ class Workload:
         from q_psdm_b200 import engine as E
         sv = self.sv
         _, _, dtype, pform = FORMS[form]
+        tz, tx = self.tile if form == "batched" else (0, 0)
         kw = dict(nxi=sv.nxi, nzi=sv.nzi, ntl=sv.ntl, dt=float(sv.dt), dxi=sv.dxi, dyi=sv.dyi,
                   dzi=sv.dzi, fci=sv.fci, scaled=sv.scaled, fxv=sv.fxv, fyv=sv.fyv,
                   nxv=sv.nxi, nyv=sv.nyi, fc=30.0, max_batch=max_batch)
         if pform is None:
             return E.static_params(**kw)
         return E.static_params(**kw, mode=1, panel_dtype=dtype, nbins=16, dtstar=0.002,
-                               form=pform, dzii=self.tables().dzii)
+                               form=pform, dzii=self.tables().dzii, tile_z=tz, tile_x=tx)
 
     def lines(self, form: str, contract_rad: float):
         sv = self.sv
@@ -335,7 +346,11 @@ def run_ours(args, rank, world, dist):
     import torch
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    wl = Workload(rank)
+    if args.shots or args.lines:
+        ns, nl, dt, pf = FORMS[args.form]
+        FORMS[args.form] = (args.shots or ns, args.lines or nl, dt, pf)
+    tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else (0, 0)
+    wl = Workload(rank, tile)
     head = run_form(args.form, wl, args, dev, dist, steps=args.steps, warmup=args.warmup,
                     e2e=not args.no_e2e)
     forms = {args.form: {k: head[k] for k in ("value", "ms_per_step", "point_traces_per_step",
@@ -375,6 +390,77 @@ def run_ours(args, rank, world, dist):
            "point_traces_per_step": head["point_traces_per_step"],
            "kernel_ms_per_step": head["kernel_ms_per_step"], "forms": forms}
     return res, wl
+
+
+# ---------------------------------------------------------------------------
+# the surrogate network (tcgen05 kernels)
+# ---------------------------------------------------------------------------
+# algorithmic multiply-adds per query: 5x128 + 3 x 128x128 + 128x2
+MLP_MAC = 5 * 128 + 3 * 128 * 128 + 128 * 2
+
+
+def run_surrogate(dev, steps, warmup, n_query=1 << 22, batch=1 << 16):
+    """Inference (one launch over n_query points) and one Adam training step
+    over `batch` samples, CUDA events around each on the launching stream.
+    Training FLOPs are counted as 3x the forward (forward, data gradient and
+    weight gradient); the kernel's recomputation of activations is extra work
+    not counted."""
+    import torch
+    from q_psdm_b200 import surrogate as S
+    torch.cuda.set_device(dev)
+    net = S.Mlp(dev, seed=0)
+    net.set_scaling(np.zeros(5), np.ones(5), (1.0, 25.0))
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    x = torch.rand((n_query, 5), generator=g, device="cuda") * 2 - 1
+    y = torch.empty((n_query, 2), device="cuda")
+    xb = torch.rand((batch, 5), generator=g, device="cuda") * 2 - 1
+    tb = torch.sin(3 * xb[:, :2]).contiguous()
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, k):
+        evs = []
+        for _ in range(k):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    for _ in range(warmup):
+        net.forward(x, out=y)
+        net.train_step(xb, tb, 1e-3)
+    torch.cuda.synchronize()
+    inf = timed(lambda: net.forward(x, out=y), steps)
+    trn = timed(lambda: net.train_step(xb, tb, 1e-3), steps)
+    net.status()
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    peak = peaks.get("bf16_tflops")
+    src = "MEASURED_PEAKS.json bf16_tflops (burst, of measured)"
+    if peak is None:
+        peak, src = 1590.0, "fallback 1.59 PFLOP/s (of fallback)"
+    ms_i = statistics.median(inf)
+    ms_t = statistics.median(trn)
+    tf_i = 2.0 * MLP_MAC * n_query / (ms_i * 1e-3) / 1e12
+    tf_t = 3 * 2.0 * MLP_MAC * batch / (ms_t * 1e-3) / 1e12
+    net.close()
+    return {"network": "5 -> 128x4 (SiLU) -> 2, BF16 operands, FP32 accumulation (tcgen05)",
+            "inference": {"kernel": "k_mlp_forward", "queries_per_launch": n_query,
+                          "ms_per_launch": ms_i, "gqueries_per_s": n_query / ms_i / 1e6,
+                          "roofline": {"bound": "tensor", "achieved": tf_i, "peak": peak,
+                                       "unit": "TFLOP/s", "frac": tf_i / peak,
+                                       "flop_per_query": 2 * MLP_MAC, "peak_source": src}},
+            "training": {"kernels": "k_mlp_grad + k_mlp_reduce + k_mlp_adam + k_mlp_pack",
+                         "batch": batch, "ms_per_step": ms_t,
+                         "msamples_per_s": batch / ms_t / 1e3,
+                         "roofline": {"bound": "tensor", "achieved": tf_t, "peak": peak,
+                                      "unit": "TFLOP/s", "frac": tf_t / peak,
+                                      "flop_per_sample": 6 * MLP_MAC, "peak_source": src}}}
 
 
 # ---------------------------------------------------------------------------
@@ -540,10 +626,15 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
-    if args.impl == "reference":
+    if args.only_surrogate:
+        res = run_surrogate(int(os.environ.get("LOCAL_RANK", "0")), args.steps, args.warmup)
+    elif args.impl == "reference":
         res = run_reference(args, rank, world)
     else:
         res, wl = run_ours(args, rank, world, dist)
+        if res is not None and not args.no_surrogate:
+            res["surrogate"] = run_surrogate(int(os.environ.get("LOCAL_RANK", "0")),
+                                             args.steps, args.warmup)
         if res is not None and not args.no_cpu:
             res["cpu_baseline"] = (cpu_compat_rate(wl) if args.form == "compat"
                                    else cpu_physics_rate(wl))

@@ -4,16 +4,34 @@
 // 16).  BF16 weights and activations, FP32 accumulation in tensor memory,
 // FP32 master weights and Adam moments in global memory.
 //
-// One persistent CTA of 128 threads (a warpgroup) per SM walks 128-sample
-// tiles.  Every layer is one tcgen05 tile GEMM (tc.cuh): activations are the
-// A operand ([sample][feature], K-major), weights [out][in] the B operand.
-// Backward re-computes what it needs (all activations do not fit in shared
-// memory next to the weights) and forms
+// Every layer is one 128-sample tcgen05 tile GEMM (tc.cuh): activations are
+// the A operand ([sample][feature], K-major), weights [out][in] the B
+// operand, the FP32 accumulator 128 TMEM columns.  A team of 8 warps owns a
+// tile: warp w reads TMEM lane quarter (w mod 4) -- the quarter a warp may
+// access is fixed by its warp index -- and column half (w / 4), so the
+// epilogue of a layer (bias, SiLU, BF16 store) is spread over 256 threads.
+//
+// Inference: two teams per CTA work on two tiles at once, each with its own
+// mbarrier, TMEM columns and activation buffer (a layer's output overwrites
+// its input once the MMA that read it has completed), so one team's MMAs run
+// while the other team is in its epilogue.  Each thread loads its inputs of
+// the next tile while the current one is computed.
+//
+// Training: one team per CTA.  Backward re-computes what it needs (all
+// activations do not fit in shared memory next to the weights) and forms
 //   dW_l = dZ_l^T H_{l-1}   (A = dZ MN-major view, B = H MN-major view)
 //   dH_{l-1} = dZ_l W_l      (A = dZ K-major, B = W MN-major view)
 // Each CTA accumulates gradients into its own slice of a global buffer
-// (plain read-modify-write, no atomics); a reduction over the slices in a
-// fixed order and an Adam step follow, so training is deterministic.
+// (plain read-modify-write, no atomics); bias gradients are reduced across
+// a warp by a butterfly transpose-sum and across warps in a fixed order; a
+// reduction over the slices in a fixed order and an Adam step follow, so
+// training is deterministic.
+//
+// SiLU(z) = z sigma(z) = h + h tanh(h), h = z / 2, with the hardware FP32
+// tanh (tanh.approx.f32, about 2^-11 relative, below the BF16 rounding of
+// the stored activations).  (The packed f16x2 tanh would halve the
+// special-function work of the epilogue, the inference kernel's limiter,
+// but its error is no longer small against BF16.)
 #include <cuda_bf16.h>
 #include <math.h>
 
@@ -38,15 +56,24 @@ constexpr int kSlice = kParams + 16;  // + loss sum and padding
 constexpr int sW1 = 0, sW2 = sW1 + kH * kIn * 2, sW3 = sW2 + kH * kH * 2;
 constexpr int sW4 = sW3 + kH * kH * 2, sW5 = sW4 + kH * kH * 2;
 constexpr int kWBytes = sW5 + kOut * kH * 2;  // 106496
-// shared memory map
+constexpr int kTeam = 256;                    // threads of a team
+constexpr int kXBytes = kTile * kIn * 2, kHBytes = kTile * kH * 2;
+// biases in shared memory: half biases of layers 1-4 (the SiLU argument is
+// h = (z + b) / 2), then b5
+constexpr int kBiasBytes = (4 * kH + kOut) * 4;  // 2112
+// training shared memory map
 constexpr int sX = kWBytes;                   // [128][16] bf16
-constexpr int sH0 = sX + kTile * kIn * 2;     // [128][128] bf16
-constexpr int sH1 = sH0 + kTile * kH * 2;
-constexpr int sG = sH1 + kTile * kH * 2;      // dZ, [128][128] or [128][16]
-constexpr int sBias = sG + kTile * kH * 2;    // fp32 biases (4*128 + 16)
-constexpr int sDb = sBias + (4 * kH + kOut) * 4;  // fp32 bias-gradient partials [4 warps][128]
-constexpr int sLoss = sDb + 4 * kH * 4;       // fp32 loss partials [4 warps]
-constexpr int kSmem = sLoss + 16;             // 214,096 bytes
+constexpr int sH0 = sX + kXBytes;             // [128][128] bf16
+constexpr int sH1 = sH0 + kHBytes;
+constexpr int sG = sH1 + kHBytes;             // dZ, [128][128] or [128][16]
+constexpr int sBias = sG + kHBytes;
+constexpr int sDb = sBias + kBiasBytes;       // fp32 bias-gradient partials [4 quarters][128]
+constexpr int sLoss = sDb + 4 * kH * 4;       // fp32 loss partials [8 warps]
+constexpr int kSmem = sLoss + 32;             // 214,112 bytes
+// inference shared memory map: weights, biases, then per team X and H
+constexpr int fBias = kWBytes;
+constexpr int fTeam0 = fBias + 2304;
+constexpr int kFwdSmem = fTeam0 + 2 * (kXBytes + kHBytes);  // 182,528 bytes
 
 struct MlpTileArgs {
   float in_scale[5], in_shift[5];  // features = (raw - shift) * scale
@@ -54,10 +81,17 @@ struct MlpTileArgs {
   float inv_batch;
 };
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
-__device__ __forceinline__ float silu_grad(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
-  return s * (1.0f + z * (1.0f - s));
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+// h = (z + b) / 2 -> SiLU(z + b)
+__device__ __forceinline__ float silu_h(float h) { return fmaf(h, tanh_hw(h), h); }
+// SiLU'(u) = s (1 + u (1 - s)), s = sigma(u) = (1 + tanh(u / 2)) / 2, h = u / 2
+__device__ __forceinline__ float silu_grad_h(float h) {
+  const float s = fmaf(0.5f, tanh_hw(h), 0.5f);
+  return s * fmaf(2.0f * h, 1.0f - s, 1.0f);
 }
 
 // 8 bf16 of row r, columns c..c+7 of a K-major core-matrix buffer (rowlen K).
@@ -68,20 +102,58 @@ __device__ __forceinline__ void st_row8(uint8_t *buf, int r, int c, int K, const
   *reinterpret_cast<uint4 *>(buf + tc::kmaj_off(r, c, K)) = *reinterpret_cast<uint4 *>(p);
 }
 
+// A group of threads synchronised by its own named barrier.
+struct Team {
+  uint32_t id, nthr;
+  __device__ __forceinline__ void sync() const {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthr) : "memory");
+  }
+  // true on every thread of the team if p is true on any
+  __device__ __forceinline__ bool any(bool p) const {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(id), "r"(nthr)
+        : "memory");
+    return r != 0;
+  }
+};
+
+// Position of a team thread: TMEM lane quarter, column half, tile row.
+struct Role {
+  int lane, quarter, half, row;
+  uint32_t lane_base;  // TMEM address bits of the quarter's first lane
+  __device__ __forceinline__ explicit Role(int t) {
+    const int w = t >> 5;
+    lane = t & 31;
+    quarter = w & 3;
+    half = w >> 2;
+    row = quarter * 32 + lane;
+    lane_base = (uint32_t)(quarter * 32) << 16;
+  }
+};
+
 struct Gemm {
+  Team team;
   uint64_t *bar;
   uint32_t phase;
   int *err;
+  bool leader;
   // D (TMEM) = A * B^T.  a/b: core-matrix buffers with storage row length
   // a_len/b_len; *_mn = 1 reads the buffer transposed (MN-major).  K: the
-  // reduction length.  All threads call; thread 0 issues.
-  __device__ bool run(uint32_t d, const uint8_t *a, int a_len, int a_mn, const uint8_t *b,
-                      int b_len, int b_mn, int N, int K) {
+  // reduction length.  Every team thread calls; the leader issues.  The
+  // result is the same on every thread: false if the wait gave up.
+  __device__ __forceinline__ bool run(uint32_t d, const uint8_t *a, int a_len, int a_mn,
+                                      const uint8_t *b, int b_len, int b_mn, int N, int K) {
     tc::fence_smem_to_async();
     tc::fence_before_sync();
-    __syncthreads();
+    team.sync();
     tc::fence_after_sync();
-    if (threadIdx.x == 0) {
+    if (leader) {
       const uint32_t a_lbo = a_mn ? (a_len / 8) * 128 : 128, a_sbo = a_mn ? 128 : (a_len / 8) * 128;
       const uint32_t b_lbo = b_mn ? (b_len / 8) * 128 : 128, b_sbo = b_mn ? 128 : (b_len / 8) * 128;
       tc::gemm_issue(d, tc::smem_u32(a), a_lbo, a_sbo, a_mn ? 2 * a_lbo : 256, tc::smem_u32(b),
@@ -90,234 +162,349 @@ struct Gemm {
     }
     const bool timed_out = !tc::mbar_wait(bar, phase, 1u << 30);
     phase ^= 1u;
-    // one decision for the whole CTA, so that every thread leaves together
-    const bool ok = !__syncthreads_or(timed_out);
-    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+    const bool ok = !team.any(timed_out);
+    if (!ok && leader) atomicExch(err, 1);
     tc::fence_after_sync();
     return ok;
   }
 };
 
-// Row r of the accumulator, 16 columns at col.
-__device__ __forceinline__ void acc_row16(uint32_t acc, int col, float *v) {
-  const int warp = threadIdx.x >> 5;
-  tc::tmem_ld16(acc + ((uint32_t)(warp * 32) << 16) + col, v);
-}
-
-// Z = A W^T (acc) then H = SiLU(Z + b) into hout ([128][128] bf16).
-__device__ __forceinline__ bool layer_fwd(Gemm &g, uint32_t acc, const uint8_t *a, int a_len,
-                                          const uint8_t *w, const float *bias, uint8_t *hout) {
-  if (!g.run(acc, a, a_len, 0, w, a_len, 0, kH, a_len)) return false;
-  const int r = threadIdx.x;
-  for (int c = 0; c < kH; c += 16) {
-    float v[16];
-    acc_row16(acc, c, v);
+// 64 accumulator columns [c0, c0+64) of this thread's row.
+__device__ __forceinline__ void acc_ld64(uint32_t acc, const Role &ro, int c0, float *v) {
+  uint32_t r[64];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = silu(v[j] + bias[c + j]);
-    st_row8(hout, r, c, kH, v);
-    st_row8(hout, r, c + 8, kH, v + 8);
-  }
-  return true;
+  for (int k = 0; k < 4; ++k) tc::tmem_ld16_nowait(acc + ro.lane_base + c0 + 16 * k, r + 16 * k);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) tc::tmem_wait_ld_dep16(r + 16 * k);
+#pragma unroll
+  for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void acc_ld16(uint32_t acc, const Role &ro, int c0, float *v) {
+  tc::tmem_ld16(acc + ro.lane_base + c0, v);
 }
 
-// Forward of one tile from sX: H1..H4 alternate in sH0/sH1 (H4 in sH1),
-// outputs y[2] of this thread's sample.
-__device__ __forceinline__ bool forward(Gemm &g, uint32_t acc0, uint32_t acc1, uint8_t *sm,
-                                        float y[2]) {
-  const float *bias = reinterpret_cast<const float *>(sm + sBias);
-  if (!layer_fwd(g, acc0, sm + sX, kIn, sm + sW1, bias + 0 * kH, sm + sH0)) return false;
-  if (!layer_fwd(g, acc0, sm + sH0, kH, sm + sW2, bias + 1 * kH, sm + sH1)) return false;
-  if (!layer_fwd(g, acc0, sm + sH1, kH, sm + sW3, bias + 2 * kH, sm + sH0)) return false;
-  if (!layer_fwd(g, acc0, sm + sH0, kH, sm + sW4, bias + 3 * kH, sm + sH1)) return false;
-  if (!g.run(acc1, sm + sH1, kH, 0, sm + sW5, kH, 0, kOut, kH)) return false;
-  float v[16];
-  acc_row16(acc1, 0, v);
-  y[0] = v[0] + bias[4 * kH + 0];
-  y[1] = v[1] + bias[4 * kH + 1];
-  return true;
+// H = SiLU(acc + b) for this thread's 64 columns, into a [128][128] buffer.
+__device__ __forceinline__ void epi_silu(uint32_t acc, const Role &ro, const float *hb,
+                                         uint8_t *hout) {
+  const int c0 = ro.half * 64;
+  float v[64];
+  acc_ld64(acc, ro, c0, v);
+#pragma unroll
+  for (int i = 0; i < 64; ++i) v[i] = silu_h(fmaf(0.5f, v[i], hb[c0 + i]));
+#pragma unroll
+  for (int k = 0; k < 8; ++k) st_row8(hout, ro.row, c0 + 8 * k, kH, v + 8 * k);
 }
 
-// Copy weights (bf16 images) and biases into shared memory.
-__device__ __forceinline__ void load_weights(uint8_t *sm, const uint8_t *__restrict__ wimg,
-                                             const float *__restrict__ params) {
-  const uint4 *src = reinterpret_cast<const uint4 *>(wimg);
-  uint4 *dst = reinterpret_cast<uint4 *>(sm);
-  for (int i = threadIdx.x; i < kWBytes / 16; i += blockDim.x) dst[i] = src[i];
-  float *bias = reinterpret_cast<float *>(sm + sBias);
-  for (int i = threadIdx.x; i < kH; i += blockDim.x) {
-    bias[i] = params[oB1 + i];
-    bias[kH + i] = params[oB2 + i];
-    bias[2 * kH + i] = params[oB3 + i];
-    bias[3 * kH + i] = params[oB4 + i];
-  }
-  if (threadIdx.x < kOut) bias[4 * kH + threadIdx.x] = params[oB5 + threadIdx.x];
-}
-
-// Normalised features of sample r into the X tile (zero padding to 16).
-__device__ __forceinline__ void put_x(uint8_t *sm, int r, const float *raw,
-                                      const MlpTileArgs &ta, bool live) {
+// Normalised features of one sample into the X tile (zero padding to 16).
+__device__ __forceinline__ void put_raw(uint8_t *sx, int row, const float *raw, bool live,
+                                        const MlpTileArgs &ta) {
   float v[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) v[j] = 0.0f;
   if (live)
 #pragma unroll
     for (int j = 0; j < 5; ++j) v[j] = (raw[j] - ta.in_shift[j]) * ta.in_scale[j];
-  st_row8(sm + sX, r, 0, kIn, v);
-  st_row8(sm + sX, r, 8, kIn, v + 8);
+  st_row8(sx, row, 0, kIn, v);
+  st_row8(sx, row, 8, kIn, v + 8);
+}
+__device__ __forceinline__ void load_raw(const float *__restrict__ x, int s, bool live,
+                                         float *raw) {
+#pragma unroll
+  for (int j = 0; j < 5; ++j) raw[j] = live ? __ldg(x + (size_t)s * 5 + j) : 0.0f;
+}
+__device__ __forceinline__ void put_x(uint8_t *sx, int row, const float *__restrict__ x, int s,
+                                      bool live, const MlpTileArgs &ta) {
+  float raw[5];
+  load_raw(x, s, live, raw);
+  put_raw(sx, row, raw, live, ta);
 }
 
-// dZ = dH (acc1) * SiLU'(Z + b) (Z in acc0) into sG; bias-gradient partials
-// of this warp's 32 samples into its own row of sDb (no atomics: the order
-// of every sum is fixed).
-__device__ __forceinline__ void dz_epilogue(uint32_t acc0, uint32_t acc1, const float *bias,
-                                            uint8_t *sm, bool live) {
-  const int r = threadIdx.x, lane = r & 31;
-  float *db = reinterpret_cast<float *>(sm + sDb) + (r >> 5) * kH;
-  for (int c = 0; c < kH; c += 16) {
-    float z[16], d[16];
-    acc_row16(acc0, c, z);
-    acc_row16(acc1, c, d);
-#pragma unroll
-    for (int j = 0; j < 16; ++j) d[j] = live ? d[j] * silu_grad(z[j] + bias[c + j]) : 0.0f;
-    st_row8(sm + sG, r, c, kH, d);
-    st_row8(sm + sG, r, c + 8, kH, d + 8);
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      float s = d[j];
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) db[c + j] = s;
-    }
+// Copy weights (bf16 images) and biases (half biases for layers 1-4).
+__device__ __forceinline__ void load_weights(uint8_t *sm, float *bias,
+                                             const uint8_t *__restrict__ wimg,
+                                             const float *__restrict__ params) {
+  const uint4 *src = reinterpret_cast<const uint4 *>(wimg);
+  uint4 *dst = reinterpret_cast<uint4 *>(sm);
+  for (int i = threadIdx.x; i < kWBytes / 16; i += blockDim.x) dst[i] = src[i];
+  for (int i = threadIdx.x; i < kH; i += blockDim.x) {
+    bias[i] = 0.5f * params[oB1 + i];
+    bias[kH + i] = 0.5f * params[oB2 + i];
+    bias[2 * kH + i] = 0.5f * params[oB3 + i];
+    bias[3 * kH + i] = 0.5f * params[oB4 + i];
   }
+  if (threadIdx.x < kOut) bias[4 * kH + threadIdx.x] = params[oB5 + threadIdx.x];
 }
 
-// this CTA's gradient slice: add a [rows][cols] accumulator tile (row = TMEM
-// lane).  transpose: the accumulator holds W^T (rows = in, cols = out).
-__device__ __forceinline__ void add_grad(uint32_t acc, int ncols, float *gs, int off,
-                                         int row_len, bool transpose) {
-  const int r = threadIdx.x;
-  for (int c = 0; c < ncols; c += 16) {
-    float v[16];
-    acc_row16(acc, c, v);
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      float *p = transpose ? gs + off + (c + j) * row_len + r : gs + off + r * row_len + c + j;
-      *p += v[j];
-    }
+// ---------------------------------------------------------------------------
+// inference: y[n][2] from x[n][5]; two teams of 256 threads per CTA
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(2 * kTeam, 1)
+    k_mlp_forward(const uint8_t *__restrict__ wimg, const float *__restrict__ params,
+                  const float *__restrict__ x, int nsamp, MlpTileArgs ta, float *__restrict__ y,
+                  int *err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  __shared__ uint64_t bars[2];
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, team_id = tid / kTeam, t = tid % kTeam;
+  if (tid < 32) tc::tmem_alloc(&tslot, 256);
+  if (tid == 0) {
+    tc::mbar_init(&bars[0], 1);
+    tc::mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-}
-
-// add the four warps' bias partials (in warp order) to the gradient slice
-__device__ __forceinline__ void flush_db(uint8_t *sm, float *gs, int off, int n) {
+  float *bias = reinterpret_cast<float *>(sm + fBias);
+  load_weights(sm, bias, wimg, params);
+  tc::fence_before_sync();
   __syncthreads();
+  tc::fence_after_sync();
+  const Role ro(t);
+  uint8_t *sx = sm + fTeam0 + team_id * (kXBytes + kHBytes), *sh = sx + kXBytes;
+  const uint32_t acc = tslot + 128 * team_id;
+  Gemm g{Team{1u + team_id, kTeam}, &bars[team_id], 0u, err, t == 0};
+  const int ntiles = (nsamp + kTile - 1) / kTile;
+  // this thread's inputs of its next tile, loaded one tile ahead
+  float raw[5];
+  {
+    const int s0 = (2 * blockIdx.x + team_id) * kTile + ro.row;
+    load_raw(x, s0, ro.half == 0 && s0 < nsamp, raw);
+  }
+  for (int tile = 2 * blockIdx.x + team_id; tile < ntiles; tile += 2 * gridDim.x) {
+    const int s = tile * kTile + ro.row;
+    const bool live = s < nsamp;
+    if (ro.half == 0) {
+      put_raw(sx, ro.row, raw, live, ta);
+      const int sn = s + 2 * gridDim.x * kTile;
+      load_raw(x, sn, sn < nsamp, raw);
+    }
+    if (!g.run(acc, sx, kIn, 0, sm + sW1, kIn, 0, kH, kIn)) break;
+    epi_silu(acc, ro, bias, sh);
+    bool ok = true;
+    for (int l = 1; l < 4 && ok; ++l) {
+      ok = g.run(acc, sh, kH, 0, sm + sW2 + (l - 1) * kH * kH * 2, kH, 0, kH, kH);
+      if (ok) epi_silu(acc, ro, bias + l * kH, sh);
+    }
+    if (!ok || !g.run(acc, sh, kH, 0, sm + sW5, kH, 0, kOut, kH)) break;
+    if (ro.half == 0) {
+      float v[16];
+      acc_ld16(acc, ro, 0, v);
+      if (live) {
+        y[(size_t)s * 2] = v[0] + bias[4 * kH];
+        y[(size_t)s * 2 + 1] = v[1] + bias[4 * kH + 1];
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid < 32) tc::tmem_free(tslot, 256);
+}
+
+// ---------------------------------------------------------------------------
+// training
+// ---------------------------------------------------------------------------
+// Butterfly transpose-sum of 64 per-lane values over the warp: afterwards
+// lane l holds in v[0], v[1] the sums of columns 2l and 2l+1 (fixed order).
+template <int O, int N>
+__device__ __forceinline__ void xsum_step(float *v, int lane) {
+  const bool up = (lane & O) != 0;
+#pragma unroll
+  for (int i = 0; i < N / 2; ++i) {
+    const float send = up ? v[i] : v[i + N / 2];
+    const float keep = up ? v[i + N / 2] : v[i];
+    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+  }
+}
+__device__ __forceinline__ void xsum64(float *v, int lane) {
+  xsum_step<16, 64>(v, lane);
+  xsum_step<8, 32>(v, lane);
+  xsum_step<4, 16>(v, lane);
+  xsum_step<2, 8>(v, lane);
+  xsum_step<1, 4>(v, lane);
+}
+
+// dZ = dH (acc1) * SiLU'(Z + b) (Z in acc0) into sG for this thread's 64
+// columns; this warp's bias-gradient partials (its 32 rows) into
+// sDb[quarter][column].
+__device__ __forceinline__ void dz_epilogue(uint32_t acc0, uint32_t acc1, const Role &ro,
+                                            const float *hb, uint8_t *sm, bool live) {
+  const int c0 = ro.half * 64;
+  float d[64];
+  {
+    float z[64];
+    acc_ld64(acc0, ro, c0, z);
+    acc_ld64(acc1, ro, c0, d);
+#pragma unroll
+    for (int i = 0; i < 64; ++i)
+      d[i] = live ? d[i] * silu_grad_h(fmaf(0.5f, z[i], hb[c0 + i])) : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) st_row8(sm + sG, ro.row, c0 + 8 * k, kH, d + 8 * k);
+  xsum64(d, ro.lane);
+  float *db = reinterpret_cast<float *>(sm + sDb) + ro.quarter * kH + c0 + 2 * ro.lane;
+  db[0] = d[0];
+  db[1] = d[1];
+}
+
+// add the four quarters' bias partials (in order) to the gradient slice
+__device__ __forceinline__ void flush_db(const Team &team, uint8_t *sm, float *gs, int off,
+                                         int n) {
+  team.sync();
   const float *db = reinterpret_cast<const float *>(sm + sDb);
   for (int i = threadIdx.x; i < n; i += blockDim.x)
     gs[off + i] += ((db[i] + db[kH + i]) + db[2 * kH + i]) + db[3 * kH + i];
-  __syncthreads();
+  team.sync();
 }
 
-// ---------------------------------------------------------------------------
-// training: gradients of the weighted MSE over nsamp samples
+// dW [128 out][128 in] tile (rows = TMEM lanes) into the slice, this
+// thread's row and 64 columns.
+__device__ __forceinline__ void add_grad128(uint32_t acc, const Role &ro, float *gs, int off) {
+  const int c0 = ro.half * 64;
+  float v[64];
+  acc_ld64(acc, ro, c0, v);
+  float4 *p = reinterpret_cast<float4 *>(gs + off + ro.row * kH + c0);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    float4 q = p[k];
+    q.x += v[4 * k];
+    q.y += v[4 * k + 1];
+    q.z += v[4 * k + 2];
+    q.w += v[4 * k + 3];
+    p[k] = q;
+  }
+}
+
 // x: [n][5], t: [n][2]; grads: [gridDim.x][kSlice] (slice zeroed here)
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kTeam, 1)
     k_mlp_grad(const uint8_t *__restrict__ wimg, const float *__restrict__ params,
                const float *__restrict__ x, const float *__restrict__ t, int nsamp,
                MlpTileArgs ta, float *__restrict__ grads, int *err) {
   extern __shared__ __align__(1024) uint8_t sm[];
   __shared__ uint64_t bar;
   __shared__ uint32_t tslot;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x;
   float *gs = grads + (size_t)blockIdx.x * kSlice;
   for (int i = tid; i < kSlice; i += blockDim.x) gs[i] = 0.0f;
-  if (warp == 0) tc::tmem_alloc(&tslot, 256);
+  if (tid < 32) tc::tmem_alloc(&tslot, 256);
   if (tid == 0) {
     tc::mbar_init(&bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  load_weights(sm, wimg, params);
+  float *bias = reinterpret_cast<float *>(sm + sBias);
+  load_weights(sm, bias, wimg, params);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t acc0 = tslot, acc1 = tslot + 128;
-  Gemm g{&bar, 0u, err};
-  const float *bias = reinterpret_cast<const float *>(sm + sBias);
+  const Role ro(tid);
+  const Team team{1u, kTeam};
+  Gemm g{team, &bar, 0u, err, tid == 0};
   float loss = 0.0f;
   const int ntiles = (nsamp + kTile - 1) / kTile;
   bool ok = true;
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int s = tile * kTile + tid;
+    const int s = tile * kTile + ro.row;
     const bool live = s < nsamp;
-    float raw[5] = {0, 0, 0, 0, 0};
-    if (live)
-      for (int j = 0; j < 5; ++j) raw[j] = x[(size_t)s * 5 + j];
-    put_x(sm, tid, raw, ta, live);
-    const float tg0 = live ? t[(size_t)s * 2] : 0.0f, tg1 = live ? t[(size_t)s * 2 + 1] : 0.0f;
-    float y[2];
-    if (!(ok = forward(g, acc0, acc1, sm, y))) break;
-    // loss and dZ5 = dY (2 live columns of a [128][16] tile in sG)
-    float d5[16];
+    if (ro.half == 0) put_x(sm + sX, ro.row, x, s, live, ta);
+    // forward: H1 sH0, H2 sH1, H3 sH0, H4 sH1
+    if (!(ok = g.run(acc0, sm + sX, kIn, 0, sm + sW1, kIn, 0, kH, kIn))) break;
+    epi_silu(acc0, ro, bias, sm + sH0);
+    if (!(ok = g.run(acc0, sm + sH0, kH, 0, sm + sW2, kH, 0, kH, kH))) break;
+    epi_silu(acc0, ro, bias + kH, sm + sH1);
+    if (!(ok = g.run(acc0, sm + sH1, kH, 0, sm + sW3, kH, 0, kH, kH))) break;
+    epi_silu(acc0, ro, bias + 2 * kH, sm + sH0);
+    if (!(ok = g.run(acc0, sm + sH0, kH, 0, sm + sW4, kH, 0, kH, kH))) break;
+    epi_silu(acc0, ro, bias + 3 * kH, sm + sH1);
+    if (!(ok = g.run(acc1, sm + sH1, kH, 0, sm + sW5, kH, 0, kOut, kH))) break;
+    // loss and dZ5 = dY ([128][16] tile in sG, 2 live columns)
+    if (ro.half == 0) {
+      float v[16], d5[16];
+      acc_ld16(acc1, ro, 0, v);
 #pragma unroll
-    for (int j = 0; j < 16; ++j) d5[j] = 0.0f;
-    if (live) {
-      const float e0 = y[0] - tg0, e1 = y[1] - tg1;
-      loss += ta.w_out[0] * e0 * e0 + ta.w_out[1] * e1 * e1;
-      d5[0] = 2.0f * ta.w_out[0] * e0 * ta.inv_batch;
-      d5[1] = 2.0f * ta.w_out[1] * e1 * ta.inv_batch;
-    }
-    st_row8(sm + sG, tid, 0, kOut, d5);
-    st_row8(sm + sG, tid, 8, kOut, d5 + 8);
-    {  // db5 partials of this warp (columns 0 and 1; the rest stay zero)
-      float *db = reinterpret_cast<float *>(sm + sDb) + warp * kH;
-      for (int j = 0; j < kOut; ++j) {
-        float v = d5[j];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((tid & 31) == 0) db[j] = v;
+      for (int j = 0; j < 16; ++j) d5[j] = 0.0f;
+      if (live) {
+        const float e0 = v[0] + bias[4 * kH] - t[(size_t)s * 2];
+        const float e1 = v[1] + bias[4 * kH + 1] - t[(size_t)s * 2 + 1];
+        loss += ta.w_out[0] * e0 * e0 + ta.w_out[1] * e1 * e1;
+        d5[0] = 2.0f * ta.w_out[0] * e0 * ta.inv_batch;
+        d5[1] = 2.0f * ta.w_out[1] * e1 * ta.inv_batch;
       }
+      st_row8(sm + sG, ro.row, 0, kOut, d5);
+      st_row8(sm + sG, ro.row, 8, kOut, d5 + 8);
+      float *db = reinterpret_cast<float *>(sm + sDb) + ro.quarter * kH;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        float a = d5[j];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (ro.lane == 0) db[j] = a;
+      }
+      if (ro.lane < kOut - 2) db[2 + ro.lane] = 0.0f;
     }
-    flush_db(sm, gs, oB5, kOut);
+    flush_db(team, sm, gs, oB5, kOut);
     // layer 5: dW5^T = H4^T dZ5 (rows = in), dH4 = dZ5 W5
     if (!(ok = g.run(acc0, sm + sH1, kH, 1, sm + sG, kOut, 1, kOut, kTile))) break;
-    add_grad(acc0, kOut, gs, oW5, kH, true);
+    if (ro.half == 0) {
+      float v[16];
+      acc_ld16(acc0, ro, 0, v);
+#pragma unroll
+      for (int j = 0; j < kOut; ++j) gs[oW5 + j * kH + ro.row] += v[j];
+    }
     if (!(ok = g.run(acc1, sm + sG, kOut, 0, sm + sW5, kH, 1, kH, kOut))) break;
     // layer 4: Z4 = H3 W4^T (H3 still in sH0)
     if (!(ok = g.run(acc0, sm + sH0, kH, 0, sm + sW4, kH, 0, kH, kH))) break;
-    dz_epilogue(acc0, acc1, bias + 3 * kH, sm, live);
-    flush_db(sm, gs, oB4, kH);
+    dz_epilogue(acc0, acc1, ro, bias + 3 * kH, sm, live);
+    flush_db(team, sm, gs, oB4, kH);
     if (!(ok = g.run(acc0, sm + sG, kH, 1, sm + sH0, kH, 1, kH, kTile))) break;
-    add_grad(acc0, kH, gs, oW4, kH, false);
+    add_grad128(acc0, ro, gs, oW4);
     if (!(ok = g.run(acc1, sm + sG, kH, 0, sm + sW4, kH, 1, kH, kH))) break;
     // layer 3: recompute H1 (sH1), H2 (sH0), Z3
-    if (!(ok = layer_fwd(g, acc0, sm + sX, kIn, sm + sW1, bias, sm + sH1))) break;
-    if (!(ok = layer_fwd(g, acc0, sm + sH1, kH, sm + sW2, bias + kH, sm + sH0))) break;
+    if (!(ok = g.run(acc0, sm + sX, kIn, 0, sm + sW1, kIn, 0, kH, kIn))) break;
+    epi_silu(acc0, ro, bias, sm + sH1);
+    if (!(ok = g.run(acc0, sm + sH1, kH, 0, sm + sW2, kH, 0, kH, kH))) break;
+    epi_silu(acc0, ro, bias + kH, sm + sH0);
     if (!(ok = g.run(acc0, sm + sH0, kH, 0, sm + sW3, kH, 0, kH, kH))) break;
-    dz_epilogue(acc0, acc1, bias + 2 * kH, sm, live);
-    flush_db(sm, gs, oB3, kH);
+    dz_epilogue(acc0, acc1, ro, bias + 2 * kH, sm, live);
+    flush_db(team, sm, gs, oB3, kH);
     if (!(ok = g.run(acc0, sm + sG, kH, 1, sm + sH0, kH, 1, kH, kTile))) break;
-    add_grad(acc0, kH, gs, oW3, kH, false);
+    add_grad128(acc0, ro, gs, oW3);
     if (!(ok = g.run(acc1, sm + sG, kH, 0, sm + sW3, kH, 1, kH, kH))) break;
     // layer 2: H1 in sH1, recompute Z2
     if (!(ok = g.run(acc0, sm + sH1, kH, 0, sm + sW2, kH, 0, kH, kH))) break;
-    dz_epilogue(acc0, acc1, bias + kH, sm, live);
-    flush_db(sm, gs, oB2, kH);
+    dz_epilogue(acc0, acc1, ro, bias + kH, sm, live);
+    flush_db(team, sm, gs, oB2, kH);
     if (!(ok = g.run(acc0, sm + sG, kH, 1, sm + sH1, kH, 1, kH, kTile))) break;
-    add_grad(acc0, kH, gs, oW2, kH, false);
+    add_grad128(acc0, ro, gs, oW2);
     if (!(ok = g.run(acc1, sm + sG, kH, 0, sm + sW2, kH, 1, kH, kH))) break;
     // layer 1: recompute Z1 from X
     if (!(ok = g.run(acc0, sm + sX, kIn, 0, sm + sW1, kIn, 0, kH, kIn))) break;
-    dz_epilogue(acc0, acc1, bias, sm, live);
-    flush_db(sm, gs, oB1, kH);
+    dz_epilogue(acc0, acc1, ro, bias, sm, live);
+    flush_db(team, sm, gs, oB1, kH);
     if (!(ok = g.run(acc0, sm + sG, kH, 1, sm + sX, kIn, 1, kIn, kTile))) break;
-    add_grad(acc0, kIn, gs, oW1, kIn, false);
+    if (ro.half == 0) {
+      float v[16];
+      acc_ld16(acc0, ro, 0, v);
+      float4 *p = reinterpret_cast<float4 *>(gs + oW1 + ro.row * kIn);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        float4 q = p[k];
+        q.x += v[4 * k];
+        q.y += v[4 * k + 1];
+        q.z += v[4 * k + 2];
+        q.w += v[4 * k + 3];
+        p[k] = q;
+      }
+    }
   }
   // loss sum of this CTA, in warp order
   for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
   float *ls = reinterpret_cast<float *>(sm + sLoss);
-  if ((tid & 31) == 0) ls[warp] = loss;
-  __syncthreads();
-  if (tid == 0) gs[kParams] = (((ls[0] + ls[1]) + ls[2]) + ls[3]) * ta.inv_batch;
+  if (ro.lane == 0) ls[tid >> 5] = loss;
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_free(tslot, 256);
+  if (tid == 0) {
+    float a = 0.0f;
+    for (int w = 0; w < kTeam / 32; ++w) a += ls[w];
+    gs[kParams] = a * ta.inv_batch;
+  }
+  if (tid < 32) tc::tmem_free(tslot, 256);
 }
 
 // Sum the per-CTA slices in a fixed order.
@@ -367,49 +554,8 @@ __global__ void k_mlp_adam(float *__restrict__ p, float *__restrict__ m, float *
   }
 }
 
-// ---------------------------------------------------------------------------
-// inference: y[n][2] from x[n][5]
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 1)
-    k_mlp_forward(const uint8_t *__restrict__ wimg, const float *__restrict__ params,
-                  const float *__restrict__ x, int nsamp, MlpTileArgs ta, float *__restrict__ y,
-                  int *err) {
-  extern __shared__ __align__(1024) uint8_t sm[];
-  __shared__ uint64_t bar;
-  __shared__ uint32_t tslot;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  if (warp == 0) tc::tmem_alloc(&tslot, 256);
-  if (tid == 0) {
-    tc::mbar_init(&bar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  load_weights(sm, wimg, params);
-  tc::fence_before_sync();
-  __syncthreads();
-  tc::fence_after_sync();
-  const uint32_t acc0 = tslot, acc1 = tslot + 128;
-  Gemm g{&bar, 0u, err};
-  const int ntiles = (nsamp + kTile - 1) / kTile;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int s = tile * kTile + tid;
-    const bool live = s < nsamp;
-    float raw[5] = {0, 0, 0, 0, 0};
-    if (live)
-      for (int j = 0; j < 5; ++j) raw[j] = x[(size_t)s * 5 + j];
-    put_x(sm, tid, raw, ta, live);
-    float out[2];
-    if (!forward(g, acc0, acc1, sm, out)) break;
-    if (live) {
-      y[(size_t)s * 2] = out[0];
-      y[(size_t)s * 2 + 1] = out[1];
-    }
-  }
-  tc::fence_before_sync();
-  __syncthreads();
-  if (warp == 0) tc::tmem_free(tslot, 256);
-}
-
 }  // namespace qpsdm
+
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -471,8 +617,8 @@ extern "C" int qpsdm_mlp_create(int device, qpsdm_mlp **out) {
   h->ta.w_out[0] = h->ta.w_out[1] = 1.0f;
   if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) !=
           cudaSuccess ||
-      cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem) !=
-          cudaSuccess) {
+      cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kFwdSmem) != cudaSuccess) {
     qpsdm_mlp_destroy(h);
     return QPSDM_ECUDA;
   }
@@ -547,7 +693,7 @@ extern "C" int qpsdm_mlp_gradients(qpsdm_mlp *h, const float *d_x, const float *
   MlpTileArgs ta = h->ta;
   ta.inv_batch = 1.0f / n;
   const int grid = mlp_grid(h, n);
-  k_mlp_grad<<<grid, 128, kSmem, st>>>(h->wimg, h->p, d_x, d_t, n, ta, h->slices, h->err);
+  k_mlp_grad<<<grid, kTeam, kSmem, st>>>(h->wimg, h->p, d_x, d_t, n, ta, h->slices, h->err);
   k_mlp_reduce<<<64, 256, 0, st>>>(h->slices, grid, h->g);
   if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
     return QPSDM_ECUDA;
@@ -567,7 +713,7 @@ extern "C" int qpsdm_mlp_train_step(qpsdm_mlp *h, const float *d_x, const float 
   MlpTileArgs ta = h->ta;
   ta.inv_batch = 1.0f / n;
   const int grid = mlp_grid(h, n);
-  k_mlp_grad<<<grid, 128, kSmem, st>>>(h->wimg, h->p, d_x, d_t, n, ta, h->slices, h->err);
+  k_mlp_grad<<<grid, kTeam, kSmem, st>>>(h->wimg, h->p, d_x, d_t, n, ta, h->slices, h->err);
   k_mlp_reduce<<<64, 256, 0, st>>>(h->slices, grid, h->g);
   h->step += 1;
   const float b1 = 0.9f, b2 = 0.999f;
@@ -590,8 +736,10 @@ extern "C" int qpsdm_mlp_forward(qpsdm_mlp *h, const float *d_x, int n, float *d
                                  void *stream) {
   if (!h || !d_x || !d_y || n <= 0) return QPSDM_EINVAL;
   cudaSetDevice(h->device);
-  k_mlp_forward<<<mlp_grid(h, n), 128, kSmem, (cudaStream_t)stream>>>(h->wimg, h->p, d_x, n,
-                                                                      h->ta, d_y, h->err);
+  const int pairs = ((n + kTile - 1) / kTile + 1) / 2;
+  const int grid = pairs < h->nsm ? pairs : h->nsm;
+  k_mlp_forward<<<grid, 2 * kTeam, kFwdSmem, (cudaStream_t)stream>>>(h->wimg, h->p, d_x, n,
+                                                                     h->ta, d_y, h->err);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
 
