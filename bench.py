@@ -10,7 +10,7 @@ A point-trace is one (image point, trace) pair inside the trace's aperture;
 the engine counts them on the device.
 
 Forms (a step = one pass over one batch):
-  batched  4 shot gathers (36864 traces) into a brick of 8 image lines; BF16
+  batched  8 shot gathers (73728 traces) into a brick of 8 image lines; BF16
            t* panels computed once per trace and shared by the brick;
            receiver-grouped persistent kernel.  The headline.
   plain    1 shot gather into 1 image line, FP32 panels, launch per shot and
@@ -54,7 +54,7 @@ METRIC = "Gpoint-traces/s, plain vs batched+BF16+surrogate form, at NRMSE<=1e-3 
 # Compat: the stub body of image_depth_gpu (src/q-psdm.cu:2303-2378).
 F_PT = {"batched": 64, "plain": 64, "compat": 35}
 FORMS = {  # shots per step, lines per step, panel dtype, physics form
-    "batched": (4, 8, 1, 1),
+    "batched": (8, 8, 1, 1),
     "plain": (1, 1, 0, 0),
     "compat": (1, 1, 0, None),
 }
