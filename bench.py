@@ -10,14 +10,15 @@ A point-trace is one (image point, trace) pair inside the trace's aperture;
 the engine counts them on the device.
 
 Forms (a step = one pass over one batch):
-  batched  8 shot gathers (73728 traces) into a brick of 8 image lines; BF16
-           t* panels computed once per trace and shared by the brick;
+  batched  8 shot gathers (73728 traces) into a brick of 8 image lines; FP16
+           t* panels (each trace scaled by a power of two into FP16's range)
+           computed once per trace and shared by the brick;
            receiver-grouped persistent kernel.  The headline.
   plain    1 shot gather into 1 image line, FP32 panels, launch per shot and
            per line, as the reference organises its work.
   compat   the reference's own (stub) kernel semantics, 1 shot into 1 line.
 With --form batched the plain form is also timed in the same run and
-reported under "forms" (the north star's plain-vs-batched ratio).
+reported under "forms" with the batched-over-plain ratio.
 
 `value`: records resident in HBM, CUDA events on the engine's stream around
 each step, L2 flushed (256 MiB write) before each step.  `e2e`: the host API
@@ -49,12 +50,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Gpoint-traces/s, plain vs batched+BF16+surrogate form, at NRMSE<=1e-3 vs FP64"
-# FP32 operations per point-trace.  Physics (SURVEY 8d): 42 table
+# FP32 operations per point-trace.  Physics: 42 table
 # interpolation, 14 ray geometry and weights, 6 time/t* pick, 2 accumulate.
 # Compat: the stub body of image_depth_gpu (src/q-psdm.cu:2303-2378).
 F_PT = {"batched": 64, "plain": 64, "compat": 35}
 FORMS = {  # shots per step, lines per step, panel dtype, physics form
-    "batched": (8, 8, 1, 1),
+    "batched": (8, 8, 2, 1),
     "plain": (1, 1, 0, 0),
     "compat": (1, 1, 0, None),
 }
@@ -70,6 +71,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--only-surrogate", action="store_true",
                     help="time only the surrogate network's kernels (for profiling)")
     ap.add_argument("--shots", type=int, default=0,
@@ -384,7 +386,7 @@ def run_ours(args, rank, world, dist):
     res = {"metric": METRIC, "value": head["value"], "unit": "Gpoint-traces/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32 (bf16 panels)" if args.form == "batched" else "f32",
+           "dtype": "f32 (fp16 panels)" if args.form == "batched" else "f32",
            "data": "synthetic", "config": wl.config(args.form), "roofline": roof,
            "e2e": head.get("e2e"), "gpu_launches": head["launches"], "clocks": head["clocks"],
            "point_traces_per_step": head["point_traces_per_step"],
@@ -590,6 +592,53 @@ def cpu_physics_rate(wl, budget_s=10.0):
                       f"the physics method (numpy float64 panels + C imaging), {nthr} threads"}
 
 
+def accuracy_vs_fp64(wl, dev, ntr=1536, seed=2):
+    """NRMSE of the batched-form image and of the plain FP32 image against the
+    FP64 oracle on the same input: a seeded sample of `ntr` traces of the
+    step's first two shot gathers, imaged into the brick's first line."""
+    from oracle import oracle as O
+    from q_psdm_b200 import engine as E
+    sv = wl.sv
+    line = wl.LINE0
+    rec = wl.records(0, 2)
+    rng = np.random.default_rng(seed)
+    rec = np.ascontiguousarray(rec[np.sort(rng.choice(rec.shape[0], ntr, replace=False))])
+    hdr, traces = _hdr_traces(rec)
+    st = O.derive_static(sv.ntl, np.float32(sv.dt), 600.0, 3.0, 8.0)
+    tab = wl.tables()
+    pp = O.PhysParams(nzi=sv.nzi, nxb=sv.nxi, ixstart=0, nt=st["nffti"], nbins=16,
+                      dt1=float(st["dt1"]), dxi=sv.dxi, dzi=sv.dzi,
+                      taperzone=float(st["taperzone"]), dtstar=float(np.float32(0.002)),
+                      dzii=tab.dzii, tcdp1=tab.cdp1 - sv.fci, tcdp2=tab.cdp2 - sv.fci,
+                      nxg=tab.nxg, nzg=tab.nzg, nxi1=tab.nxi1, nzi1=tab.nzi1)
+    filt = O.physics_filter(st["nfft"], np.float32(sv.dt), 130.0, 140.0, 30.0, 600.0, 16, 0.002)
+    dips = [d.ravel() for d in wl.synth.dip_fields(sv.nxi, sv.nzi, float(st["contract"]))]
+    ints, geom = O.gate_traces(_gate_params(O, wl, line), hdr)
+    ok = ints[:, 0] == 3
+    pan = O.physics_panels(traces[ok], np.float32(sv.dt), st["nfft"], st["nffti"], filt)
+    ref, npt = O.physics_image(pp, geom[ok], ints[ok][:, [4, 5, 7]], pan, dips,
+                               tab.as_engine_dict())
+    ref = np.asarray(ref, np.float64).reshape(sv.nxi, sv.nzi)
+    out = {"sample": f"{ntr} seeded traces of 2 config-2 shot gathers into line {line} "
+                     f"({npt} point-traces); FP64 oracle: numpy float64 panels + C imaging"}
+    for form in ("batched", "plain"):
+        p = wl.static(form, max_batch=ntr)
+        eng = E.Engine(p, device=dev)
+        try:
+            eng.set_lines(wl.lines(form, p.contract)[:1])
+            az = wl.aperture()
+            eng.begin_offset(E.offset_params(p, 0, p.nxi, aznx1=az[0], aznx2=az[1],
+                                             azny1=az[2], azny2=az[3]))
+            eng.submit(rec)
+            img = np.asarray(eng.get_image(False), np.float64).reshape(sv.nxi, sv.nzi)
+        finally:
+            eng.close()
+        e = float(np.sqrt(np.mean((img - ref) ** 2)) / np.sqrt(np.mean(ref ** 2)))
+        dt_name = {0: "fp32", 1: "bf16", 2: "fp16"}[FORMS[form][2]]
+        out[f"nrmse_{form}_{dt_name}_panels_vs_fp64"] = e
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -632,6 +681,8 @@ def main():
         res = run_reference(args, rank, world)
     else:
         res, wl = run_ours(args, rank, world, dist)
+        if res is not None and not args.no_accuracy:
+            res["accuracy"] = accuracy_vs_fp64(wl, int(os.environ.get("LOCAL_RANK", "0")))
         if res is not None and not args.no_surrogate:
             res["surrogate"] = run_surrogate(int(os.environ.get("LOCAL_RANK", "0")),
                                              args.steps, args.warmup)

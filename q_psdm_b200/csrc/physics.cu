@@ -26,6 +26,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <cmath>
 #include <cub/cub.cuh>
 #include <vector>
@@ -42,6 +43,8 @@ struct PhysicsState {
   float dtstar = 0.0f;
   float2 *d_filter = nullptr;  // [nbins][nfft/2+1]
   float2 *d_spec = nullptr;    // [max_batch][nfft/2+1]
+  float *d_fmax = nullptr;     // [nfft/2+1] max over bins of |filter|
+  float *d_pscale = nullptr;   // [max_batch] FP16 panels: per-trace sample multiplier
   void *d_panels = nullptr;    // [max_batch][nbins][nffti]
   float *d_comp = nullptr;     // Kahan compensation, [img_cap]
   size_t comp_cap = 0;
@@ -81,7 +84,7 @@ static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p);
 
 // (-i ww_k) * A(pi f t*) * exp(-2 i f t* ln(f/fc)) / nfft for every bin.
 static void filter_table(const qpsdm_static_params &p, int nbins, float dtstar,
-                         std::vector<float2> &out) {
+                         std::vector<float2> &out, std::vector<float> &fmax) {
   const int nk = p.nfft / 2 + 1;
   const double df = 1.0 / ((double)p.nfft * (double)p.dt);
   const double dw = 2.0 * M_PI * df;
@@ -116,6 +119,12 @@ static void filter_table(const qpsdm_static_params &p, int nbins, float dtstar,
       out[(size_t)b * nk + k] = make_float2((float)re, (float)im);
     }
   }
+  fmax.assign(nk, 0.0f);
+  for (int b = 0; b < nbins; ++b)
+    for (int k = 0; k < nk; ++k) {
+      const float2 v = out[(size_t)b * nk + k];
+      fmax[k] = std::max(fmax[k], std::hypot(v.x, v.y) * 1.0001f);
+    }
 }
 
 int physics_create(PhysicsState **out, const qpsdm_static_params &p, std::string *err) {
@@ -128,6 +137,10 @@ int physics_create(PhysicsState **out, const qpsdm_static_params &p, std::string
     if (err) *err = "bad panel dtype";
     return QPSDM_EINVAL;
   }
+  if (p.form == QPSDM_FORM_BATCHED && p.max_batch >= (1 << 24)) {
+    if (err) *err = "batched form: max_batch must be below 2^24 traces";
+    return QPSDM_EINVAL;
+  }
   auto *s = new PhysicsState;
   s->nfft = p.nfft;
   s->nffti = p.nffti;
@@ -136,7 +149,8 @@ int physics_create(PhysicsState **out, const qpsdm_static_params &p, std::string
   s->max_batch = p.max_batch;
   s->dtype = p.panel_dtype;
   std::vector<float2> f;
-  filter_table(p, p.nbins, p.dtstar, f);
+  std::vector<float> fmax;
+  filter_table(p, p.nbins, p.dtstar, f, fmax);
   const size_t nk = (size_t)p.nfft / 2 + 1;
   auto bad = [&](const char *w) {
     if (err) *err = std::string("physics_create: ") + w;
@@ -146,6 +160,9 @@ int physics_create(PhysicsState **out, const qpsdm_static_params &p, std::string
   if (cudaMalloc(&s->d_filter, sizeof(float2) * f.size()) != cudaSuccess) return bad("filter");
   cudaMemcpy(s->d_filter, f.data(), sizeof(float2) * f.size(), cudaMemcpyHostToDevice);
   if (cudaMalloc(&s->d_spec, sizeof(float2) * nk * p.max_batch) != cudaSuccess) return bad("spectra");
+  if (cudaMalloc(&s->d_fmax, sizeof(float) * nk) != cudaSuccess) return bad("filter bound");
+  cudaMemcpy(s->d_fmax, fmax.data(), sizeof(float) * nk, cudaMemcpyHostToDevice);
+  if (cudaMalloc(&s->d_pscale, sizeof(float) * p.max_batch) != cudaSuccess) return bad("scales");
   const size_t pb = dtype_bytes(p.panel_dtype) * (size_t)p.nbins * p.nffti * p.max_batch;
   if (cudaMalloc(&s->d_panels, pb) != cudaSuccess) return bad("panels");
   if (cudaMalloc(&s->d_any, sizeof(int) * p.max_batch) != cudaSuccess) return bad("flags");
@@ -181,6 +198,8 @@ void physics_destroy(PhysicsState *s) {
   cudaFree(s->d_cub);
   cudaFree(s->d_filter);
   cudaFree(s->d_spec);
+  cudaFree(s->d_fmax);
+  cudaFree(s->d_pscale);
   cudaFree(s->d_panels);
   cudaFree(s->d_comp);
   for (auto &t : s->tabs) {
@@ -297,11 +316,19 @@ __device__ __forceinline__ float phys_tapered(float v, int j, int n, const float
   return v;
 }
 
+// Forward spectrum of one trace.  For FP16 panels also the trace's sample
+// multiplier: every panel sample of the trace is bounded by
+// B = 2 sum_k |X_k| max_b |F_b,k| (triangle inequality over the c2r sum), and
+// the panels store x / 2^e with e chosen so that B / 2^e lies in [2^13, 2^14):
+// no overflow of FP16 (max 65504) and no loss to its subnormal range; the
+// image kernels multiply the samples by 2^e again (exact).
 __global__ void __launch_bounds__(256) k_phys_fwd(const uint8_t *__restrict__ rec, int rec_bytes,
                                                   int be, const int *__restrict__ status,
                                                   int sstride, int ntl,
                                                   float dt, const float *__restrict__ tap,
-                                                  FftPlan p, float2 *__restrict__ spec) {
+                                                  FftPlan p, float2 *__restrict__ spec,
+                                                  const float *__restrict__ fmax,
+                                                  float *__restrict__ pscale) {
   const int itr = blockIdx.x;
   if (status[(size_t)itr * sstride] != kAccepted) return;
   extern __shared__ float2 sm[];
@@ -325,7 +352,28 @@ __global__ void __launch_bounds__(256) k_phys_fwd(const uint8_t *__restrict__ re
   const int cur = fft_complex_smem(b0, b1, p, twm, false);
   const float2 *Z = cur ? b1 : b0;
   float2 *o = spec + (size_t)itr * (p.m + 1);
-  for (int k = threadIdx.x; k <= p.m; k += blockDim.x) o[k] = rfft_bin(Z, twn, p.m, k);
+  float bound = 0.0f;
+  for (int k = threadIdx.x; k <= p.m; k += blockDim.x) {
+    const float2 v = rfft_bin(Z, twn, p.m, k);
+    o[k] = v;
+    if (pscale) bound = fmaf(sqrtf(v.x * v.x + v.y * v.y), fmax[k], bound);
+  }
+  if (!pscale) return;
+  __shared__ float s_part[8];
+  for (int off = 16; off > 0; off >>= 1) bound += __shfl_xor_sync(0xffffffffu, bound, off);
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = bound;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float b = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += s_part[w];
+    b *= 2.0f;
+    int e = 0;
+    if (b > 0.0f && isfinite(b)) {
+      frexpf(b, &e);  // b = m 2^e, m in [0.5, 1)
+      e = min(max(e - 14, -126), 127);
+    }
+    pscale[itr] = ldexpf(1.0f, e);
+  }
 }
 
 template <typename T>
@@ -344,7 +392,8 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_phys_panels(const int *__restrict__ status, int sstride,
                                                      const float2 *__restrict__ spec, int nk,
                                                      const float2 *__restrict__ filt, FftPlan p,
-                                                     int nbins, T *__restrict__ panels) {
+                                                     int nbins, T *__restrict__ panels,
+                                                     const float *__restrict__ pscale) {
   const int itr = blockIdx.x, b = blockIdx.y;
   if (status[(size_t)itr * sstride] != kAccepted) return;
   extern __shared__ float2 sm[];
@@ -369,9 +418,11 @@ __global__ void __launch_bounds__(256) k_phys_panels(const int *__restrict__ sta
   const int cur = fft_complex_smem(b0, b1, p, twm, true);
   const float2 *z = cur ? b1 : b0;
   T *out = panels + ((size_t)itr * nbins + b) * p.n;
+  // 2 / 2^e for FP16 (exact), 2 otherwise
+  const float mul = std::is_same<T, __half>::value ? 2.0f / pscale[itr] : 2.0f;
   for (int j = threadIdx.x; j < p.m; j += blockDim.x) {
-    store_sample<T>(out + 2 * j, 2.0f * z[j].x);
-    store_sample<T>(out + 2 * j + 1, 2.0f * z[j].y);
+    store_sample<T>(out + 2 * j, mul * z[j].x);
+    store_sample<T>(out + 2 * j + 1, mul * z[j].y);
   }
 }
 
@@ -531,7 +582,8 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
                   const float *__restrict__ geom, int ntr,
                   const qpsdm_ttt_desc *__restrict__ dt, const float *__restrict__ ttt,
                   const qpsdm_ttt_desc *__restrict__ dq, const float *__restrict__ qqq,
-                  const T *__restrict__ panels, unsigned long long *npt) {
+                  const T *__restrict__ panels, const float *__restrict__ pscale,
+                  unsigned long long *npt) {
   __shared__ float4 s_geom[kPhysChunk];
   __shared__ int4 s_rng[kPhysChunk];
   __shared__ unsigned long long s_cnt;
@@ -621,7 +673,8 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
       const float p00 = ld_sample<T>(pp), p01 = ld_sample<T>(pp + 1);
       const float p10 = ld_sample<T>(pp + a.nt), p11 = ld_sample<T>(pp + a.nt + 1);
       const float s0 = p00 + wt * (p01 - p00), s1 = p10 + wt * (p11 - p10);
-      const float smp = s0 + wb * (s1 - s0);
+      float smp = s0 + wb * (s1 - s0);
+      if (std::is_same<T, __half>::value) smp *= __ldg(pscale + c0 + i);
       // amplitude weight (src/q-psdm.cu:2366-2374)
       const float v = t > 0.1f ? 100.0f / (t * t) : 10000.0f;
       const float r = (ds * rg2) * (ds * rg2) * (ds * rg2) * (tg / ts);
@@ -711,13 +764,19 @@ __global__ void k_batch_groups(const unsigned long long *__restrict__ ukey,
 __global__ void k_batch_members(const uint8_t *__restrict__ rec, int rec_bytes, int be, int ntr,
                                 const int *__restrict__ sval, const int *__restrict__ ints,
                                 const int *__restrict__ sid, const int *__restrict__ srcflag,
-                                double scaled, double fxi, double cyi, int4 *__restrict__ mem,
+                                double scaled, double fxi, double cyi,
+                                const float *__restrict__ pscale, int4 *__restrict__ mem,
                                 float2 *__restrict__ srcpos) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= ntr) return;
   const int j = sval[p];
   const int *q = ints + (size_t)j * kGateInts;
-  mem[p] = q[0] == kAccepted ? make_int4(j, sid[j] - 1, q[4], q[5]) : make_int4(j, -1, 1, 0);
+  // member record: trace, source slot (bits 0-23) with the exponent of the
+  // trace's FP16 sample multiplier + 128 (bits 24-31), cdp range
+  int e = 0;
+  if (pscale && q[0] == kAccepted) e = min(max(ilogbf(pscale[j]), -126), 127);
+  mem[p] = q[0] == kAccepted ? make_int4(j, (sid[j] - 1) | ((e + 128) << 24), q[4], q[5])
+                             : make_int4(j, -1, 1, 0);
   if (srcflag[p]) {  // p as a trace index: first trace of a source run
     const uint8_t *r = rec + (size_t)p * rec_bytes;
     const double sx = __dmul_rn((double)su_i32(r, kOffSx, be), scaled);
@@ -841,7 +900,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
           float tnx[U], tny[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
-            const int sl = mi[u].y - s0;
+            const int sl = (mi[u].y & 0xFFFFFF) - s0;
             const bool inr = sl >= 0 && sl < ns && ixi >= mi[u].z && ixi <= mi[u].w;
             cnt += inr ? 1u : 0u;
             slv[u] = inr ? sl : 0;
@@ -887,6 +946,8 @@ __global__ void __launch_bounds__(TZ *TX, MB)
             const float r = m[kMapCA * sc * NT].x * gfac;
             const bool far = t > 0.1f;
             fac[u] = w * fmaf(r, r, 1.0f) * __fdividef(far ? 100.0f : 10000.0f, far ? r * t * t : r);
+            if (std::is_same<T, __half>::value)  // 2^e from the record's exponent bits
+              fac[u] *= __int_as_float((int)((((unsigned)mi[u].y >> 24) - 1u) << 23));
             on[u] = true;
           }
           float smp[U];
@@ -1112,6 +1173,7 @@ static int batched_group(PhysicsState *s, const qpsdm_static_params &p, const Li
                                       v.ints, s->d_sid, s->d_grp, s->d_grppos, n);
   k_batch_members<<<grd, blk, 0, st>>>(b.d_rec, b.rec_bytes, b.big_endian, n, s->d_val[1],
                                        v.ints, s->d_sid, s->d_srcflag, p.scaled, l.fxi, l.cyi,
+                                       s->dtype == QPSDM_PANEL_FP16 ? s->d_pscale : nullptr,
                                        s->d_mem, s->d_srcpos);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
@@ -1138,8 +1200,10 @@ static int run_panels(PhysicsState *s, const qpsdm_static_params &p, const Physi
   const int ntr = b.ntr;
   size_t sm = fft_smem_bytes(pf.m);
   if ((rc = fft_set_smem_attr((const void *)k_phys_fwd, sm))) return rc;
+  const bool fp16 = s->dtype == QPSDM_PANEL_FP16;
   k_phys_fwd<<<ntr, 256, sm, st>>>(b.d_rec, b.rec_bytes, b.big_endian, status, sstride, p.ntl,
-                                   p.dt, b.d_taper200, pf, s->d_spec);
+                                   p.dt, b.d_taper200, pf, s->d_spec, s->d_fmax,
+                                   fp16 ? s->d_pscale : nullptr);
   const int nk = p.nfft / 2 + 1;
   sm = fft_smem_bytes(pi.m);
   dim3 gp(ntr, s->nbins);
@@ -1147,18 +1211,19 @@ static int run_panels(PhysicsState *s, const qpsdm_static_params &p, const Physi
     case QPSDM_PANEL_FP32:
       if ((rc = fft_set_smem_attr((const void *)k_phys_panels<float>, sm))) return rc;
       k_phys_panels<float><<<gp, 256, sm, st>>>(status, sstride, s->d_spec, nk, s->d_filter, pi,
-                                                s->nbins, (float *)s->d_panels);
+                                                s->nbins, (float *)s->d_panels, nullptr);
       break;
     case QPSDM_PANEL_BF16:
       if ((rc = fft_set_smem_attr((const void *)k_phys_panels<__nv_bfloat16>, sm))) return rc;
       k_phys_panels<__nv_bfloat16><<<gp, 256, sm, st>>>(status, sstride, s->d_spec, nk,
                                                         s->d_filter, pi, s->nbins,
-                                                        (__nv_bfloat16 *)s->d_panels);
+                                                        (__nv_bfloat16 *)s->d_panels, nullptr);
       break;
     default:
       if ((rc = fft_set_smem_attr((const void *)k_phys_panels<__half>, sm))) return rc;
       k_phys_panels<__half><<<gp, 256, sm, st>>>(status, sstride, s->d_spec, nk, s->d_filter,
-                                                 pi, s->nbins, (__half *)s->d_panels);
+                                                 pi, s->nbins, (__half *)s->d_panels,
+                                                 s->d_pscale);
   }
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
@@ -1190,12 +1255,12 @@ static PhysImageArgs image_args(const PhysicsState *s, const qpsdm_static_params
 
 template <typename T>
 static void launch_plain(const PhysImageArgs &a, const PhysicsBatch &b, const LineView &v,
-                         const T *panels, cudaStream_t st) {
+                         const T *panels, const float *pscale, cudaStream_t st) {
   dim3 block(kPhysBz, kPhysBx);
   dim3 grid((a.nzi + kPhysBz - 1) / kPhysBz, (a.nxb + kPhysBx - 1) / kPhysBx);
   k_image_plain<T><<<grid, block, 0, st>>>(v.img, v.comp, a, v.dips, v.ints, v.geom, b.ntr,
                                            v.tab->dt, v.tab->ttt, v.tab->dq, v.tab->qqq,
-                                           panels, b.d_npt);
+                                           panels, pscale, b.d_npt);
 }
 
 int physics_process(PhysicsState *s, const qpsdm_static_params &p,
@@ -1229,11 +1294,12 @@ int physics_process(PhysicsState *s, const qpsdm_static_params &p,
       const PhysImageArgs a = image_args(s, p, lines[il], o, b.nxz);
       b.prof->begin(QPSDM_K_IMAGE, st);
       if (s->dtype == QPSDM_PANEL_FP32)
-        launch_plain<float>(a, b, v, (const float *)s->d_panels, st);
+        launch_plain<float>(a, b, v, (const float *)s->d_panels, s->d_pscale, st);
       else if (s->dtype == QPSDM_PANEL_BF16)
-        launch_plain<__nv_bfloat16>(a, b, v, (const __nv_bfloat16 *)s->d_panels, st);
+        launch_plain<__nv_bfloat16>(a, b, v, (const __nv_bfloat16 *)s->d_panels, s->d_pscale,
+                                    st);
       else
-        launch_plain<__half>(a, b, v, (const __half *)s->d_panels, st);
+        launch_plain<__half>(a, b, v, (const __half *)s->d_panels, s->d_pscale, st);
       b.prof->end(st);
       if (cudaGetLastError() != cudaSuccess) rc = QPSDM_ECUDA;
     }

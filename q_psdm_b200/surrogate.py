@@ -15,7 +15,7 @@ anomalies and the Q layers add.
 It is trained (on the GPU, by the library's own forward and backward
 kernels) on the tables the eikonal generator writes at a coarse surface
 spacing, and is then evaluated at the table nodes of a finer surface grid to
-densify them.  The tables stay the judge of its error: every coarse surface
+densify them.  The tables keep the last word on its error: every coarse surface
 patch of every table cell whose corner nodes the network misses by more than
 ``gate_ms`` (2 ms) keeps plain bilinear interpolation of the coarse tables.
 The reference has no counterpart; it reads precomputed tables only

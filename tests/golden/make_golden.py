@@ -12,12 +12,13 @@ the preprocessing spectra of seeded traces driven through the reference's
 fetch_and_taper + pfarc.
 
     make -C oracle ref-gpu        # builds oracle/_ref/libqpsdm_refgpu.so
-    python tests/golden/make_golden.py gpu   (on a machine with a B200)
+    python tests/golden/make_golden.py gpu [OUTDIR]   (on a machine with a B200)
 
 The GPU vectors come from the reference's own psdm_kernel + image_depth_gpu
 (compiled with its own -O2 --use_fast_math flags for sm_100a) run on seeded
 traces: per-trace acceptance, spectra and the accumulated stub image.  They
-are written to gpurun_out/ and copied here by hand.
+are written to OUTDIR (default tests/golden/) and copied here by hand when
+they were made on another machine.
 """
 from __future__ import annotations
 
@@ -100,14 +101,14 @@ def gpu_case(name: str):
     return make_case(name)
 
 
-def gpu() -> None:
+def gpu(outdir: str | None = None) -> None:
     path = os.path.join(ROOT, "oracle", "_ref", "libqpsdm_refgpu.so")
     L = C.CDLL(path)
     f32 = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
     i32 = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
     L.ref_gpu_run.argtypes = [C.POINTER(RefGpuArgs), C.c_int, i32, f32, i32, i32, f32,
                               f32, i32, f32, f32]
-    outdir = os.path.join(ROOT, "gpurun_out")
+    outdir = outdir or os.path.join(ROOT, "tests", "golden")
     os.makedirs(outdir, exist_ok=True)
     for name in ("small", "block"):
         case = gpu_case(name)
@@ -136,4 +137,7 @@ def gpu() -> None:
 
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "cpu"
-    {"cpu": cpu, "gpu": gpu}[what]()
+    if what == "gpu":
+        gpu(sys.argv[2] if len(sys.argv) > 2 else None)
+    else:
+        cpu()
