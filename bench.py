@@ -54,6 +54,13 @@ METRIC = "Gpoint-traces/s, plain vs batched+BF16+surrogate form, at NRMSE<=1e-3 
 # interpolation, 14 ray geometry and weights, 6 time/t* pick, 2 accumulate.
 # Compat: the stub body of image_depth_gpu (src/q-psdm.cu:2303-2378).
 F_PT = {"batched": 64, "plain": 64, "compat": 35}
+# DRAM bytes (read + write) per point-trace of the image kernel, from one ncu
+# capture each (profiles/): scaled to a launch by its point-traces.
+TRAFFIC_B_PER_PT = {
+    "batched": (340.8e6 + 4.5e6) / 1.943e9,   # 2 gathers x 1 line capture
+    "plain": (255.3e6 + 5.1e6) / 9.58e8,      # the plain form's own step
+    "compat": 4.55e6 / 9.83e8,                # the compat form's own step
+}
 FORMS = {  # shots per step, lines per step, panel dtype, physics form
     "batched": (8, 8, 2, 1),
     "plain": (1, 1, 0, 0),
@@ -74,6 +81,10 @@ def parse():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--only-surrogate", action="store_true",
                     help="time only the surrogate network's kernels (for profiling)")
+    ap.add_argument("--only-eikonal", action="store_true",
+                    help="time only the eikonal / t* table generator (one image line)")
+    ap.add_argument("--eik-half", type=float, default=2000.0,
+                    help="half aperture in x (m) of the eikonal tables (y: half of it)")
     ap.add_argument("--shots", type=int, default=0,
                     help="shot gathers per step of the chosen form (default: the form's own)")
     ap.add_argument("--lines", type=int, default=0,
@@ -375,7 +386,10 @@ def run_ours(args, rank, world, dist):
     roof = {"bound": "fp32", "kernel": {"batched": "k_image_batched", "plain": "k_image_plain",
                                         "compat": "k_image_compat"}[args.form],
             "achieved": achieved, "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32,
-            "traffic": None, "flop_per_point_trace": F_PT[args.form],
+            "traffic": TRAFFIC_B_PER_PT[args.form] * npt_launch,
+            "traffic_note": "DRAM bytes per launch: ncu dram__bytes_read+write per point-trace "
+                            "of a smaller capture (profiles/) x this launch's point-traces",
+            "flop_per_point_trace": F_PT[args.form],
             "point_traces_per_launch": npt_launch,
             "kernel_ms_per_launch": head["image_ms_per_launch"],
             "peak_source": "measured in this run: cuBLAS SGEMM 8192^3, TF32 off (of measured)",
@@ -463,6 +477,46 @@ def run_surrogate(dev, steps, warmup, n_query=1 << 22, batch=1 << 16):
                          "roofline": {"bound": "tensor", "achieved": tf_t, "peak": peak,
                                       "unit": "TFLOP/s", "frac": tf_t / peak,
                                       "flop_per_sample": 6 * MLP_MAC, "peak_source": src}}}
+
+
+# ---------------------------------------------------------------------------
+# the eikonal / t* table generator
+# ---------------------------------------------------------------------------
+def run_eikonal(dev, half_x=2000.0):
+    """Tables of one config-2 image line (512 cdps, depth to 3990 m at 80 m
+    nodes, 160 m surface nodes over +-half_x, +-half_x/2) from the config-2
+    model (v = 1800 + 0.5 z with two +-15 % anomalies, 5 Q layers) on a 40 m
+    grid, background-corrected (two solves per source).  Wall time of the
+    whole generator, device synchronised at both ends."""
+    import torch
+    from q_psdm_b200 import synth
+    from q_psdm_b200 import tables as T
+    torch.cuda.set_device(dev)
+    sv = synth.config2(seed=11)
+    h = 40.0
+    model = synth.config2_model(h=h)
+    bg = synth.config2_model(h=h, anomalies=False, layered_q=False)
+    line_y = (Workload.LINE0) * sv.dyi
+    kw = dict(fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi, zmax=(sv.nzi - 1) * sv.dzi, line_y=line_y,
+              dzii=80.0, nxi1=16, surf_dx=160, surf_dy=160, half_x=half_x,
+              half_y=half_x / 2, h=h, init_radius=200.0, background=bg, q_background=80.0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tab = T.eikonal_line_tables(model, **kw)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    nsrc = len({(round(float(x), 3), round(float(y), 3))
+                for c in range(tab.nxg * tab.nzg)
+                for x in T.cell_surface_nodes(tab, c // tab.nzg, c % tab.nzg, sv.fci)[0]
+                for y in T.cell_surface_nodes(tab, c // tab.nzg, c % tab.nzg, sv.fci)[1]})
+    return {"generator": "Godunov relaxation of the eikonal and the t* transport on a local "
+                         "grid per surface node, background-corrected (2 solves per source)",
+            "model": "config-2: 1800+0.5z, two +-15% Gaussian anomalies (300 m), Q layers "
+                     "200/120/80/50/30, 40 m grid",
+            "line_tables": {"cells": tab.nxg * tab.nzg, "surface_nodes": nsrc,
+                            "values": int(tab.ttt.size), "half_x_m": half_x},
+            "seconds": el, "surface_nodes_per_s": nsrc / el,
+            "finite": bool(np.isfinite(tab.ttt).all() and np.isfinite(tab.qqq).all())}
 
 
 # ---------------------------------------------------------------------------
@@ -677,6 +731,8 @@ def main():
         dist = tdist
     if args.only_surrogate:
         res = run_surrogate(int(os.environ.get("LOCAL_RANK", "0")), args.steps, args.warmup)
+    elif args.only_eikonal:
+        res = run_eikonal(int(os.environ.get("LOCAL_RANK", "0")), args.eik_half)
     elif args.impl == "reference":
         res = run_reference(args, rank, world)
     else:
