@@ -2,7 +2,8 @@
 
 ``python -m q_psdm_b200.build`` compiles every ``csrc/*.cu`` / ``csrc/*.cpp``
 with nvcc (``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``) into
-``q_psdm_b200/libqpsdm_b200.so``.  Objects go to ``q_psdm_b200/_build/``;
+``q_psdm_b200/libqpsdm_b200.so``, then the ``q-psdm`` command-line driver
+(``driver/q_psdm.cpp``) into ``q_psdm_b200/bin/q-psdm``.  Objects go to ``q_psdm_b200/_build/``;
 a source is recompiled only when it, or a header, is newer than its object.
 """
 from __future__ import annotations
@@ -18,6 +19,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libqpsdm_b200.so")
+DRIVER = os.path.join(PKG, "driver")
+DRIVER_BIN = os.path.join(PKG, "bin", "q-psdm")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
@@ -49,6 +52,24 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
+def build_driver() -> str:
+    """The q-psdm command-line driver (host C++ over the C ABI), linked
+    against the in-tree library (rpath $ORIGIN/..)."""
+    src = os.path.join(DRIVER, "q_psdm.cpp")
+    os.makedirs(os.path.dirname(DRIVER_BIN), exist_ok=True)
+    if (os.path.exists(DRIVER_BIN) and os.path.getmtime(DRIVER_BIN) >= os.path.getmtime(src)
+            and os.path.getmtime(DRIVER_BIN) >= os.path.getmtime(LIB)
+            and os.path.getmtime(DRIVER_BIN) >= _headers_mtime()):
+        return DRIVER_BIN
+    cmd = [NVCC, "-O2", "-std=c++17", "-x", "c++", src, "-o", DRIVER_BIN,
+           "-I" + os.path.join(ROOT, "include"), "-L" + PKG, "-lqpsdm_b200", "-lpthread",
+           "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/.."]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
+    return DRIVER_BIN
+
+
 def build(verbose: bool = False) -> str:
     os.makedirs(OUT, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
@@ -60,6 +81,7 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_driver()
     return LIB
 
 

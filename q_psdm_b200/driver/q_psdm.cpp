@@ -1,0 +1,853 @@
+// q-psdm -- the command-line driver of the B200 imaging engine.
+//
+// A drop-in for the reference program's driver (src/q-psdm.cu:383-1160 main,
+// :1161-1860 qpsdm, :1862-1926 producer): the same command-line keys and
+// par.dat keys with the same defaults, the same project layout
+//   <path> = <projpath>/<iproc>/<task>
+//   <projpath>/data<idata>/nofffile.rcd            "nofffile=N"
+//   <projpath>/data<idata>/off<k>/ell_off<k>        "offmin,offmax"
+//   <projpath>/data<idata>/off<k>/line<l>           input SU (big-endian)
+//   <ttpath>/Lxxx.{tidx,qidx}, <ttpath>/L<line>.{ttt,qqq}
+//   <projpath>/<idata>/<task>/result/<node>_<idata>.off<k>.L<line>.su   output
+// and the same checkpoint markers (<offspath>/break_point.txt holding the
+// last finished line, an empty <infopath>/<node>_<line> per line, an empty
+// <infopath of data 0>/<node> at the end).  The imaging itself goes through
+// the engine's C ABI (include/qpsdm_engine.h); a reader thread fills pinned
+// host buffers with raw SU records while the engine images the previous one.
+//
+// Keys this driver adds (the reference has no counterpart):
+//   engine=compat|physics   compat (default) reproduces the reference's stub
+//                           kernel; physics images with the t / t* tables
+//   form=plain|batched      physics form (default batched)
+//   panels=fp32|bf16|fp16   physics panel type (default fp16 batched, fp32 plain)
+//   nbins=16 dtstar=0.002   t* bins of the compensated panels
+//   aperx, apery            half aperture in cdps / lines for every azimuth
+//                           (the reference allocates but never fills its
+//                           aperture tables, src/q-psdm.cu:1542-1545;
+//                           default: the whole image)
+//   dzii                    table depth-node spacing (default 48 m as the
+//                           reference derives it, src/q-psdm.cu:880-882)
+//   max_batch               traces per submit (default 16384)
+//   resume=1                skip the lines up to <offspath>/break_point.txt
+//   check=1                 resolve and print the parameters, image nothing
+// Errors print a message and exit 1, as the reference does; the library
+// itself never exits.
+#include <cuda_runtime.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <cmath>
+#include <condition_variable>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "qpsdm_engine.h"
+
+namespace {
+
+[[noreturn]] void die(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::fprintf(stderr, "Error: ");
+  std::vfprintf(stderr, fmt, ap);
+  std::fprintf(stderr, "\n");
+  va_end(ap);
+  std::exit(1);
+}
+
+void logf(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::vfprintf(stderr, fmt, ap);
+  va_end(ap);
+}
+
+bool exists(const std::string &p) { return access(p.c_str(), F_OK) == 0; }
+
+// ---------------------------------------------------------------------------
+// command line and par.dat
+// ---------------------------------------------------------------------------
+// Command line: "key=value" words; the first word with that key wins
+// (getparstr, src/psdmpkg.cc:233-334).
+struct CmdLine {
+  std::vector<std::string> words;
+  bool get(const std::string &key, std::string &out) const {
+    for (const auto &w : words)
+      if (w.size() > key.size() && w.compare(0, key.size(), key) == 0 && w[key.size()] == '=') {
+        out = w.substr(key.size() + 1);
+        return true;
+      }
+    return false;
+  }
+};
+
+// par.dat: "key=value" records, '#' comments (whole line or trailing), a
+// trailing backslash continues a record, blanks around a record ignored.  A
+// key counts only when exactly one record has it (readparfile,
+// src/psdmpkg.cc:338-574); the value is the record's first word.
+struct ParFile {
+  std::vector<std::string> recs;
+  void load(const std::string &path) {
+    FILE *fp = std::fopen(path.c_str(), "r");
+    if (!fp) die("Parameter File [%s] Open Error", path.c_str());
+    std::string cur;
+    char buf[4096];
+    while (std::fgets(buf, sizeof buf, fp)) {
+      cur += buf;
+      if (cur.empty() || cur.back() != '\n') continue;  // long line: keep reading
+      cur.pop_back();
+      if (!cur.empty() && cur.back() == '\\') {  // continuation
+        cur.pop_back();
+        continue;
+      }
+      add(cur);
+      cur.clear();
+    }
+    if (!cur.empty()) add(cur);
+    std::fclose(fp);
+  }
+  void add(std::string s) {
+    size_t b = 0;
+    while (b < s.size() && std::isspace((unsigned char)s[b])) ++b;
+    s = s.substr(b);
+    if (s.empty() || s[0] == '#') return;
+    const size_t h = s.find('#');
+    if (h != std::string::npos) s = s.substr(0, h);
+    while (!s.empty() && std::isspace((unsigned char)s.back())) s.pop_back();
+    if (!s.empty()) recs.push_back(s);
+  }
+  bool get(const std::string &key, std::string &out) const {
+    int n = 0;
+    std::string v;
+    for (const auto &r : recs)
+      if (r.size() > key.size() && r.compare(0, key.size(), key) == 0 && r[key.size()] == '=') {
+        ++n;
+        v = r.substr(key.size() + 1);
+      }
+    if (n != 1) return false;
+    const size_t e = v.find_first_of(" \t");
+    out = e == std::string::npos ? v : v.substr(0, e);
+    return !out.empty();
+  }
+};
+
+struct Keys {
+  CmdLine cmd;
+  ParFile par;
+  bool str(const char *k, std::string &out) const { return cmd.get(k, out) || par.get(k, out); }
+  std::string str_or(const char *k, const std::string &def) const {
+    std::string v;
+    return str(k, v) ? v : def;
+  }
+  std::string str_req(const char *k) const {
+    std::string v;
+    if (!str(k, v)) die("%s must be specified", k);
+    return v;
+  }
+  int int_or(const char *k, int def) const {
+    std::string v;
+    return str(k, v) ? (int)std::strtol(v.c_str(), nullptr, 10) : def;
+  }
+  int int_req(const char *k) const { return (int)std::strtol(str_req(k).c_str(), nullptr, 10); }
+  float flt_or(const char *k, float def) const {
+    std::string v;
+    return str(k, v) ? (float)std::strtod(v.c_str(), nullptr) : def;
+  }
+  float flt_req(const char *k) const { return (float)std::strtod(str_req(k).c_str(), nullptr); }
+};
+
+// "1,5-8,10:2:16" -> 1 5 6 7 8 10 12 14 16 (parseline, src/psdmpkg.cc:108-206)
+std::vector<int> parse_list(const std::string &s) {
+  std::vector<int> out;
+  size_t i = 0;
+  while (i < s.size()) {
+    size_t j = s.find(',', i);
+    if (j == std::string::npos) j = s.size();
+    const std::string item = s.substr(i, j - i);
+    int a, b, c;
+    if (std::sscanf(item.c_str(), "%d:%d:%d", &a, &b, &c) == 3) {
+      if (b > 0)
+        for (int v = a; v <= c; v += b) out.push_back(v);
+      else if (b < 0)
+        for (int v = a; v >= c; v += b) out.push_back(v);
+    } else if (std::sscanf(item.c_str(), "%d-%d", &a, &b) == 2) {
+      for (int v = a; v <= b; ++v) out.push_back(v);
+    } else if (std::sscanf(item.c_str(), "%d", &a) == 1) {
+      out.push_back(a);
+    }
+    i = j + 1;
+  }
+  return out;
+}
+
+// "(d1,o1),(d2,o2)..." -> pairs (parsetuple, src/psdmpkg.cc:686-880)
+std::vector<std::pair<float, float>> parse_pairs(const std::string &s) {
+  std::vector<std::pair<float, float>> out;
+  size_t i = 0;
+  while ((i = s.find('(', i)) != std::string::npos) {
+    const size_t j = s.find(')', i);
+    if (j == std::string::npos) break;
+    float a, b;
+    if (std::sscanf(s.c_str() + i + 1, "%f%*[ ,;\t]%f", &a, &b) == 2) out.push_back({a, b});
+    i = j + 1;
+  }
+  return out;
+}
+
+// Monotone (depth, offset) pairs, then the depth of a given offset:
+// linear inside, the end segments extended outside
+// (time_offset_mute_santity / time_offset_mute, src/psdmpkg.cc:576-600, :1030-1075).
+void mute_sanity(std::vector<std::pair<float, float>> &m) {
+  for (size_t i = 0; i + 1 < m.size(); ++i) {
+    if (m[i].first > m[i + 1].first) m[i + 1].first = 2.0f * m[i].first - m[i + 1].first;
+    if (m[i].second > m[i + 1].second) m[i + 1].second = 2.0f * m[i].second - m[i + 1].second;
+  }
+  for (size_t i = 0; i + 1 < m.size(); ++i) {
+    if (m[i].first >= m[i + 1].first) m[i + 1].first = m[i].first + 0.01f;
+    if (m[i].second >= m[i + 1].second) m[i + 1].second = m[i].second + 10.0f;
+  }
+}
+float mute_depth(const std::vector<std::pair<float, float>> &m, float o) {
+  const size_t n = m.size();
+  if (n == 0) return 0.0f;
+  if (n == 1) return m[0].first;
+  size_t a = 0;
+  if (o < m[0].second)
+    a = 0;
+  else if (o >= m[n - 1].second)
+    a = n - 2;
+  else
+    for (size_t i = 0; i + 1 < n; ++i)
+      if (m[i].second <= o && o < m[i + 1].second) {
+        a = i;
+        break;
+      }
+  const float o1 = m[a].second, o2 = m[a + 1].second, t1 = m[a].first, t2 = m[a + 1].first;
+  return t1 + (t2 - t1) / (o2 - o1) * (o - o1);
+}
+
+// <projpath>/<projname>/<iproc>/<task> split as parsepath (src/psdmpkg.cc:633-684)
+struct ProjPath {
+  std::string projpath, projname, task;
+  int iproc = 0;
+};
+ProjPath parse_path(std::string path) {
+  while (!path.empty() && path.back() == '/') path.pop_back();
+  ProjPath r;
+  size_t s = path.rfind('/');
+  r.task = s == std::string::npos ? path : path.substr(s + 1);
+  const std::string rest = s == std::string::npos ? "" : path.substr(0, s);
+  s = rest.rfind('/');
+  r.iproc = std::atoi((s == std::string::npos ? rest : rest.substr(s + 1)).c_str());
+  r.projpath = s == std::string::npos ? "" : rest.substr(0, s);
+  s = r.projpath.rfind('/');
+  r.projname = s == std::string::npos ? r.projpath : r.projpath.substr(s + 1);
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// SU records (big-endian on disk, SEG-Y trace header offsets)
+// ---------------------------------------------------------------------------
+constexpr int kHdr = 240;
+enum { oTracl = 0, oFldr = 8, oCdp = 20, oTrid = 28, oNvs = 30, oOffset = 36, oScalco = 70,
+       oSx = 72, oSy = 76, oGx = 80, oGy = 84, oCounit = 88, oNs = 114, oDt = 116 };
+
+int32_t be_i32(const uint8_t *p) {
+  return (int32_t)((uint32_t)p[0] << 24 | (uint32_t)p[1] << 16 | (uint32_t)p[2] << 8 | p[3]);
+}
+int16_t be_i16(const uint8_t *p) { return (int16_t)((uint16_t)p[0] << 8 | p[1]); }
+void put_i32(uint8_t *p, int32_t v) {
+  const uint32_t u = (uint32_t)v;
+  p[0] = u >> 24;
+  p[1] = u >> 16;
+  p[2] = u >> 8;
+  p[3] = u;
+}
+void put_i16(uint8_t *p, int16_t v) {
+  const uint16_t u = (uint16_t)v;
+  p[0] = u >> 8;
+  p[1] = u;
+}
+
+struct TraceHdr {
+  uint8_t h[kHdr];
+};
+// header of trace k of an SU file whose traces have ns samples
+bool read_header(FILE *fp, long k, int ns, TraceHdr &t) {
+  if (std::fseek(fp, k * (kHdr + 4L * ns), SEEK_SET) != 0) return false;
+  return std::fread(t.h, 1, kHdr, fp) == (size_t)kHdr;
+}
+// getscale (src/psdmpkg.cc:1013-1027): single precision, as the reference
+// derives its geometry from it in float
+float su_scale(int16_t scalco) {
+  if (scalco == 0) return 1.0f;
+  return scalco > 0 ? (float)scalco : -1.0f / scalco;
+}
+
+// ---------------------------------------------------------------------------
+// tables: Lxxx.{tidx,qidx} + L<line>.{ttt,qqq}, inter-line lerp
+// (get_ttt_all, src/q-psdm.cu:2382-2622)
+// ---------------------------------------------------------------------------
+struct Tables {
+  int cdp1 = 0, cdp2 = 0, nzg = 0, nxg = 0, nzi1 = 0, nxi1 = 0;
+  std::vector<qpsdm_ttt_desc> desc;
+  std::vector<float> data;
+};
+bool load_tables(const std::string &ttpath, bool q, int line, int line1, int line2, Tables &t) {
+  const std::string idx = ttpath + (q ? "/Lxxx.qidx" : "/Lxxx.tidx");
+  const char *suff = q ? "qqq" : "ttt";
+  FILE *fp = std::fopen(idx.c_str(), "rb");
+  if (!fp) return false;
+  int32_t h[2];
+  float dxdz[2];
+  int32_t g[4];
+  bool ok = std::fread(h, 4, 2, fp) == 2 && std::fread(dxdz, 4, 2, fp) == 2 &&
+            std::fread(g, 4, 4, fp) == 4;
+  if (ok) {
+    t.cdp1 = h[0];
+    t.cdp2 = h[1];
+    t.nzg = g[0];
+    t.nxg = g[1];
+    t.nzi1 = g[2];
+    t.nxi1 = g[3];
+    t.desc.resize((size_t)t.nxg * t.nzg);
+    ok = t.nxg > 0 && t.nzg > 0 &&
+         std::fread(t.desc.data(), sizeof(qpsdm_ttt_desc), t.desc.size(), fp) == t.desc.size();
+  }
+  std::fclose(fp);
+  if (!ok) die("travel time table or qfield index size error %s", idx.c_str());
+  auto path_of = [&](int l) { return ttpath + "/L" + std::to_string(l) + "." + suff; };
+  int lo = -1, hi = -1;
+  for (int l = line; l >= line1; --l)
+    if (exists(path_of(l))) {
+      lo = l;
+      break;
+    }
+  for (int l = line; l <= line2; ++l)
+    if (exists(path_of(l))) {
+      hi = l;
+      break;
+    }
+  if (lo < 0 || hi < 0) die("no %s table brackets line %d in %s", suff, line, ttpath.c_str());
+  auto read_all = [&](int l, std::vector<float> &v) {
+    FILE *f = std::fopen(path_of(l).c_str(), "rb");
+    if (!f) die("cannot open %s", path_of(l).c_str());
+    std::fseek(f, 0, SEEK_END);
+    const long bytes = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    v.resize((size_t)bytes / 4);
+    if (std::fread(v.data(), 4, v.size(), f) != v.size()) die("read %s", path_of(l).c_str());
+    std::fclose(f);
+  };
+  read_all(lo, t.data);
+  if (hi != lo) {
+    std::vector<float> b;
+    read_all(hi, b);
+    if (b.size() != t.data.size()) die("table sizes of lines %d and %d differ", lo, hi);
+    const float c2 = (float)(1.0 * (line - lo) / (hi - lo)), c1 = 1.0f - c2;
+    for (size_t i = 0; i < b.size(); ++i) t.data[i] = t.data[i] * c1 + b[i] * c2;
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// producer: a reader thread filling pinned buffers with raw SU records
+// ---------------------------------------------------------------------------
+class Producer {
+ public:
+  Producer(size_t rec_bytes, int max_batch, int nbuf) : rec_bytes_(rec_bytes), max_(max_batch) {
+    for (int i = 0; i < nbuf; ++i) {
+      void *p = nullptr;
+      if (cudaMallocHost(&p, rec_bytes * max_batch) != cudaSuccess)
+        die("pinned host buffer of %zu bytes", rec_bytes * max_batch);
+      bufs_.push_back((uint8_t *)p);
+      free_.push_back(i);
+    }
+  }
+  ~Producer() {
+    if (th_.joinable()) th_.join();
+    for (auto *p : bufs_) cudaFreeHost(p);
+  }
+  // start reading the files in order
+  void start(std::vector<std::string> files) {
+    done_ = false;
+    th_ = std::thread([this, files] { run(files); });
+  }
+  // next filled buffer (index, traces); false when all files are read
+  bool next(int &buf, int &ntr) {
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [&] { return !full_.empty() || done_; });
+    if (full_.empty()) return false;
+    buf = full_.front().first;
+    ntr = full_.front().second;
+    full_.pop_front();
+    return true;
+  }
+  void release(int buf) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      free_.push_back(buf);
+    }
+    cv_.notify_all();
+  }
+  void join() {
+    if (th_.joinable()) th_.join();
+  }
+  const uint8_t *data(int buf) const { return bufs_[buf]; }
+  long traces_read = 0;
+
+ private:
+  void run(std::vector<std::string> files) {
+    for (const auto &f : files) {
+      FILE *fp = std::fopen(f.c_str(), "rb");
+      if (!fp) continue;  // a missing data line contributes nothing
+      struct stat st;
+      fstat(fileno(fp), &st);
+      long left = (long)(st.st_size / (long)rec_bytes_);
+      while (left > 0) {
+        int b;
+        {
+          std::unique_lock<std::mutex> lk(mu_);
+          cv_.wait(lk, [&] { return !free_.empty(); });
+          b = free_.front();
+          free_.pop_front();
+        }
+        const int n = (int)std::min<long>(left, max_);
+        const size_t got = std::fread(bufs_[b], rec_bytes_, n, fp);
+        if ((int)got != n) die("Read %s fail: %s", f.c_str(), std::strerror(errno));
+        left -= n;
+        traces_read += n;
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          full_.push_back({b, n});
+        }
+        cv_.notify_all();
+      }
+      std::fclose(fp);
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      done_ = true;
+    }
+    cv_.notify_all();
+  }
+  size_t rec_bytes_;
+  int max_;
+  std::vector<uint8_t *> bufs_;
+  std::deque<int> free_;
+  std::deque<std::pair<int, int>> full_;
+  bool done_ = true;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::thread th_;
+};
+
+void touch(const std::string &p, const std::string &content) {
+  FILE *fp = std::fopen(p.c_str(), "w");
+  if (fp) {
+    std::fputs(content.c_str(), fp);
+    std::fclose(fp);
+  }
+}
+
+void check_engine(int rc, qpsdm_engine *e, const char *what) {
+  if (rc != QPSDM_OK) die("%s failed (%d): %s", what, rc, e ? qpsdm_last_error(e) : "");
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  Keys K;
+  for (int i = 1; i < argc; ++i) K.cmd.words.push_back(argv[i]);
+  std::string path, parfilepath, nodename, ttpath;
+  if (!K.cmd.get("path", path)) die("path must be specified");
+  if (!K.cmd.get("parfilepath", parfilepath)) die("parfilepath must be specified");
+  if (!K.cmd.get("nodename", nodename)) die("nodename must be specified");
+  if (!K.cmd.get("ttpath", ttpath)) die("ttpath must be specified");
+  while (!path.empty() && path.back() == '/') path.pop_back();
+  K.par.load(parfilepath);
+  const ProjPath pp = parse_path(path);
+
+  // ---- keys (src/q-psdm.cu:433-714) ----
+  std::string offspath = K.str_or("offspath", pp.projpath + "/data" + std::to_string(pp.iproc));
+  const std::string velfilepath = K.str_or("velfilepath", pp.projpath + "/vel/vel_loadin");
+  std::string infopath = K.str_or("infopath", path);
+  const float fc = K.flt_or("fc", 40.0f), contract = K.flt_or("contract", 3.0f);
+  const float taperzone = K.flt_or("taperzone", 8.0f), threshold = K.flt_or("threshold", 600.0f);
+  const float f1 = K.flt_or("f1", 1.0f);
+  float f3 = K.flt_or("f3", 130.0f), f4 = K.flt_or("f4", 140.0f);
+  const int ntl = K.int_req("ntl");
+  const float dt = K.flt_req("dt");
+  const int line1 = K.int_req("line1"), line2 = K.int_req("line2");
+  const float zmin = K.flt_req("zmin"), zmax = K.flt_req("zmax"), dzi = K.flt_req("dzi");
+  const int cdp1 = K.int_req("cdp1"), cdp2 = K.int_req("cdp2");
+  const std::vector<int> lines = parse_list(K.str_req("line"));
+  const std::string zmute = K.str_or("mute", "(1,9999),(100,9999)");
+  const int xline = K.int_req("extxline");
+  const int opcrp = K.int_or("opcrp", 0);
+  const std::vector<int> cdps =
+      parse_list(K.str_or("cdps", std::to_string(cdp1) + "-" + std::to_string(cdp2)));
+  const int nblock = std::max(1, K.int_or("nblock", 1));
+  // the reference reads ndata but clamps it to its GPU count, which it sets
+  // to 1 (src/q-psdm.cu:786-798): one data directory, data<iproc>'s sibling 0
+  const int ndata = std::min(std::max(1, K.int_or("ndata", 1)), 1);
+  // Nyquist clamps (src/q-psdm.cu:711-723)
+  if (f3 > 0.5f / dt - 10.0f) f3 = 0.5f / dt - 10.0f;
+  if (f4 > 0.5f / dt - 5.0f) f4 = 0.5f / dt - 5.0f;
+  if (f4 - f3 <= 5.0f) f3 = f4 - 5.0f;
+  // this driver's keys
+  const std::string engine_mode = K.str_or("engine", "compat");
+  const std::string form = K.str_or("form", "batched");
+  const std::string panels = K.str_or("panels", form == "plain" ? "fp32" : "fp16");
+  const int nbins = K.int_or("nbins", 16);
+  const float dtstar = K.flt_or("dtstar", 0.002f);
+  const int max_batch = std::max(1, K.int_or("max_batch", 16384));
+  const int resume = K.int_or("resume", 0);
+  const int check_only = K.int_or("check", 0);
+  if (engine_mode != "compat" && engine_mode != "physics") die("engine must be compat or physics");
+  if (form != "plain" && form != "batched") die("form must be plain or batched");
+  if (panels != "fp32" && panels != "bf16" && panels != "fp16") die("panels must be fp32, bf16 or fp16");
+
+  // GPU from the node name "<name>_<gpu>" (src/q-psdm.cu:725-786)
+  int igpu = 0;
+  if (std::sscanf(nodename.c_str(), "%*[^_]_%d", &igpu) != 1)
+    die("Nodename [%s] Format Error or This Machine has no GPUs", nodename.c_str());
+  const std::string node0 = nodename.substr(0, nodename.find('_'));
+
+  // image space (src/q-psdm.cu:826-834)
+  const int fci = cdp1, nxi = cdp2 - cdp1 + 1, nyi = (int)lines.size();
+  const int nzi = (int)(zmax / dzi + 0.5f) + 1;
+  if (nxi <= 0 || nzi <= 0 || nyi <= 0) die("empty image (cdp1..cdp2, zmax, line)");
+
+  // velocity-file geometry: first and last trace (src/q-psdm.cu:836-880)
+  if (!exists(velfilepath)) die("On Node [%s], Velocity File [%s] Does Not Exist", nodename.c_str(),
+                                velfilepath.c_str());
+  FILE *vf = std::fopen(velfilepath.c_str(), "rb");
+  TraceHdr v0, v1;
+  if (!vf || std::fread(v0.h, 1, kHdr, vf) != (size_t)kHdr) die("velocity file header");
+  const int ntv = (uint16_t)be_i16(v0.h + oNs);
+  std::fseek(vf, -(long)(kHdr + 4L * ntv), SEEK_END);
+  if (std::fread(v1.h, 1, kHdr, vf) != (size_t)kHdr) die("velocity file last header");
+  // float arithmetic as src/q-psdm.cu:846-858 (int x float -> float)
+  const float scalev = su_scale(be_i16(v0.h + oScalco));
+  const double fxv = (float)be_i32(v0.h + oGx) * scalev;
+  const double fyv = (float)be_i32(v0.h + oGy) * scalev;
+  const int fcv = be_i32(v0.h + oCdp), flv = be_i32(v0.h + oFldr);
+  const int nxv = be_i32(v1.h + oCdp) - fcv + 1, nyv = be_i32(v1.h + oFldr) - flv + 1;
+  if (nxv < 2) die("velocity file has a single cdp");
+  const float dxv = (float)(be_i32(v1.h + oGx) - be_i32(v0.h + oGx)) * scalev / (float)(nxv - 1);
+  float dyv;
+  if (nyv == 1) {
+    std::string s;
+    if (!K.str("dyv", s))
+      die("since first fldr and last fldr in the velocity file is the same:%d please specify dyv!",
+          flv);
+    dyv = (float)std::strtod(s.c_str(), nullptr);
+  } else {
+    dyv = (float)(be_i32(v1.h + oGy) - be_i32(v0.h + oGy)) * scalev / (float)(nyv - 1);
+    dyv = K.flt_or("dyv", dyv);
+  }
+  const float dxi = dxv, dyi = dyv;
+  const float dzii = K.flt_or("dzii", 8.0f * std::round(50.0f / 8.0f));
+  const int aperx = K.int_or("aperx", nxi), apery = K.int_or("apery", nyv);
+
+  // data-space scale and sanity (src/q-psdm.cu:886-915)
+  double scaled = 1.0;
+  for (int l = lines[0] - 1000; l < lines[0] + 1000; ++l) {
+    const std::string f = offspath + "/off0/line" + std::to_string(l);
+    if (!exists(f)) continue;
+    FILE *fp = std::fopen(f.c_str(), "rb");
+    TraceHdr t;
+    if (fp && std::fread(t.h, 1, kHdr, fp) == (size_t)kHdr) {
+      scaled = su_scale(be_i16(t.h + oScalco));
+      if ((uint16_t)be_i16(t.h + oNs) != ntl)
+        die("In Data Space (tr.ns=%d)!=(ntl=%d)", (uint16_t)be_i16(t.h + oNs), ntl);
+      if ((uint16_t)be_i16(t.h + oDt) != (int)(dt * 1.0E6f))
+        die("In Data Space (tr.dt=%d)!=(dt=%g*1.0E6)", (uint16_t)be_i16(t.h + oDt), dt);
+    }
+    if (fp) std::fclose(fp);
+    break;
+  }
+
+  // offset groups of each data directory (src/q-psdm.cu:917-972)
+  std::vector<std::vector<float>> offmin(ndata), offmax(ndata);
+  for (int id = 0; id < ndata; ++id) {
+    const std::string op = pp.projpath + "/data" + std::to_string(id);
+    const std::string rcd = op + "/nofffile.rcd";
+    FILE *fp = std::fopen(rcd.c_str(), "r");
+    int n = 0;
+    if (!fp || std::fscanf(fp, "nofffile=%d", &n) != 1)
+      die("On %s_%d,[%s] Does Not Exist or unreadable", node0.c_str(), id, rcd.c_str());
+    std::fclose(fp);
+    for (int k = 0; k < n; ++k) {
+      const std::string e = op + "/off" + std::to_string(k) + "/ell_off" + std::to_string(k);
+      FILE *f = std::fopen(e.c_str(), "r");
+      float a, b;
+      if (!f || std::fscanf(f, "%f,%f", &a, &b) != 2) die("Read offmin and offmax from %s fail!", e.c_str());
+      std::fclose(f);
+      offmin[id].push_back(a);
+      offmax[id].push_back(b);
+    }
+  }
+  auto mute = parse_pairs(zmute);
+  mute_sanity(mute);
+
+  logf("q-psdm: node %s gpu %d  image %d cdps x %d lines x %d depths  dx %g dy %g dz %g\n",
+       nodename.c_str(), igpu, nxi, nyi, nzi, dxi, dyi, dzi);
+  logf("        velocity grid fxv %.3f fyv %.3f fcv %d flv %d nxv %d nyv %d; data scale %g\n", fxv,
+       fyv, fcv, flv, nxv, nyv, scaled);
+  logf("        engine %s form %s panels %s nbins %d dtstar %g aperture %d x %d opcrp %d\n",
+       engine_mode.c_str(), form.c_str(), panels.c_str(), nbins, dtstar, aperx, apery, opcrp);
+
+  // ---- engine (src/q-psdm.cu:1161-1376) ----
+  qpsdm_static_params sp;
+  std::memset(&sp, 0, sizeof sp);
+  sp.dyi = dyi;
+  sp.dxi = dxi;
+  sp.nxi = nxi;
+  sp.nzi = nzi;
+  sp.ntl = ntl;
+  sp.scaled = scaled;
+  sp.fci = fci;
+  sp.dzi = dzi;
+  sp.dt = dt;
+  sp.fc = fc;
+  sp.f1 = f1;
+  sp.f3 = f3;
+  sp.f4 = f4;
+  sp.threshold = threshold;
+  sp.contract = contract;
+  sp.taperzone = taperzone;
+  sp.fxv1 = (float)(fxv - 2000.0);
+  sp.exv1 = (float)(fxv + nxv * dxi + 2000.0);
+  sp.fyv1 = (float)(fyv - 1000.0);
+  sp.eyv1 = (float)(fyv + nyv * dyi + 1000.0);
+  sp.dzii = dzii;
+  sp.mode = engine_mode == "physics" ? QPSDM_MODE_PHYSICS : QPSDM_MODE_COMPAT;
+  sp.panel_dtype = panels == "fp32" ? QPSDM_PANEL_FP32
+                   : panels == "bf16" ? QPSDM_PANEL_BF16 : QPSDM_PANEL_FP16;
+  sp.nbins = nbins;
+  sp.dtstar = dtstar;
+  sp.max_batch = max_batch;
+  sp.form = form == "plain" ? QPSDM_FORM_PLAIN : QPSDM_FORM_BATCHED;
+  if (qpsdm_static_params_init(&sp) != QPSDM_OK) die("bad parameters");
+  logf("        nfft %d nffti %d dt1 %g contract %g taperzone %g (rad)\n", sp.nfft, sp.nffti,
+       sp.dt1, sp.contract, sp.taperzone);
+  if (check_only) {
+    std::printf("{\"projpath\":\"%s\",\"projname\":\"%s\",\"iproc\":%d,\"task\":\"%s\","
+                "\"offspath\":\"%s\",\"velfilepath\":\"%s\",\"infopath\":\"%s\","
+                "\"nxi\":%d,\"nyi\":%d,\"nzi\":%d,\"fci\":%d,\"dxi\":%.9g,\"dyi\":%.9g,"
+                "\"fxv\":%.17g,\"fyv\":%.17g,\"fcv\":%d,\"flv\":%d,\"nxv\":%d,\"nyv\":%d,"
+                "\"scaled\":%.17g,\"f1\":%.6g,\"f3\":%.6g,\"f4\":%.6g,\"fc\":%.6g,"
+                "\"threshold\":%.6g,\"contract_deg\":%.6g,\"taperzone_deg\":%.6g,"
+                "\"extxline\":%d,\"opcrp\":%d,\"aperx\":%d,\"apery\":%d,\"dzii\":%.6g,"
+                "\"engine\":\"%s\",\"form\":\"%s\",\"panels\":\"%s\",\"nbins\":%d,"
+                "\"dtstar\":%.6g,\"max_batch\":%d,\"nblock\":%d,\"gpu\":%d,\"node0\":\"%s\","
+                "\"noffs\":%d,\"offmin\":%.6g,\"offmax\":%.6g,\"nfft\":%d,\"nffti\":%d,"
+                "\"lines\":[",
+                pp.projpath.c_str(), pp.projname.c_str(), pp.iproc, pp.task.c_str(),
+                offspath.c_str(), velfilepath.c_str(), infopath.c_str(), nxi, nyi, nzi, fci, dxi,
+                dyi, fxv, fyv, fcv, flv, nxv, nyv, scaled, f1, f3, f4, fc, threshold, contract,
+                taperzone, xline, opcrp, aperx, apery, dzii, engine_mode.c_str(), form.c_str(),
+                panels.c_str(), nbins, dtstar, max_batch, nblock, igpu, node0.c_str(),
+                (int)offmin[0].size(), offmin[0].empty() ? 0.0 : offmin[0][0],
+                offmax[0].empty() ? 0.0 : offmax[0][0], sp.nfft, sp.nffti);
+    for (size_t i = 0; i < lines.size(); ++i) std::printf("%s%d", i ? "," : "", lines[i]);
+    std::printf("],\"mute_depth_off0\":%.6g}\n",
+                offmin[0].empty() ? 0.0 : (double)mute_depth(mute, offmin[0][0]));
+    return 0;
+  }
+  int ngpu = 0;
+  if (cudaGetDeviceCount(&ngpu) != cudaSuccess || ngpu <= 0) die("no CUDA device");
+  if (igpu >= ngpu) {
+    logf("Warn: This Machine [%s] has no such GPU using id=%d instead\n", nodename.c_str(),
+         igpu % ngpu);
+    igpu %= ngpu;
+  }
+  std::vector<int> iaz(4096);
+  const int naz = qpsdm_build_iaztab(sp.eps, iaz.data(), (int)iaz.size());
+  qpsdm_engine *eng = nullptr;
+  check_engine(qpsdm_engine_create(&sp, iaz.data(), naz, igpu, &eng), nullptr, "engine create");
+
+  // constant dip limits (src/q-psdm.cu:1463-1472): the argument summed in
+  // double and rounded to float, then the float tangent
+  const size_t nxz = (size_t)nxi * nzi;
+  std::vector<float> dx1(nxz, tanf((float)(-10 * 0.0174532925199 + (double)sp.contract)));
+  std::vector<float> dx2(nxz, tanf((float)(10 * 0.0174532925199 - (double)sp.contract)));
+  const size_t rec_bytes = kHdr + 4 * (size_t)ntl;
+  Producer prod(rec_bytes, max_batch, 2);
+  const int nxb1 = (int)(nxi / nblock + 0.5);
+
+  // resume after the last finished line
+  size_t first = 0;
+  if (resume) {
+    FILE *fp = std::fopen((offspath + "/break_point.txt").c_str(), "r");
+    int done_line;
+    if (fp && std::fscanf(fp, "%d", &done_line) == 1)
+      for (size_t i = 0; i < lines.size(); ++i)
+        if (lines[i] == done_line) first = i + 1;
+    if (fp) std::fclose(fp);
+    logf("resume: starting at line index %zu\n", first);
+  }
+
+  std::vector<float> img;
+  for (size_t iyi = first; iyi < lines.size(); ++iyi) {
+    const int line = lines[iyi];
+    const time_t tic = std::time(nullptr);
+    const double fxi = fxv + (double)((float)(fci - fcv) * dxi);  // src/q-psdm.cu:1430-1431
+    const double cyi = fyv + (double)((float)(line - flv) * dyi);
+    logf("Start Image Line:%d\n", line);
+    const int ioffl1 = std::max(line - xline, line1), ioffl2 = std::min(line + xline, line2);
+    // output coordinates from the velocity file (get_vel_coor, src/psdmpkg.cc:979-1011)
+    std::vector<int32_t> csx(nxi), csy(nxi);
+    const int16_t vel_scalco = be_i16(v0.h + oScalco);
+    {
+      const int vl = std::min(line, flv + nyv - 1);
+      for (int i = 0; i < nxi; ++i) {
+        TraceHdr t;
+        if (!read_header(vf, (long)(vl - flv) * nxv + fci - fcv + i, ntv, t))
+          die("velocity file too short for line %d", line);
+        csx[i] = be_i32(t.h + oSx);
+        csy[i] = be_i32(t.h + oSy);
+      }
+    }
+    // tables (required in physics mode)
+    Tables tt, tq;
+    const bool have_t = load_tables(ttpath, false, line, line1, line2, tt);
+    const bool have_q = have_t && load_tables(ttpath, true, line, line1, line2, tq);
+    if (sp.mode == QPSDM_MODE_PHYSICS && !(have_t && have_q))
+      die("physics mode needs %s/Lxxx.tidx and Lxxx.qidx", ttpath.c_str());
+    if (have_q && (tt.cdp1 != tq.cdp1 || tt.cdp2 != tq.cdp2 || tt.cdp1 >= tt.cdp2))
+      die("travel time table cdp range error, or not confirm with qfield");
+    qpsdm_line_params lp;
+    std::memset(&lp, 0, sizeof lp);
+    lp.fxi = fxi;
+    lp.cyi = cyi;
+    lp.dipx1 = dx1.data();
+    lp.dipx2 = dx2.data();
+    lp.dipy1 = dx1.data();
+    lp.dipy2 = dx2.data();
+    if (have_q) {
+      lp.nxg = tt.nxg;
+      lp.nzg = tt.nzg;
+      lp.nxi1 = tt.nxi1;
+      lp.nzi1 = tt.nzi1;
+      lp.ttt_cdp1 = tt.cdp1;
+      lp.ttt_cdp2 = tt.cdp2;
+      lp.ttt_desc = tt.desc.data();
+      lp.qqq_desc = tq.desc.data();
+      lp.ttt = tt.data.data();
+      lp.qqq = tq.data.data();
+      lp.ttt_len = (int64_t)tt.data.size();
+      lp.qqq_len = (int64_t)tq.data.size();
+    }
+    check_engine(qpsdm_set_line(eng, &lp), eng, "set_line");
+
+    for (int iblock = 0; iblock < nblock; ++iblock) {
+      const int ixstart = iblock * nxb1, ixend = iblock == nblock - 1 ? nxi : (iblock + 1) * nxb1;
+      const int nxb = ixend - ixstart;
+      img.assign((size_t)nxb * nzi, 0.0f);
+      for (int id = 0; id < ndata; ++id) {
+        const std::string outputpath =
+            pp.projpath + "/" + std::to_string(id) + "/" + pp.task + "/result";
+        const std::string node_i = node0 + "_" + std::to_string(id);
+        offspath = pp.projpath + "/data" + std::to_string(id);
+        infopath = pp.projpath + "/" + std::to_string(id) + "/" + pp.task;
+        for (size_t k = 0; k < offmin[id].size(); ++k) {
+          const std::string out = outputpath + "/" + node_i + ".off" + std::to_string(k) + ".L" +
+                                  std::to_string(line) + ".su";
+          if (iblock == 0 && exists(out)) unlink(out.c_str());
+          float tm = mute_depth(mute, offmin[id][k]);
+          if (tm < 0) tm = 0;
+          if (tm < zmin) tm = zmin;
+          if ((int)(tm / dzi) > nzi) {
+            logf("Warn: Offset=%f is greater than the offset mute parameter: no image\n", tm);
+            continue;
+          }
+          qpsdm_offset_params op;
+          check_engine(qpsdm_offset_params_init(&sp, ixstart, ixend, &op), eng, "offset params");
+          op.ioffs = (int)k;
+          for (int a = 0; a < QPSDM_NAZ; ++a) {
+            op.aznx1[a] = op.aznx2[a] = aperx;
+            op.azny1[a] = op.azny2[a] = apery;
+          }
+          op.zero_image = opcrp;
+          check_engine(qpsdm_begin_offset(eng, &op), eng, "begin_offset");
+          std::vector<std::string> files;
+          for (int l = ioffl1; l <= ioffl2; ++l)
+            files.push_back(offspath + "/off" + std::to_string(k) + "/line" + std::to_string(l));
+          prod.start(files);
+          int b, n;
+          while (prod.next(b, n)) {
+            check_engine(qpsdm_submit_traces(eng, prod.data(b), n, ntl, 1), eng, "submit_traces");
+            prod.release(b);
+          }
+          prod.join();
+          if (!opcrp) continue;  // no crp output: the image keeps accumulating
+          check_engine(qpsdm_get_image(eng, img.data(), 1), eng, "get_image");
+          // append the block's traces (src/q-psdm.cu:1766-1806)
+          mkdir((pp.projpath + "/" + std::to_string(id)).c_str(), 0755);
+          mkdir(infopath.c_str(), 0755);
+          mkdir(outputpath.c_str(), 0755);
+          FILE *fo = std::fopen(out.c_str(), "ab");
+          if (!fo) die("On [%s], File [%s] Open Error: %s", node_i.c_str(), out.c_str(), std::strerror(errno));
+          std::vector<uint8_t> rec(kHdr + 4 * (size_t)nzi);
+          int tracl = 0;
+          for (int c : cdps) {
+            const int ixi = c - cdp1;
+            if (ixi < ixstart || ixi >= ixend) continue;
+            std::memset(rec.data(), 0, kHdr);
+            put_i32(rec.data() + oTracl, ++tracl);
+            put_i32(rec.data() + oFldr, line);
+            put_i32(rec.data() + oCdp, fci + ixi);
+            put_i16(rec.data() + oTrid, 1);
+            put_i16(rec.data() + oNvs, 1);
+            put_i32(rec.data() + oOffset, (int32_t)offmin[id][k]);
+            put_i16(rec.data() + oScalco, vel_scalco);
+            put_i32(rec.data() + oSx, csx[ixi]);
+            put_i32(rec.data() + oSy, csy[ixi]);
+            put_i32(rec.data() + oGx, csx[ixi]);
+            put_i32(rec.data() + oGy, csy[ixi]);
+            put_i16(rec.data() + oCounit, 1);
+            put_i16(rec.data() + oNs, (int16_t)nzi);
+            put_i16(rec.data() + oDt, (int16_t)(int)(dzi * 1.0E3f));
+            const float *col = img.data() + (size_t)(ixi - ixstart) * nzi;
+            for (int z = 0; z < nzi; ++z) {
+              uint32_t u;
+              std::memcpy(&u, col + z, 4);
+              put_i32(rec.data() + kHdr + 4 * z, (int32_t)u);
+            }
+            std::fwrite(rec.data(), 1, rec.size(), fo);
+          }
+          std::fclose(fo);
+          logf("Write Image(crp) To Disk For Line %d:%s\n", line, out.c_str());
+        }
+      }
+    }
+    // checkpoint markers (src/q-psdm.cu:1820-1831)
+    touch(offspath + "/break_point.txt", std::to_string(line) + "\n");
+    touch(infopath + "/" + node0 + "_" + std::to_string(ndata - 1) + "_" + std::to_string(line),
+          "");
+    logf("Time Elapse of Line-%d:%.0fs\n", line, std::difftime(std::time(nullptr), tic));
+  }
+  touch(pp.projpath + "/0/" + pp.task + "/" + node0, "");
+  int64_t acc = 0, npt = 0;
+  qpsdm_get_counters(eng, &acc, &npt);
+  logf("%s: All Migration Work Done (%lld traces accepted, %lld point-traces)\n", nodename.c_str(),
+       (long long)acc, (long long)npt);
+  qpsdm_engine_destroy(eng);
+  std::fclose(vf);
+  return 0;
+}

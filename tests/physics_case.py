@@ -49,7 +49,9 @@ def gate(case):
     az = case["az"]
     keep = [np.ascontiguousarray(O.iaztab(), np.int32)] + [np.ascontiguousarray(az[i]) for i in range(4)]
     ip = lambda x: x.ctypes.data_as(C.POINTER(C.c_int))
-    gp = O.GateParams(scaled=sv.scaled, fxv1=np.float32(sv.fxv - 2000.0),
+    # the data scale: the survey's, or a caller's (the driver takes it from
+    # getscale in single precision, as the reference)
+    gp = O.GateParams(scaled=case.get("scaled", sv.scaled), fxv1=np.float32(sv.fxv - 2000.0),
                       fyv1=np.float32(sv.fyv - 1000.0),
                       exv1=np.float32(sv.fxv + sv.nxi * sv.dxi + 2000.0),
                       eyv1=np.float32(sv.fyv + sv.nyi * sv.dyi + 1000.0), fxi=case["fxi"],
