@@ -99,8 +99,11 @@ typedef struct {
  * lookups per point-trace (source terms reused while consecutive traces share
  * a source).  BATCHED: traces of a batch grouped by receiver position and
  * source; source terms built once per shot and image tile, receiver terms
- * once per receiver position, a persistent kernel over image tiles, and t*
- * panels stored as neighbouring-bin pairs. */
+ * once per receiver position, a persistent kernel over image tiles; t*
+ * panels computed once per trace and shared by every line of a brick
+ * (qpsdm_set_lines).  FP16 panels are scaled per trace by a power of two
+ * from a bound on the trace's filtered amplitude, so any data amplitude
+ * stays inside FP16's range. */
 enum { QPSDM_FORM_PLAIN = 0, QPSDM_FORM_BATCHED = 1 };
 
 /* Per-line state: mirrors the line part of CPUParamsWithLine
