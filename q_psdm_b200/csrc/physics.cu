@@ -72,7 +72,7 @@ struct PhysicsState {
   void *d_cub = nullptr;
   size_t cub_bytes = 0;
   int num_sms = 0;
-  int tile_z = 0, tile_x = 0, src_chunk = 16;
+  int tile_z = 0, tile_x = 0;
   int variant = -1;          // batched kernel variant (autotuned)
   float *d_tune = nullptr;   // scratch image of the autotuner
   size_t tune_cap = 0;
@@ -786,10 +786,14 @@ __global__ void k_batch_members(const uint8_t *__restrict__ rec, int rec_bytes, 
   }
 }
 
-// Source terms kept per (source, point) in shared memory, as three float2
-// planes [plane][source][point]: (T, t*), (CS = ds^3 / ts, AX), (AY, AZ),
-// A = the unit vector from the point to the source.
-enum { kMapTQ = 0, kMapCA, kMapYZ, kMapN };
+// Source terms kept per (source, point) in shared memory, as four float2
+// planes [plane][source][point]: (T, t*), (CS = ds^3 / ts, AZ), (PX1, PX2),
+// (PY1, PY2), with A the unit vector from the point to the source and
+//   PX1 = AX - tanx1c AZ, PX2 = tanx2c AZ - AX   (PY likewise with tany)
+// so that the dip test of a (source, receiver) pair needs no division: for
+// uz = AZ + AZg > 0, tanx1c < ux / uz < tanx2c is PX1 > tanx1c AZg - AXg and
+// PX2 > AXg - tanx2c AZg (the receiver's thresholds, once per receiver).
+enum { kMapTQ = 0, kMapCZ, kMapPX, kMapPY, kMapN };
 
 template <int TZ, int TX, int MB, typename T>
 __global__ void __launch_bounds__(TZ *TX, MB)
@@ -854,19 +858,22 @@ __global__ void __launch_bounds__(TZ *TX, MB)
         float ts, qs;
         float2 *m = smap + (size_t)s * NT + tid;
         if (!lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, sp.x, sp.y, ts, qs)) {
-          // no table value: NaN directions fail every member's dip test
+          // no table value: NaN fails every member's dip test
           m[kMapTQ * sc * NT] = make_float2(NAN, 0.0f);
-          m[kMapCA * sc * NT] = make_float2(0.0f, NAN);
-          m[kMapYZ * sc * NT] = make_float2(NAN, NAN);
+          m[kMapCZ * sc * NT] = make_float2(0.0f, NAN);
+          m[kMapPX * sc * NT] = make_float2(NAN, NAN);
+          m[kMapPY * sc * NT] = make_float2(NAN, NAN);
           continue;
         }
         const float dsx = sp.x - x;
         const float ds = sqrtf(dsx * dsx + sp.y * sp.y + z2);
         const float rds = __fdividef(1.0f, ds);
+        const float ax = dsx * rds, ay = sp.y * rds, az = z * rds;
         m[kMapTQ * sc * NT] = make_float2(ts, qs);
         // source factor of (ds/dg)^3 tg/ts
-        m[kMapCA * sc * NT] = make_float2(__fdividef(ds * ds * ds, ts), dsx * rds);
-        m[kMapYZ * sc * NT] = make_float2(sp.y * rds, z * rds);
+        m[kMapCZ * sc * NT] = make_float2(__fdividef(ds * ds * ds, ts), az);
+        m[kMapPX * sc * NT] = make_float2(fmaf(-tanx1c, az, ax), fmaf(tanx2c, az, -ax));
+        m[kMapPY * sc * NT] = make_float2(fmaf(-tany1c, az, ay), fmaf(tany2c, az, -ay));
       }
       for (int g = 0; g < ngroups; ++g) {
         const int4 gr = __ldg(grp + 2 * g);
@@ -880,8 +887,11 @@ __global__ void __launch_bounds__(TZ *TX, MB)
         const float dgx = gp.x - x;
         const float dg = sqrtf(dgx * dgx + gp.y * gp.y + z2);
         const float rdg = __fdividef(1.0f, dg);
-        // no receiver table value: a NaN direction fails every member's dip test
-        const float agx = rok ? dgx * rdg : NAN, agy = gp.y * rdg, agz = z * rdg;
+        const float agx = dgx * rdg, agy = gp.y * rdg, agz = z * rdg;
+        // dip-test thresholds of this receiver (NaN: no table value, every
+        // member fails)
+        const float qx1 = rok ? fmaf(tanx1c, agz, -agx) : NAN, qx2 = fmaf(-tanx2c, agz, agx);
+        const float qy1 = fmaf(tany1c, agz, -agy), qy2 = fmaf(-tany2c, agz, agy);
         const float gfac = tg * rdg * rdg * rdg;  // receiver factor of (ds/dg)^3 tg/ts
         // Members in blocks of U.  Phase 1, without branches, for all U: the
         // member record, the aperture check (counted), the source direction
@@ -897,7 +907,6 @@ __global__ void __launch_bounds__(TZ *TX, MB)
             mi[u] = p0 + u < gr.y ? __ldg(mem + p0 + u) : make_int4(0, -1, 1, 0);
           bool on[U];
           int slv[U];
-          float tnx[U], tny[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const int sl = (mi[u].y & 0xFFFFFF) - s0;
@@ -905,15 +914,8 @@ __global__ void __launch_bounds__(TZ *TX, MB)
             cnt += inr ? 1u : 0u;
             slv[u] = inr ? sl : 0;
             const float2 *m = smap + (size_t)slv[u] * NT + tid;
-            const float2 ca = m[kMapCA * sc * NT], yz = m[kMapYZ * sc * NT];
-            const float ux = ca.y + agx;
-            const float uy = yz.x + agy;
-            const float uz = yz.y + agz;
-            const float ruz = __fdividef(1.0f, uz);
-            tnx[u] = ux * ruz;
-            tny[u] = uy * ruz;
-            on[u] = inr && tnx[u] > tanx1c && tnx[u] < tanx2c && tny[u] > tany1c &&
-                    tny[u] < tany2c;
+            const float2 px = m[kMapPX * sc * NT], py = m[kMapPY * sc * NT];
+            on[u] = inr && px.x > qx1 && px.y > qx2 && py.x > qy1 && py.y > qy2;
           }
           const T *pp[U];
           float fwt[U], fwb[U], fac[U];
@@ -924,9 +926,15 @@ __global__ void __launch_bounds__(TZ *TX, MB)
             if (!on[u]) continue;
             on[u] = false;
             const float2 *m = smap + (size_t)slv[u] * NT + tid;
-            const float2 tq = m[kMapTQ * sc * NT];
+            const float2 tq = m[kMapTQ * sc * NT], cz = m[kMapCZ * sc * NT];
             const float ts = tq.x;
-            const float tanx = tnx[u], tany = tny[u];
+            // the pair's dip tangents (for the taper) from the stored terms
+            const float azs = cz.y;
+            const float uz = azs + agz;
+            const float ux = fmaf(tanx1c, azs, m[kMapPX * sc * NT].x) + agx;
+            const float uy = fmaf(tany1c, azs, m[kMapPY * sc * NT].x) + agy;
+            const float ruz = __fdividef(1.0f, uz);
+            const float tanx = ux * ruz, tany = uy * ruz;
             float w = 1.0f;
             if (tanx < tanx1) w *= (tanx - tanx1c) / (tanx1 - tanx1c);
             if (tanx > tanx2) w *= (tanx2c - tanx) / (tanx2c - tanx2);
@@ -943,7 +951,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
             pp[u] = panels + (size_t)mi[u].x * pstride + (unsigned)(b0 * a.nt + it1);
             // w v (r + 1/r), v = 100 / t^2 (10^4 below 0.1 s), with one reciprocal:
             // w (r^2 + 1) * 100 / (r t^2)
-            const float r = m[kMapCA * sc * NT].x * gfac;
+            const float r = cz.x * gfac;
             const bool far = t > 0.1f;
             fac[u] = w * fmaf(r, r, 1.0f) * __fdividef(far ? 100.0f : 10000.0f, far ? r * t * t : r);
             if (std::is_same<T, __half>::value)  // 2^e from the record's exponent bits
@@ -1039,23 +1047,26 @@ struct LineView {
 };
 
 // Launch variants of the batched kernel: image tile (depth x cdps, one
-// thread per point, a warp along depth) and the minimum resident blocks per SM
-// the register allocation is held to.  The autotuner times them all on the
-// first batch and keeps the fastest.
+// thread per point, a warp along depth), the minimum resident blocks per SM
+// the register allocation is held to, and the sources per shared-memory
+// chunk (more sources per chunk: fewer passes over the receiver groups, more
+// shared memory per block).  The autotuner times them all on the first batch
+// and keeps the fastest.
 struct BatchedVariant {
-  int tz, tx, mb;
+  int tz, tx, mb, sc;
 };
 static const BatchedVariant kVariants[] = {
-    {32, 8, 2}, {32, 8, 3}, {32, 4, 4}, {32, 4, 6}, {64, 4, 2}, {64, 4, 3}, {128, 2, 2},
+    {32, 8, 2, 8},  {32, 8, 3, 8},  {32, 4, 4, 8},  {32, 4, 6, 8},  {64, 4, 2, 8},
+    {64, 4, 3, 8},  {128, 2, 2, 8}, {32, 4, 4, 16}, {32, 4, 3, 16}, {32, 8, 2, 16},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 template <int TZ, int TX, int MB, typename T>
 static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
                                const LineView &v, float *img, float *comp,
-                               unsigned long long *npt, cudaStream_t st) {
+                               unsigned long long *npt, int sc, cudaStream_t st) {
   const int ntz = (a.nzi + TZ - 1) / TZ, ntx = (a.nxb + TX - 1) / TX;
-  const size_t smem = sizeof(float2) * kMapN * (size_t)s->src_chunk * TZ * TX;
+  const size_t smem = sizeof(float2) * kMapN * (size_t)sc * TZ * TX;
   auto kern = k_image_batched<TZ, TX, MB, T>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
@@ -1067,7 +1078,7 @@ static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const Ph
   kern<<<grid, TZ * TX, smem, st>>>(img, comp, a, v.dips, s->d_grp, s->d_grppos, s->d_nruns,
                                     s->d_mem, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
                                     v.tab->ttt, v.tab->dq, v.tab->qqq, (const T *)s->d_panels,
-                                    s->d_tile_ctr, ntz, ntx, s->src_chunk, npt);
+                                    s->d_tile_ctr, ntz, ntx, sc, npt);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
 
@@ -1075,14 +1086,18 @@ template <typename T>
 static int launch_variant(int vi, PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
                           const LineView &v, float *img, float *comp, unsigned long long *npt,
                           cudaStream_t st) {
+  const int sc = kVariants[vi].sc;
   switch (vi) {
-    case 0: return launch_batched_tile<32, 8, 2, T>(s, a, b, v, img, comp, npt, st);
-    case 1: return launch_batched_tile<32, 8, 3, T>(s, a, b, v, img, comp, npt, st);
-    case 2: return launch_batched_tile<32, 4, 4, T>(s, a, b, v, img, comp, npt, st);
-    case 3: return launch_batched_tile<32, 4, 6, T>(s, a, b, v, img, comp, npt, st);
-    case 4: return launch_batched_tile<64, 4, 2, T>(s, a, b, v, img, comp, npt, st);
-    case 5: return launch_batched_tile<64, 4, 3, T>(s, a, b, v, img, comp, npt, st);
-    default: return launch_batched_tile<128, 2, 2, T>(s, a, b, v, img, comp, npt, st);
+    case 0: return launch_batched_tile<32, 8, 2, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 1: return launch_batched_tile<32, 8, 3, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 2: return launch_batched_tile<32, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 3: return launch_batched_tile<32, 4, 6, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 4: return launch_batched_tile<64, 4, 2, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 5: return launch_batched_tile<64, 4, 3, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 6: return launch_batched_tile<128, 2, 2, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 7: return launch_batched_tile<32, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 8: return launch_batched_tile<32, 4, 3, T>(s, a, b, v, img, comp, npt, sc, st);
+    default: return launch_batched_tile<32, 8, 2, T>(s, a, b, v, img, comp, npt, sc, st);
   }
 }
 

@@ -97,11 +97,12 @@ def test_batched_matches_fp64(cuda, case, dtype, tol, tile):
 
 
 def test_batched_many_shots_and_splits(cuda):
-    # 11 shots exceed one source chunk of the batched kernel; irregular split
+    # 11 shots exceed one source chunk (8 sources with the forced 32 x 4 tile);
+    # irregular split
     c = make_case(shots=range(2, 13), rstep=8, half_x=50, half_y=40)
     ref, npt, _ = oracle_run(c)
     rec = records(c)
-    eng, p, o = engine(c, form=1, max_batch=1000, kahan=1)
+    eng, p, o = engine(c, form=1, max_batch=1000, kahan=1, tile=(32, 4))
     try:
         eng.submit(rec[:333])
         eng.submit(rec[333:])
