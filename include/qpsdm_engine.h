@@ -202,6 +202,15 @@ int qpsdm_submit_traces_device(qpsdm_engine *e, const void *d_records, int ntr,
  * device-side error. */
 int qpsdm_fence(qpsdm_engine *e);
 
+/* Lines of the current brick (qpsdm_set_lines) that the following submits
+ * feed: bit il selects line il (lines from 64 on always take every batch);
+ * default all.  The reference reads, for each image line, only the data
+ * lines within +-extxline of it (src/q-psdm.cu:1432-1435, :1882-1886); a
+ * driver imaging a brick in one pass sets, before each data line's traces,
+ * the image lines that data line belongs to.  No counterpart in the
+ * reference, which images one line per pass. */
+int qpsdm_set_line_mask(qpsdm_engine *e, unsigned long long mask);
+
 /* Replaces the D2H + host sum + /nsb of qpsdm() (src/q-psdm.cu:1745-1765).
  * host_img: [nxb][nzi] floats (nxb = ixend - ixstart). */
 int qpsdm_get_image(qpsdm_engine *e, float *host_img, int apply_nsb_scale);

@@ -103,6 +103,7 @@ SYMBOLS = [
     ("qpsdm_submit_traces", _I, [_P, _P, _I, _I, _I]),
     ("qpsdm_submit_traces_device", _I, [_P, _P, _I, _I, _I]),
     ("qpsdm_fence", _I, [_P]),
+    ("qpsdm_set_line_mask", _I, [_P, C.c_ulonglong]),
     ("qpsdm_get_image", _I, [_P, _P, _I]),
     ("qpsdm_image_device_ptr", _I, [_P, C.POINTER(C.c_void_p)]),
     ("qpsdm_set_stream", _I, [_P, _P]),

@@ -29,6 +29,7 @@ using namespace qpsdm;
 
 struct qpsdm_engine {
   int device = 0;
+  unsigned long long line_mask = ~0ull;  // lines of the brick the next batches feed
   qpsdm_static_params p{};
   std::string err;
   cudaStream_t s_comp = nullptr, s_copy = nullptr;
@@ -71,7 +72,7 @@ struct qpsdm_engine {
     cudaGraphExec_t exec;
     int64_t launches[4];
   };
-  std::map<std::tuple<const void *, int, int>, GraphRec> graphs;
+  std::map<std::tuple<const void *, int, int, unsigned long long>, GraphRec> graphs;
   int64_t batches_run = 0;
   int64_t graph_replays = 0;
 };
@@ -320,8 +321,10 @@ int process_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
   const size_t ints_ls = (size_t)kGateInts * e->p.max_batch;  // per-line strides
   const size_t geom_ls = (size_t)kGateF * e->p.max_batch;
   const size_t img_ls = (size_t)nxb * e->p.nzi;
+  auto line_on = [&](int il) { return il >= 64 || ((e->line_mask >> il) & 1ull); };
   // gate every line of the brick (src/q-psdm.cu:2107-2171 for each line's cyi)
   for (int il = 0; il < nlines; ++il) {
+    if (!line_on(il)) continue;
     const qpsdm_line_params &ln = e->lines[il];
     GateArgs g{};
     g.scaled = e->p.scaled;
@@ -352,6 +355,7 @@ int process_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
   if (e->p.mode == QPSDM_MODE_COMPAT) {
     // the reference preprocesses and images each trace once per line
     for (int il = 0; il < nlines; ++il) {
+      if (!line_on(il)) continue;
       const qpsdm_line_params &ln = e->lines[il];
       SpectraArgs a{};
       a.ntl = e->p.ntl;
@@ -407,6 +411,7 @@ int process_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
   b.d_npt = e->d_npt;
   b.d_err = e->d_err;
   b.prof = &e->prof;
+  b.line_mask = e->line_mask;
   return physics_process(e->phys, e->p, e->lines.data(), e->off, b, e->s_comp, &e->err);
 }
 
@@ -424,7 +429,7 @@ int run_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
     ++e->batches_run;
     return process_batch(e, d_rec, ntr, be);
   }
-  const auto key = std::make_tuple((const void *)d_rec, ntr, be);
+  const auto key = std::make_tuple((const void *)d_rec, ntr, be, e->line_mask);
   auto it = e->graphs.find(key);
   if (it != e->graphs.end()) {
     CK(cudaGraphLaunch(it->second.exec, e->s_comp));
@@ -508,6 +513,13 @@ extern "C" int qpsdm_submit_traces(qpsdm_engine *e, const void *records, int ntr
     src += bytes;
     ntr -= n;
   }
+  return QPSDM_OK;
+}
+
+extern "C" int qpsdm_set_line_mask(qpsdm_engine *e, unsigned long long mask) {
+  if (!e) return QPSDM_EINVAL;
+  if (mask == 0) return fail(e, QPSDM_EINVAL, "line mask selects no line");
+  e->line_mask = mask;
   return QPSDM_OK;
 }
 

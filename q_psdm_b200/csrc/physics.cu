@@ -1195,12 +1195,13 @@ static int batched_group(PhysicsState *s, const qpsdm_static_params &p, const Li
 
 // Any line of the brick accepted the trace: its panels are needed.
 __global__ void k_any_line(const int *__restrict__ ints, size_t ints_ls, int nlines, int ntr,
-                           int *__restrict__ any) {
+                           unsigned long long mask, int *__restrict__ any) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ntr) return;
   int a = 0;
   for (int il = 0; il < nlines; ++il)
-    a |= ints[il * ints_ls + (size_t)i * kGateInts] == kAccepted;
+    if (il >= 64 || ((mask >> il) & 1ull))
+      a |= ints[il * ints_ls + (size_t)i * kGateInts] == kAccepted;
   any[i] = a ? kAccepted : 0;
 }
 
@@ -1301,6 +1302,7 @@ int physics_process(PhysicsState *s, const qpsdm_static_params &p,
   if (s->form == QPSDM_FORM_PLAIN) {
     // as the reference: each line preprocesses its accepted traces again
     for (int il = 0; il < b.nlines && !rc; ++il) {
+      if (!batch_line_on(b, il)) continue;
       const LineView v = view(il);
       b.prof->begin(QPSDM_K_PRE, st);
       rc = run_panels(s, p, b, v.ints, kGateInts, st, err);
@@ -1324,11 +1326,12 @@ int physics_process(PhysicsState *s, const qpsdm_static_params &p,
   // batched: panels once for every trace any line accepted, shared by the brick
   b.prof->begin(QPSDM_K_PRE, st);
   k_any_line<<<(b.ntr + 255) / 256, 256, 0, st>>>(b.d_ints, b.ints_ls, b.nlines, b.ntr,
-                                                  s->d_any);
+                                                  b.line_mask, s->d_any);
   rc = run_panels(s, p, b, s->d_any, 1, st, err);
   b.prof->end(st);
   if (rc) return rc;
   for (int il = 0; il < b.nlines; ++il) {
+    if (!batch_line_on(b, il)) continue;
     const LineView v = view(il);
     b.prof->begin(QPSDM_K_OTHER, st);
     rc = batched_group(s, p, v, b, st);

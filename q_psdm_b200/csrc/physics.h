@@ -30,7 +30,13 @@ struct PhysicsBatch {
   unsigned long long *d_npt;
   unsigned *d_err;
   KernelProfiler *prof;
+  unsigned long long line_mask;  // bit il: line il of the brick takes this batch
 };
+
+// Line il of a brick takes the batch (lines past 64 always do).
+inline bool batch_line_on(const PhysicsBatch &b, int il) {
+  return il >= 64 || ((b.line_mask >> il) & 1ull);
+}
 
 int physics_create(PhysicsState **out, const qpsdm_static_params &p, std::string *err);
 void physics_destroy(PhysicsState *s);

@@ -28,6 +28,10 @@
 //   dzii                    table depth-node spacing (default 48 m as the
 //                           reference derives it, src/q-psdm.cu:880-882)
 //   max_batch               traces per submit (default 16384)
+//   brick=N                 image N consecutive lines of the line list in one
+//                           pass over the data (default 1, as the reference;
+//                           each data line still feeds only the image lines
+//                           within +-extxline of it)
 //   resume=1                skip the lines up to <offspath>/break_point.txt
 //   check=1                 resolve and print the parameters, image nothing
 // Errors print a message and exit 1, as the reference does; the library
@@ -380,18 +384,19 @@ class Producer {
     if (th_.joinable()) th_.join();
     for (auto *p : bufs_) cudaFreeHost(p);
   }
-  // start reading the files in order
-  void start(std::vector<std::string> files) {
+  // start reading the files (path, data line) in order
+  void start(std::vector<std::pair<std::string, int>> files) {
     done_ = false;
     th_ = std::thread([this, files] { run(files); });
   }
-  // next filled buffer (index, traces); false when all files are read
-  bool next(int &buf, int &ntr) {
+  // next filled buffer (index, traces, data line); false when all are read
+  bool next(int &buf, int &ntr, int &line) {
     std::unique_lock<std::mutex> lk(mu_);
     cv_.wait(lk, [&] { return !full_.empty() || done_; });
     if (full_.empty()) return false;
-    buf = full_.front().first;
-    ntr = full_.front().second;
+    buf = full_.front().buf;
+    ntr = full_.front().n;
+    line = full_.front().line;
     full_.pop_front();
     return true;
   }
@@ -409,8 +414,9 @@ class Producer {
   long traces_read = 0;
 
  private:
-  void run(std::vector<std::string> files) {
-    for (const auto &f : files) {
+  void run(std::vector<std::pair<std::string, int>> files) {
+    for (const auto &fl : files) {
+      const std::string &f = fl.first;
       FILE *fp = std::fopen(f.c_str(), "rb");
       if (!fp) continue;  // a missing data line contributes nothing
       struct stat st;
@@ -431,7 +437,7 @@ class Producer {
         traces_read += n;
         {
           std::lock_guard<std::mutex> lk(mu_);
-          full_.push_back({b, n});
+          full_.push_back({b, n, fl.second});
         }
         cv_.notify_all();
       }
@@ -447,7 +453,10 @@ class Producer {
   int max_;
   std::vector<uint8_t *> bufs_;
   std::deque<int> free_;
-  std::deque<std::pair<int, int>> full_;
+  struct Filled {
+    int buf, n, line;
+  };
+  std::deque<Filled> full_;
   bool done_ = true;
   std::mutex mu_;
   std::condition_variable cv_;
@@ -515,6 +524,7 @@ int main(int argc, char **argv) {
   const float dtstar = K.flt_or("dtstar", 0.002f);
   const int max_batch = std::max(1, K.int_or("max_batch", 16384));
   const int resume = K.int_or("resume", 0);
+  const int brick = std::min(std::max(1, K.int_or("brick", 1)), 64);
   const int check_only = K.int_or("check", 0);
   if (engine_mode != "compat" && engine_mode != "physics") die("engine must be compat or physics");
   if (form != "plain" && form != "batched") die("form must be plain or batched");
@@ -702,63 +712,78 @@ int main(int argc, char **argv) {
     logf("resume: starting at line index %zu\n", first);
   }
 
+  // Lines are imaged `brick` at a time (engine bricks: one pass over the data
+  // for all of them; in the batched physics form each trace's t* panels are
+  // shared).  Each data-line file feeds only the brick's image lines within
+  // +-extxline of it, as the reference's per-line passes do.
+  const int16_t vel_scalco = be_i16(v0.h + oScalco);
   std::vector<float> img;
-  for (size_t iyi = first; iyi < lines.size(); ++iyi) {
-    const int line = lines[iyi];
+  for (size_t b0 = first; b0 < lines.size(); b0 += brick) {
+    const int nl = (int)std::min((size_t)brick, lines.size() - b0);
     const time_t tic = std::time(nullptr);
-    const double fxi = fxv + (double)((float)(fci - fcv) * dxi);  // src/q-psdm.cu:1430-1431
-    const double cyi = fyv + (double)((float)(line - flv) * dyi);
-    logf("Start Image Line:%d\n", line);
-    const int ioffl1 = std::max(line - xline, line1), ioffl2 = std::min(line + xline, line2);
-    // output coordinates from the velocity file (get_vel_coor, src/psdmpkg.cc:979-1011)
-    std::vector<int32_t> csx(nxi), csy(nxi);
-    const int16_t vel_scalco = be_i16(v0.h + oScalco);
-    {
+    std::vector<int> bl(lines.begin() + b0, lines.begin() + b0 + nl);
+    std::vector<std::vector<int32_t>> csx(nl, std::vector<int32_t>(nxi)),
+        csy(nl, std::vector<int32_t>(nxi));
+    std::vector<Tables> tt(nl), tq(nl);
+    std::vector<qpsdm_line_params> lps(nl);
+    for (int j = 0; j < nl; ++j) {
+      const int line = bl[j];
+      logf("Start Image Line:%d\n", line);
+      // output coordinates from the velocity file (get_vel_coor, src/psdmpkg.cc:979-1011)
       const int vl = std::min(line, flv + nyv - 1);
       for (int i = 0; i < nxi; ++i) {
         TraceHdr t;
         if (!read_header(vf, (long)(vl - flv) * nxv + fci - fcv + i, ntv, t))
           die("velocity file too short for line %d", line);
-        csx[i] = be_i32(t.h + oSx);
-        csy[i] = be_i32(t.h + oSy);
+        csx[j][i] = be_i32(t.h + oSx);
+        csy[j][i] = be_i32(t.h + oSy);
+      }
+      // tables (required in physics mode)
+      const bool have_t = load_tables(ttpath, false, line, line1, line2, tt[j]);
+      const bool have_q = have_t && load_tables(ttpath, true, line, line1, line2, tq[j]);
+      if (sp.mode == QPSDM_MODE_PHYSICS && !(have_t && have_q))
+        die("physics mode needs %s/Lxxx.tidx and Lxxx.qidx", ttpath.c_str());
+      if (have_q && (tt[j].cdp1 != tq[j].cdp1 || tt[j].cdp2 != tq[j].cdp2 ||
+                     tt[j].cdp1 >= tt[j].cdp2))
+        die("travel time table cdp range error, or not confirm with qfield");
+      qpsdm_line_params &lp = lps[j];
+      std::memset(&lp, 0, sizeof lp);
+      lp.fxi = fxv + (double)((float)(fci - fcv) * dxi);  // src/q-psdm.cu:1430-1431
+      lp.cyi = fyv + (double)((float)(line - flv) * dyi);
+      lp.dipx1 = dx1.data();
+      lp.dipx2 = dx2.data();
+      lp.dipy1 = dx1.data();
+      lp.dipy2 = dx2.data();
+      if (have_q) {
+        lp.nxg = tt[j].nxg;
+        lp.nzg = tt[j].nzg;
+        lp.nxi1 = tt[j].nxi1;
+        lp.nzi1 = tt[j].nzi1;
+        lp.ttt_cdp1 = tt[j].cdp1;
+        lp.ttt_cdp2 = tt[j].cdp2;
+        lp.ttt_desc = tt[j].desc.data();
+        lp.qqq_desc = tq[j].desc.data();
+        lp.ttt = tt[j].data.data();
+        lp.qqq = tq[j].data.data();
+        lp.ttt_len = (int64_t)tt[j].data.size();
+        lp.qqq_len = (int64_t)tq[j].data.size();
       }
     }
-    // tables (required in physics mode)
-    Tables tt, tq;
-    const bool have_t = load_tables(ttpath, false, line, line1, line2, tt);
-    const bool have_q = have_t && load_tables(ttpath, true, line, line1, line2, tq);
-    if (sp.mode == QPSDM_MODE_PHYSICS && !(have_t && have_q))
-      die("physics mode needs %s/Lxxx.tidx and Lxxx.qidx", ttpath.c_str());
-    if (have_q && (tt.cdp1 != tq.cdp1 || tt.cdp2 != tq.cdp2 || tt.cdp1 >= tt.cdp2))
-      die("travel time table cdp range error, or not confirm with qfield");
-    qpsdm_line_params lp;
-    std::memset(&lp, 0, sizeof lp);
-    lp.fxi = fxi;
-    lp.cyi = cyi;
-    lp.dipx1 = dx1.data();
-    lp.dipx2 = dx2.data();
-    lp.dipy1 = dx1.data();
-    lp.dipy2 = dx2.data();
-    if (have_q) {
-      lp.nxg = tt.nxg;
-      lp.nzg = tt.nzg;
-      lp.nxi1 = tt.nxi1;
-      lp.nzi1 = tt.nzi1;
-      lp.ttt_cdp1 = tt.cdp1;
-      lp.ttt_cdp2 = tt.cdp2;
-      lp.ttt_desc = tt.desc.data();
-      lp.qqq_desc = tq.desc.data();
-      lp.ttt = tt.data.data();
-      lp.qqq = tq.data.data();
-      lp.ttt_len = (int64_t)tt.data.size();
-      lp.qqq_len = (int64_t)tq.data.size();
+    check_engine(qpsdm_set_lines(eng, lps.data(), nl), eng, "set_lines");
+    // the data lines some image line of the brick reads, and which ones
+    // (src/q-psdm.cu:1432-1435: line +- extxline inside [line1, line2])
+    std::vector<std::pair<int, unsigned long long>> dlines;
+    for (int l = line1; l <= line2; ++l) {
+      unsigned long long mask = 0;
+      for (int j = 0; j < nl; ++j)
+        if (l >= bl[j] - xline && l <= bl[j] + xline) mask |= 1ull << j;
+      if (mask) dlines.push_back({l, mask});
     }
-    check_engine(qpsdm_set_line(eng, &lp), eng, "set_line");
 
     for (int iblock = 0; iblock < nblock; ++iblock) {
       const int ixstart = iblock * nxb1, ixend = iblock == nblock - 1 ? nxi : (iblock + 1) * nxb1;
       const int nxb = ixend - ixstart;
-      img.assign((size_t)nxb * nzi, 0.0f);
+      img.assign((size_t)nl * nxb * nzi, 0.0f);
       for (int id = 0; id < ndata; ++id) {
         const std::string outputpath =
             pp.projpath + "/" + std::to_string(id) + "/" + pp.task + "/result";
@@ -766,9 +791,12 @@ int main(int argc, char **argv) {
         offspath = pp.projpath + "/data" + std::to_string(id);
         infopath = pp.projpath + "/" + std::to_string(id) + "/" + pp.task;
         for (size_t k = 0; k < offmin[id].size(); ++k) {
-          const std::string out = outputpath + "/" + node_i + ".off" + std::to_string(k) + ".L" +
-                                  std::to_string(line) + ".su";
-          if (iblock == 0 && exists(out)) unlink(out.c_str());
+          std::vector<std::string> out(nl);
+          for (int j = 0; j < nl; ++j) {
+            out[j] = outputpath + "/" + node_i + ".off" + std::to_string(k) + ".L" +
+                     std::to_string(bl[j]) + ".su";
+            if (iblock == 0 && exists(out[j])) unlink(out[j].c_str());
+          }
           float tm = mute_depth(mute, offmin[id][k]);
           if (tm < 0) tm = 0;
           if (tm < zmin) tm = zmin;
@@ -785,62 +813,74 @@ int main(int argc, char **argv) {
           }
           op.zero_image = opcrp;
           check_engine(qpsdm_begin_offset(eng, &op), eng, "begin_offset");
-          std::vector<std::string> files;
-          for (int l = ioffl1; l <= ioffl2; ++l)
-            files.push_back(offspath + "/off" + std::to_string(k) + "/line" + std::to_string(l));
+          std::vector<std::pair<std::string, int>> files;
+          for (const auto &d : dlines)
+            files.push_back({offspath + "/off" + std::to_string(k) + "/line" +
+                                 std::to_string(d.first), d.first});
           prod.start(files);
-          int b, n;
-          while (prod.next(b, n)) {
+          int b, n, dl;
+          size_t di = 0;
+          while (prod.next(b, n, dl)) {
+            while (di < dlines.size() && dlines[di].first != dl) ++di;
+            if (nl > 1) check_engine(qpsdm_set_line_mask(eng, dlines[di].second), eng, "line mask");
             check_engine(qpsdm_submit_traces(eng, prod.data(b), n, ntl, 1), eng, "submit_traces");
             prod.release(b);
           }
           prod.join();
+          if (nl > 1) check_engine(qpsdm_set_line_mask(eng, ~0ull), eng, "line mask");
           if (!opcrp) continue;  // no crp output: the image keeps accumulating
           check_engine(qpsdm_get_image(eng, img.data(), 1), eng, "get_image");
-          // append the block's traces (src/q-psdm.cu:1766-1806)
+          // append each line's block traces (src/q-psdm.cu:1766-1806)
           mkdir((pp.projpath + "/" + std::to_string(id)).c_str(), 0755);
           mkdir(infopath.c_str(), 0755);
           mkdir(outputpath.c_str(), 0755);
-          FILE *fo = std::fopen(out.c_str(), "ab");
-          if (!fo) die("On [%s], File [%s] Open Error: %s", node_i.c_str(), out.c_str(), std::strerror(errno));
           std::vector<uint8_t> rec(kHdr + 4 * (size_t)nzi);
-          int tracl = 0;
-          for (int c : cdps) {
-            const int ixi = c - cdp1;
-            if (ixi < ixstart || ixi >= ixend) continue;
-            std::memset(rec.data(), 0, kHdr);
-            put_i32(rec.data() + oTracl, ++tracl);
-            put_i32(rec.data() + oFldr, line);
-            put_i32(rec.data() + oCdp, fci + ixi);
-            put_i16(rec.data() + oTrid, 1);
-            put_i16(rec.data() + oNvs, 1);
-            put_i32(rec.data() + oOffset, (int32_t)offmin[id][k]);
-            put_i16(rec.data() + oScalco, vel_scalco);
-            put_i32(rec.data() + oSx, csx[ixi]);
-            put_i32(rec.data() + oSy, csy[ixi]);
-            put_i32(rec.data() + oGx, csx[ixi]);
-            put_i32(rec.data() + oGy, csy[ixi]);
-            put_i16(rec.data() + oCounit, 1);
-            put_i16(rec.data() + oNs, (int16_t)nzi);
-            put_i16(rec.data() + oDt, (int16_t)(int)(dzi * 1.0E3f));
-            const float *col = img.data() + (size_t)(ixi - ixstart) * nzi;
-            for (int z = 0; z < nzi; ++z) {
-              uint32_t u;
-              std::memcpy(&u, col + z, 4);
-              put_i32(rec.data() + kHdr + 4 * z, (int32_t)u);
+          for (int j = 0; j < nl; ++j) {
+            FILE *fo = std::fopen(out[j].c_str(), "ab");
+            if (!fo)
+              die("On [%s], File [%s] Open Error: %s", node_i.c_str(), out[j].c_str(),
+                  std::strerror(errno));
+            int tracl = 0;
+            for (int c : cdps) {
+              const int ixi = c - cdp1;
+              if (ixi < ixstart || ixi >= ixend) continue;
+              std::memset(rec.data(), 0, kHdr);
+              put_i32(rec.data() + oTracl, ++tracl);
+              put_i32(rec.data() + oFldr, bl[j]);
+              put_i32(rec.data() + oCdp, fci + ixi);
+              put_i16(rec.data() + oTrid, 1);
+              put_i16(rec.data() + oNvs, 1);
+              put_i32(rec.data() + oOffset, (int32_t)offmin[id][k]);
+              put_i16(rec.data() + oScalco, vel_scalco);
+              put_i32(rec.data() + oSx, csx[j][ixi]);
+              put_i32(rec.data() + oSy, csy[j][ixi]);
+              put_i32(rec.data() + oGx, csx[j][ixi]);
+              put_i32(rec.data() + oGy, csy[j][ixi]);
+              put_i16(rec.data() + oCounit, 1);
+              put_i16(rec.data() + oNs, (int16_t)nzi);
+              put_i16(rec.data() + oDt, (int16_t)(int)(dzi * 1.0E3f));
+              const float *col = img.data() + ((size_t)j * nxb + (ixi - ixstart)) * nzi;
+              for (int z = 0; z < nzi; ++z) {
+                uint32_t u;
+                std::memcpy(&u, col + z, 4);
+                put_i32(rec.data() + kHdr + 4 * z, (int32_t)u);
+              }
+              std::fwrite(rec.data(), 1, rec.size(), fo);
             }
-            std::fwrite(rec.data(), 1, rec.size(), fo);
+            std::fclose(fo);
+            logf("Write Image(crp) To Disk For Line %d:%s\n", bl[j], out[j].c_str());
           }
-          std::fclose(fo);
-          logf("Write Image(crp) To Disk For Line %d:%s\n", line, out.c_str());
         }
       }
     }
-    // checkpoint markers (src/q-psdm.cu:1820-1831)
-    touch(offspath + "/break_point.txt", std::to_string(line) + "\n");
-    touch(infopath + "/" + node0 + "_" + std::to_string(ndata - 1) + "_" + std::to_string(line),
-          "");
-    logf("Time Elapse of Line-%d:%.0fs\n", line, std::difftime(std::time(nullptr), tic));
+    // checkpoint markers (src/q-psdm.cu:1820-1831), after each line of the brick
+    for (int j = 0; j < nl; ++j) {
+      touch(offspath + "/break_point.txt", std::to_string(bl[j]) + "\n");
+      touch(infopath + "/" + node0 + "_" + std::to_string(ndata - 1) + "_" +
+                std::to_string(bl[j]), "");
+    }
+    logf("Time Elapse of Lines %d..%d:%.0fs\n", bl.front(), bl.back(),
+         std::difftime(std::time(nullptr), tic));
   }
   touch(pp.projpath + "/0/" + pp.task + "/" + node0, "");
   int64_t acc = 0, npt = 0;

@@ -211,6 +211,10 @@ class Engine:
     def fence(self) -> None:
         self._ck(lib().qpsdm_fence(self.h), "fence")
 
+    def set_line_mask(self, mask: int) -> None:
+        """Lines of the brick (bit il = line il) the following submits feed."""
+        self._ck(lib().qpsdm_set_line_mask(self.h, int(mask) & (2 ** 64 - 1)), "set_line_mask")
+
     def get_image(self, apply_nsb_scale: bool = True) -> np.ndarray:
         """[nxb, nzi] for one line, [nlines, nxb, nzi] for a brick."""
         nxb = self.off.ixend - self.off.ixstart

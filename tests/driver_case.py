@@ -71,7 +71,7 @@ def read_su(path, ns):
 
 
 def make_project(tmp, case, *, image_line, par_extra="", tab=None, tables_at=None,
-                 offsets="0,3000"):
+                 offsets="0,3000", extxline=300):
     """Lay out the project for `case` (a dict with sv, hdr [ntr,4] cm ints,
     traces [ntr,ntl]).  Returns (paths dict, trace order the driver reads)."""
     sv = case["sv"]
@@ -98,7 +98,7 @@ def make_project(tmp, case, *, image_line, par_extra="", tab=None, tables_at=Non
     order = np.concatenate(order)
     tt = os.path.join(tmp, "tt")
     if tab is not None:
-        for L in (tables_at or [image_line]):
+        for L in (tables_at or [int(image_line)]):
             tables.write_line(tt, L, tab)
     else:
         os.makedirs(tt, exist_ok=True)
@@ -115,7 +115,7 @@ dzi={sv.dzi:g}
 cdp1=1
 cdp2={sv.nxi}
 line={image_line}
-extxline=300
+extxline={extxline}
 opcrp=1
 threshold=600
 contract=3
