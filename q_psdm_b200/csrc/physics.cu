@@ -55,6 +55,8 @@ struct PhysicsState {
     size_t dt_cap = 0, dq_cap = 0, ttt_cap = 0, qqq_cap = 0;
   };
   std::vector<LineTab> tabs;  // one per line of the brick
+  float *d_tab_tmp = nullptr;  // batched form: table upload before the re-layout
+  size_t tab_tmp_cap = 0;
   int ntabs = 0;
   int *d_any = nullptr;       // [max_batch] accepted by any line of the brick
   // batched form: grouping scratch (sized for max_batch at create)
@@ -210,6 +212,7 @@ void physics_destroy(PhysicsState *s) {
   }
   cudaFree(s->d_any);
   cudaFree(s->d_tune);
+  cudaFree(s->d_tab_tmp);
   delete s;
 }
 
@@ -251,6 +254,24 @@ static int check_tables(const qpsdm_line_params &l, std::string *err) {
   return QPSDM_OK;
 }
 
+// Batched form: every surface node's [nxi1][nzi1] plane of a table cell
+// (the reference layout, depth fastest) re-laid out as [nzi1][nxi1] (cdp
+// fastest), so that image points of neighbouring cdps, which a warp of the
+// batched kernel holds, read neighbouring table words.  Out of place:
+// descriptors may share a block.
+__global__ void k_tab_xfast(const float *__restrict__ in, float *__restrict__ out,
+                            const qpsdm_ttt_desc *__restrict__ desc, int nxi1, int nzi1) {
+  const qpsdm_ttt_desc d = desc[blockIdx.y];
+  const int nplanes = (int)d.nys * d.nxs, plane = nxi1 * nzi1;
+  for (int pl = blockIdx.x; pl < nplanes; pl += gridDim.x) {
+    const int64_t base = d.idx + (int64_t)pl * plane;
+    for (int e = threadIdx.x; e < plane; e += blockDim.x) {
+      const int ixl = e / nzi1, izl = e - ixl * nzi1;
+      out[base + izl * nxi1 + ixl] = in[base + e];
+    }
+  }
+}
+
 int physics_set_lines(PhysicsState *s, const qpsdm_static_params &p,
                       const qpsdm_line_params *lines, int nlines, cudaStream_t st,
                       std::string *err) {
@@ -272,8 +293,21 @@ int physics_set_lines(PhysicsState *s, const qpsdm_static_params &p,
     }
     cudaMemcpyAsync(t.dt, l.ttt_desc, sizeof(qpsdm_ttt_desc) * ncell, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(t.dq, l.qqq_desc, sizeof(qpsdm_ttt_desc) * ncell, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(t.ttt, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(t.qqq, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyHostToDevice, st);
+    if (s->form == QPSDM_FORM_BATCHED) {
+      if (!grow_dev(&s->d_tab_tmp, &s->tab_tmp_cap,
+                    (size_t)std::max(l.ttt_len, l.qqq_len))) {
+        if (err) *err = "table re-layout scratch allocation failed";
+        return QPSDM_ENOMEM;
+      }
+      const dim3 g(256, (unsigned)ncell);
+      cudaMemcpyAsync(s->d_tab_tmp, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyHostToDevice, st);
+      k_tab_xfast<<<g, 256, 0, st>>>(s->d_tab_tmp, t.ttt, t.dt, l.nxi1, l.nzi1);
+      cudaMemcpyAsync(s->d_tab_tmp, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyHostToDevice, st);
+      k_tab_xfast<<<g, 256, 0, st>>>(s->d_tab_tmp, t.qqq, t.dq, l.nxi1, l.nzi1);
+    } else {
+      cudaMemcpyAsync(t.ttt, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(t.qqq, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyHostToDevice, st);
+    }
   }
   if (cudaStreamSynchronize(st) != cudaSuccess) {
     if (err) *err = "table upload failed";
@@ -435,6 +469,7 @@ struct PhysImageArgs {
   int tcdp1, tcdp2;  // relative to fci
   int nxg, nzg, nxi1, nzi1;
   size_t nxz;
+  int xfast;  // tables stored [izl][ixl] inside each surface node's plane (batched form)
 };
 
 template <typename T>
@@ -451,7 +486,7 @@ __device__ __forceinline__ float ld_sample<__half>(const __half *p) { return __h
 // Table value at one depth node of a cell for surface point (px, py).
 // Returns false outside the cell's surface grid.
 __device__ __forceinline__ bool table_node(const qpsdm_ttt_desc &d, const float *__restrict__ tab,
-                                           float px, float py, float xc, int ixl, int izl,
+                                           float px, float py, float xc, int poff,
                                            int nxi1, int nzi1, float &v) {
   const int nxs = d.nxs, nys = d.nys;
   const float fx = (px - xc) / (float)d.dxs + 0.5f * (nxs - 1);
@@ -463,7 +498,7 @@ __device__ __forceinline__ bool table_node(const qpsdm_ttt_desc &d, const float 
   const float wx = nxs > 1 ? fx - ix : 0.0f, wy = nys > 1 ? fy - iy : 0.0f;
   const int64_t sx = nxs > 1 ? (int64_t)nxi1 * nzi1 : 0;
   const int64_t sy = nys > 1 ? (int64_t)nxs * nxi1 * nzi1 : 0;
-  const int64_t base = d.idx + ((int64_t)(iy * nxs + ix) * nxi1 + ixl) * nzi1 + izl;
+  const int64_t base = d.idx + (int64_t)(iy * nxs + ix) * nxi1 * nzi1 + poff;
   const float v00 = __ldg(tab + base), v01 = __ldg(tab + base + sx);
   const float v10 = __ldg(tab + base + sy), v11 = __ldg(tab + base + sy + sx);
   const float a = v00 + wx * (v01 - v00), b = v10 + wx * (v11 - v10);
@@ -474,7 +509,7 @@ __device__ __forceinline__ bool table_node(const qpsdm_ttt_desc &d, const float 
 struct PointCells {
   bool ok;
   bool same;  // all four descriptors share one surface grid
-  int ixl, izlA, izlB;
+  int offA, offB;       // offsets of the point's two depth nodes inside a surface plane
   int cA, cB;          // cells of the two depth nodes
   int nxs, nys;        // shared surface grid (fast path)
   float c2, xc;
@@ -496,20 +531,23 @@ __device__ __forceinline__ void setup_cells(PointCells &pc, int ixi, float z,
   if (ixi < a.tcdp1 || ixi > a.tcdp2) return;
   const int lx = ixi - a.tcdp1;
   const int ixg = lx / a.nxi1;
-  pc.ixl = lx - ixg * a.nxi1;
+  const int ixl = lx - ixg * a.nxi1;
   const float fz = z / a.dzii;
   const int izn = (int)fz;
   pc.c2 = fz - (float)izn;
   int izgA = izn / a.nzi1, izgB = (izn + 1) / a.nzi1;
-  pc.izlA = izn - izgA * a.nzi1;
-  pc.izlB = izn + 1 - izgB * a.nzi1;
+  int izlA = izn - izgA * a.nzi1;
+  int izlB = izn + 1 - izgB * a.nzi1;
   if (izgB >= a.nzg) {  // deepest node: no lower neighbour
     izgB = izgA;
-    pc.izlB = pc.izlA;
+    izlB = izlA;
     pc.c2 = 0.0f;
   }
   if (ixg >= a.nxg || izgA >= a.nzg) return;
   pc.ok = true;
+  // [ixl][izl] planes (the reference layout) or [izl][ixl] (batched form)
+  pc.offA = a.xfast ? izlA * a.nxi1 + ixl : ixl * a.nzi1 + izlA;
+  pc.offB = a.xfast ? izlB * a.nxi1 + ixl : ixl * a.nzi1 + izlB;
   pc.cA = ixg * a.nzg + izgA;
   pc.cB = ixg * a.nzg + izgB;
   const qpsdm_ttt_desc tA = dt[pc.cA], tB = dt[pc.cB], qA = dq[pc.cA], qB = dq[pc.cB];
@@ -553,21 +591,21 @@ __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
     const float wx = nxs > 1 ? fx - ix : 0.0f, wy = nys > 1 ? fy - iy : 0.0f;
     const int64_t plane = (int64_t)nxi1 * nzi1;
     const int64_t sx = nxs > 1 ? plane : 0, sy = nys > 1 ? (int64_t)nxs * plane : 0;
-    const int64_t off = (int64_t)(iy * nxs + ix) * plane + (int64_t)pc.ixl * nzi1;
-    const float ta = bilin(ttt, pc.tA + off + pc.izlA, sx, sy, wx, wy);
-    const float tb = bilin(ttt, pc.tB + off + pc.izlB, sx, sy, wx, wy);
-    const float qa = bilin(qqq, pc.qA + off + pc.izlA, sx, sy, wx, wy);
-    const float qb = bilin(qqq, pc.qB + off + pc.izlB, sx, sy, wx, wy);
+    const int64_t off = (int64_t)(iy * nxs + ix) * plane;
+    const float ta = bilin(ttt, pc.tA + off + pc.offA, sx, sy, wx, wy);
+    const float tb = bilin(ttt, pc.tB + off + pc.offB, sx, sy, wx, wy);
+    const float qa = bilin(qqq, pc.qA + off + pc.offA, sx, sy, wx, wy);
+    const float qb = bilin(qqq, pc.qB + off + pc.offB, sx, sy, wx, wy);
     t = ta + pc.c2 * (tb - ta);
     q = qa + pc.c2 * (qb - qa);
     return true;
   }
   // cells with different surface grids: one lookup per descriptor
   float ta, tb, qa, qb;
-  if (!table_node(dt[pc.cA], ttt, px, py, pc.xc, pc.ixl, pc.izlA, nxi1, nzi1, ta)) return false;
-  if (!table_node(dt[pc.cB], ttt, px, py, pc.xc, pc.ixl, pc.izlB, nxi1, nzi1, tb)) return false;
-  if (!table_node(dq[pc.cA], qqq, px, py, pc.xc, pc.ixl, pc.izlA, nxi1, nzi1, qa)) return false;
-  if (!table_node(dq[pc.cB], qqq, px, py, pc.xc, pc.ixl, pc.izlB, nxi1, nzi1, qb)) return false;
+  if (!table_node(dt[pc.cA], ttt, px, py, pc.xc, pc.offA, nxi1, nzi1, ta)) return false;
+  if (!table_node(dt[pc.cB], ttt, px, py, pc.xc, pc.offB, nxi1, nzi1, tb)) return false;
+  if (!table_node(dq[pc.cA], qqq, px, py, pc.xc, pc.offA, nxi1, nzi1, qa)) return false;
+  if (!table_node(dq[pc.cB], qqq, px, py, pc.xc, pc.offB, nxi1, nzi1, qb)) return false;
   t = ta + pc.c2 * (tb - ta);
   q = qa + pc.c2 * (qb - qa);
   return true;
@@ -935,11 +973,13 @@ __global__ void __launch_bounds__(TZ *TX, MB)
             const float uy = fmaf(tany1c, azs, m[kMapPY * sc * NT].x) + agy;
             const float ruz = __fdividef(1.0f, uz);
             const float tanx = ux * ruz, tany = uy * ruz;
+            // dip taper (most passing pairs lie in a taper zone: approximate
+            // divisions, ~2 ulp)
             float w = 1.0f;
-            if (tanx < tanx1) w *= (tanx - tanx1c) / (tanx1 - tanx1c);
-            if (tanx > tanx2) w *= (tanx2c - tanx) / (tanx2c - tanx2);
-            if (tany < tany1) w *= (tany - tany1c) / (tany1 - tany1c);
-            if (tany > tany2) w *= (tany2c - tany) / (tany2c - tany2);
+            if (tanx < tanx1) w *= __fdividef(tanx - tanx1c, tanx1 - tanx1c);
+            if (tanx > tanx2) w *= __fdividef(tanx2c - tanx, tanx2c - tanx2);
+            if (tany < tany1) w *= __fdividef(tany - tany1c, tany1 - tany1c);
+            if (tany > tany2) w *= __fdividef(tany2c - tany, tany2c - tany2);
             const float t = ts + tg;
             const float ft = t * inv_dt1;
             const int it1 = (int)ft;
@@ -1058,6 +1098,7 @@ struct BatchedVariant {
 static const BatchedVariant kVariants[] = {
     {32, 8, 2, 8},  {32, 8, 3, 8},  {32, 4, 4, 8},  {32, 4, 6, 8},  {64, 4, 2, 8},
     {64, 4, 3, 8},  {128, 2, 2, 8}, {32, 4, 4, 16}, {32, 4, 3, 16}, {32, 8, 2, 16},
+    {8, 16, 4, 8},  {4, 32, 4, 8},  {16, 8, 4, 8},  {8, 16, 4, 16},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -1097,7 +1138,11 @@ static int launch_variant(int vi, PhysicsState *s, const PhysImageArgs &a, const
     case 6: return launch_batched_tile<128, 2, 2, T>(s, a, b, v, img, comp, npt, sc, st);
     case 7: return launch_batched_tile<32, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 8: return launch_batched_tile<32, 4, 3, T>(s, a, b, v, img, comp, npt, sc, st);
-    default: return launch_batched_tile<32, 8, 2, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 9: return launch_batched_tile<32, 8, 2, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 10: return launch_batched_tile<8, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 11: return launch_batched_tile<4, 32, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 12: return launch_batched_tile<16, 8, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    default: return launch_batched_tile<8, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
   }
 }
 
@@ -1266,6 +1311,7 @@ static PhysImageArgs image_args(const PhysicsState *s, const qpsdm_static_params
   a.nxi1 = l.nxi1;
   a.nzi1 = l.nzi1;
   a.nxz = nxz;
+  a.xfast = s->form == QPSDM_FORM_BATCHED;
   return a;
 }
 
