@@ -92,7 +92,8 @@ typedef struct {
   int form;        /* physics: QPSDM_FORM_PLAIN or QPSDM_FORM_BATCHED */
   int use_graph;   /* batched form: replay each batch as a captured CUDA graph */
   int tile_z, tile_x; /* batched image tile (0 = autotuned) */
-  int reserved[4];
+  int variant;     /* batched: launch variant + 1 of the autotuner's list (0 = tuned) */
+  int reserved[3];
 } qpsdm_static_params;
 
 /* Physics forms.  PLAIN: one pass per trace in submission order with table

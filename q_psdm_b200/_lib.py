@@ -42,7 +42,7 @@ class StaticParams(C.Structure):
         ("mode", C.c_int), ("panel_dtype", C.c_int), ("nbins", C.c_int),
         ("dtstar", C.c_float), ("max_batch", C.c_int), ("kahan", C.c_int),
         ("form", C.c_int), ("use_graph", C.c_int), ("tile_z", C.c_int), ("tile_x", C.c_int),
-        ("reserved", C.c_int * 4),
+        ("variant", C.c_int), ("reserved", C.c_int * 3),
     ]
 
 

@@ -74,7 +74,7 @@ struct PhysicsState {
   void *d_cub = nullptr;
   size_t cub_bytes = 0;
   int num_sms = 0;
-  int tile_z = 0, tile_x = 0;
+  int tile_z = 0, tile_x = 0, forced_variant = 0;
   int variant = -1;          // batched kernel variant (autotuned)
   float *d_tune = nullptr;   // scratch image of the autotuner
   size_t tune_cap = 0;
@@ -833,7 +833,7 @@ __global__ void k_batch_members(const uint8_t *__restrict__ rec, int rec_bytes, 
 // PX2 > AXg - tanx2c AZg (the receiver's thresholds, once per receiver).
 enum { kMapTQ = 0, kMapCZ, kMapPX, kMapPY, kMapN };
 
-template <int TZ, int TX, int MB, typename T>
+template <int TZ, int TX, int MB, int U, typename T>
 __global__ void __launch_bounds__(TZ *TX, MB)
     k_image_batched(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
                     const float *__restrict__ dips, const int4 *__restrict__ grp,
@@ -937,7 +937,6 @@ __global__ void __launch_bounds__(TZ *TX, MB)
         // time/t* pick and weight of the members that passed.  Then all panel
         // gathers, then the sums (in member order), so that U members' loads
         // are in flight together.
-        constexpr int U = 4;
         for (int p0 = gr.x; p0 < gr.y; p0 += U) {
           int4 mi[U];
 #pragma unroll
@@ -1072,6 +1071,7 @@ static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p) {
   cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
   if (p.tile_z > 0) s->tile_z = p.tile_z;
   if (p.tile_x > 0) s->tile_x = p.tile_x;
+  s->forced_variant = p.variant;
   return QPSDM_OK;
 }
 
@@ -1087,28 +1087,30 @@ struct LineView {
 };
 
 // Launch variants of the batched kernel: image tile (depth x cdps, one
-// thread per point, a warp along depth), the minimum resident blocks per SM
-// the register allocation is held to, and the sources per shared-memory
-// chunk (more sources per chunk: fewer passes over the receiver groups, more
-// shared memory per block).  The autotuner times them all on the first batch
-// and keeps the fastest.
+// thread per point; a warp spans min(TZ, 32) depths), the minimum resident
+// blocks per SM the register allocation is held to, the sources per
+// shared-memory chunk (more sources per chunk: fewer passes over the receiver
+// groups, more shared memory per block) and the members per block U.  The
+// autotuner times them all on the first batch and keeps the fastest.  (U = 8
+// was slower everywhere tried: the extra registers cost more occupancy than
+// the extra loads in flight gain.)
 struct BatchedVariant {
-  int tz, tx, mb, sc;
+  int tz, tx, mb, sc, u;
 };
 static const BatchedVariant kVariants[] = {
-    {32, 8, 2, 8},  {32, 8, 3, 8},  {32, 4, 4, 8},  {32, 4, 6, 8},  {64, 4, 2, 8},
-    {64, 4, 3, 8},  {128, 2, 2, 8}, {32, 4, 4, 16}, {32, 4, 3, 16}, {32, 8, 2, 16},
-    {8, 16, 4, 8},  {4, 32, 4, 8},  {16, 8, 4, 8},  {8, 16, 4, 16},
+    {32, 8, 2, 8, 4}, {32, 4, 4, 8, 4},  {32, 4, 6, 8, 4},  {64, 4, 3, 8, 4},
+    {32, 4, 3, 16, 4}, {8, 16, 4, 8, 4}, {4, 32, 4, 8, 4},  {16, 8, 4, 8, 4},
+    {8, 16, 4, 16, 4}, {16, 8, 3, 16, 4},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-template <int TZ, int TX, int MB, typename T>
+template <int TZ, int TX, int MB, int U, typename T>
 static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
                                const LineView &v, float *img, float *comp,
                                unsigned long long *npt, int sc, cudaStream_t st) {
   const int ntz = (a.nzi + TZ - 1) / TZ, ntx = (a.nxb + TX - 1) / TX;
   const size_t smem = sizeof(float2) * kMapN * (size_t)sc * TZ * TX;
-  auto kern = k_image_batched<TZ, TX, MB, T>;
+  auto kern = k_image_batched<TZ, TX, MB, U, T>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return QPSDM_ECUDA;
@@ -1129,20 +1131,16 @@ static int launch_variant(int vi, PhysicsState *s, const PhysImageArgs &a, const
                           cudaStream_t st) {
   const int sc = kVariants[vi].sc;
   switch (vi) {
-    case 0: return launch_batched_tile<32, 8, 2, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 1: return launch_batched_tile<32, 8, 3, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 2: return launch_batched_tile<32, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 3: return launch_batched_tile<32, 4, 6, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 4: return launch_batched_tile<64, 4, 2, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 5: return launch_batched_tile<64, 4, 3, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 6: return launch_batched_tile<128, 2, 2, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 7: return launch_batched_tile<32, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 8: return launch_batched_tile<32, 4, 3, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 9: return launch_batched_tile<32, 8, 2, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 10: return launch_batched_tile<8, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 11: return launch_batched_tile<4, 32, 4, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 12: return launch_batched_tile<16, 8, 4, T>(s, a, b, v, img, comp, npt, sc, st);
-    default: return launch_batched_tile<8, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 0: return launch_batched_tile<32, 8, 2, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 1: return launch_batched_tile<32, 4, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 2: return launch_batched_tile<32, 4, 6, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 3: return launch_batched_tile<64, 4, 3, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 4: return launch_batched_tile<32, 4, 3, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 5: return launch_batched_tile<8, 16, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 6: return launch_batched_tile<4, 32, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 7: return launch_batched_tile<16, 8, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 8: return launch_batched_tile<8, 16, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    default: return launch_batched_tile<16, 8, 3, 4, T>(s, a, b, v, img, comp, npt, sc, st);
   }
 }
 
@@ -1158,6 +1156,8 @@ template <typename T>
 static int choose_variant(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
                           const LineView &v, cudaStream_t st) {
   if (s->variant >= 0) return s->variant;
+  if (s->forced_variant > 0 && s->forced_variant <= kNumVariants)
+    return s->variant = s->forced_variant - 1;
   if (s->tile_z > 0 && s->tile_x > 0) {
     for (int i = 0; i < kNumVariants; ++i)
       if (kVariants[i].tz == s->tile_z && kVariants[i].tx == s->tile_x) return s->variant = i;

@@ -41,7 +41,7 @@ def static_params(*, nxi, nzi, ntl, dt, dxi, dyi, dzi, fci=1, scaled=1.0,
                   threshold=600.0, contract=3.0, taperzone=8.0, dzii=48.0,
                   mode=_lib.MODE_COMPAT, panel_dtype=_lib.PANEL_FP32, nbins=16,
                   dtstar=0.002, max_batch=4096, kahan=0, form=0, use_graph=0,
-                  tile_z=0, tile_x=0) -> StaticParams:
+                  tile_z=0, tile_x=0, variant=0) -> StaticParams:
     """Build line-independent parameters the way main()/qpsdm() do.
 
     The velocity-grid bounding box is padded by 2 km in x and 1 km in y
@@ -60,6 +60,7 @@ def static_params(*, nxi, nzi, ntl, dt, dxi, dyi, dzi, fci=1, scaled=1.0,
     p.mode, p.panel_dtype, p.nbins, p.dtstar = mode, panel_dtype, nbins, dtstar
     p.max_batch, p.kahan = max_batch, kahan
     p.form, p.use_graph, p.tile_z, p.tile_x = form, use_graph, tile_z, tile_x
+    p.variant = variant
     check(lib().qpsdm_static_params_init(C.byref(p)), what="static_params_init")
     return p
 

@@ -82,7 +82,7 @@ def oracle_run(case, nbins=NBINS, dtstar=DTSTAR):
 
 
 def engine(case, *, panel_dtype=0, kahan=0, nbins=NBINS, dtstar=DTSTAR, max_batch=4096,
-           device=0, form=0, tile=(0, 0), use_graph=0):
+           device=0, form=0, tile=(0, 0), use_graph=0, variant=0):
     from q_psdm_b200 import engine as E
     sv = case["sv"]
     p = E.static_params(nxi=sv.nxi, nzi=sv.nzi, ntl=NTL, dt=float(DT), dxi=sv.dxi, dyi=sv.dyi,
@@ -91,7 +91,8 @@ def engine(case, *, panel_dtype=0, kahan=0, nbins=NBINS, dtstar=DTSTAR, max_batc
                         threshold=THRESHOLD, contract=CONTRACT, taperzone=TAPERZONE,
                         dzii=case["tab"].dzii, mode=1, panel_dtype=panel_dtype,
                         nbins=nbins, dtstar=dtstar, max_batch=max_batch, kahan=kahan,
-                        form=form, tile_z=tile[0], tile_x=tile[1], use_graph=use_graph)
+                        form=form, tile_z=tile[0], tile_x=tile[1], use_graph=use_graph,
+                        variant=variant)
     eng = E.Engine(p, device=device)
     d = case["dips"].reshape(4, sv.nxi, sv.nzi)
     eng.set_line(fxi=case["fxi"], cyi=case["cyi"], dips=d, tables=case["tab"].as_engine_dict())
