@@ -57,8 +57,8 @@ F_PT = {"batched": 64, "plain": 64, "compat": 35}
 # DRAM bytes (read + write) per point-trace of the image kernel, from one ncu
 # capture each (profiles/): scaled to a launch by its point-traces.
 TRAFFIC_B_PER_PT = {
-    "batched": (340.8e6 + 4.5e6) / 1.943e9,   # 2 gathers x 1 line capture
-    "plain": (255.3e6 + 5.1e6) / 9.58e8,      # the plain form's own step
+    "batched": (347.6e6 + 7.4e6) / 1.943e9,   # 2 gathers x 1 line capture
+    "plain": (229.7e6 + 4.9e6) / 9.58e8,      # the plain form's own step
     "compat": 4.55e6 / 9.83e8,                # the compat form's own step
 }
 FORMS = {  # shots per step, lines per step, panel dtype, physics form
