@@ -321,6 +321,11 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
            "launches": int(sum(v[1] for v in kt.values())),
            "image_ms_per_launch": kt["image"][0] / max(kt["image"][1], 1),
            "image_launches": kt["image"][1], "npt": npt}
+    if form == "batched":
+        tu = eng.tuning()
+        out["tuning"] = {"variant": tu["variant"], "tile_depths_cdps": tu["tile"],
+                         "min_blocks_per_sm": tu["min_blocks"],
+                         "variant_ms": [round(x, 3) for x in tu["variant_ms"]]}
 
     if e2e:
         eng.set_stream(None)
@@ -405,6 +410,8 @@ def run_ours(args, rank, world, dist):
            "e2e": head.get("e2e"), "gpu_launches": head["launches"], "clocks": head["clocks"],
            "point_traces_per_step": head["point_traces_per_step"],
            "kernel_ms_per_step": head["kernel_ms_per_step"], "forms": forms}
+    if "tuning" in head:
+        res["config"]["autotuned"] = head["tuning"]
     return res, wl
 
 

@@ -350,63 +350,67 @@ __device__ __forceinline__ float phys_tapered(float v, int j, int n, const float
   return v;
 }
 
-// Forward spectrum of one trace.  For FP16 panels also the trace's sample
-// multiplier: every panel sample of the trace is bounded by
-// B = 2 sum_k |X_k| max_b |F_b,k| (triangle inequality over the c2r sum), and
-// the panels store x / 2^e with e chosen so that B / 2^e lies in [2^13, 2^14):
-// no overflow of FP16 (max 65504) and no loss to its subnormal range; the
-// image kernels multiply the samples by 2^e again (exact).
+// Forward spectra of the accepted traces; a persistent CTA loads the
+// twiddles into shared memory once and then takes every gridDim.x-th trace.
+// For FP16 panels also the trace's sample multiplier: every panel sample of
+// the trace is bounded by B = 2 sum_k |X_k| max_b |F_b,k| (triangle
+// inequality over the c2r sum), and the panels store x / 2^e with e chosen so
+// that B / 2^e lies in [2^13, 2^14): no overflow of FP16 (max 65504) and no
+// loss to its subnormal range; the image kernels multiply the samples by 2^e
+// again (exact).
 __global__ void __launch_bounds__(256) k_phys_fwd(const uint8_t *__restrict__ rec, int rec_bytes,
                                                   int be, const int *__restrict__ status,
-                                                  int sstride, int ntl,
+                                                  int sstride, int ntr, int ntl,
                                                   float dt, const float *__restrict__ tap,
                                                   FftPlan p, float2 *__restrict__ spec,
                                                   const float *__restrict__ fmax,
                                                   float *__restrict__ pscale) {
-  const int itr = blockIdx.x;
-  if (status[(size_t)itr * sstride] != kAccepted) return;
   extern __shared__ float2 sm[];
   float2 *b0 = sm, *b1 = sm + p.m, *twm = sm + 2 * p.m, *twn = sm + 3 * p.m;
+  __shared__ float s_part[8];
   for (int i = threadIdx.x; i < p.m; i += blockDim.x) twm[i] = p.tw_m[i];
   for (int i = threadIdx.x; i <= p.m; i += blockDim.x) twn[i] = p.tw_n[i];
-  const uint8_t *r = rec + (size_t)itr * rec_bytes;
-  float *bf = reinterpret_cast<float *>(b0);
-  for (int j = threadIdx.x; j < p.n; j += blockDim.x) {
-    float v = 0.0f;
-    if (j < ntl) {
-      v = su_sample(r, j, be);
-      const float t = __fmul_rn((float)j, dt);
-      v = ((double)t < 0.1) ? __double2float_rn(__dmul_rn((double)v, 0.1 * 0.1))
-                            : __fmul_rn(v, __fmul_rn(t, t));
-      v = phys_tapered(v, j, ntl, tap);
+  for (int itr = blockIdx.x; itr < ntr; itr += gridDim.x) {
+    if (status[(size_t)itr * sstride] != kAccepted) continue;  // uniform in the CTA
+    const uint8_t *r = rec + (size_t)itr * rec_bytes;
+    float *bf = reinterpret_cast<float *>(b0);
+    for (int j = threadIdx.x; j < p.n; j += blockDim.x) {
+      float v = 0.0f;
+      if (j < ntl) {
+        v = su_sample(r, j, be);
+        const float t = __fmul_rn((float)j, dt);
+        v = ((double)t < 0.1) ? __double2float_rn(__dmul_rn((double)v, 0.1 * 0.1))
+                              : __fmul_rn(v, __fmul_rn(t, t));
+        v = phys_tapered(v, j, ntl, tap);
+      }
+      bf[j] = v;
     }
-    bf[j] = v;
-  }
-  __syncthreads();
-  const int cur = fft_complex_smem(b0, b1, p, twm, false);
-  const float2 *Z = cur ? b1 : b0;
-  float2 *o = spec + (size_t)itr * (p.m + 1);
-  float bound = 0.0f;
-  for (int k = threadIdx.x; k <= p.m; k += blockDim.x) {
-    const float2 v = rfft_bin(Z, twn, p.m, k);
-    o[k] = v;
-    if (pscale) bound = fmaf(sqrtf(v.x * v.x + v.y * v.y), fmax[k], bound);
-  }
-  if (!pscale) return;
-  __shared__ float s_part[8];
-  for (int off = 16; off > 0; off >>= 1) bound += __shfl_xor_sync(0xffffffffu, bound, off);
-  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = bound;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float b = 0.0f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += s_part[w];
-    b *= 2.0f;
-    int e = 0;
-    if (b > 0.0f && isfinite(b)) {
-      frexpf(b, &e);  // b = m 2^e, m in [0.5, 1)
-      e = min(max(e - 14, -126), 127);
+    __syncthreads();
+    const int cur = fft_complex_smem(b0, b1, p, twm, false);
+    const float2 *Z = cur ? b1 : b0;
+    float2 *o = spec + (size_t)itr * (p.m + 1);
+    float bound = 0.0f;
+    for (int k = threadIdx.x; k <= p.m; k += blockDim.x) {
+      const float2 v = rfft_bin(Z, twn, p.m, k);
+      o[k] = v;
+      if (pscale) bound = fmaf(sqrtf(v.x * v.x + v.y * v.y), fmax[k], bound);
     }
-    pscale[itr] = ldexpf(1.0f, e);
+    if (pscale) {
+      for (int off = 16; off > 0; off >>= 1) bound += __shfl_xor_sync(0xffffffffu, bound, off);
+      if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = bound;
+    }
+    __syncthreads();  // Z and s_part complete; b0 / b1 free for the next trace
+    if (pscale && threadIdx.x == 0) {
+      float b = 0.0f;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += s_part[w];
+      b *= 2.0f;
+      int e = 0;
+      if (b > 0.0f && isfinite(b)) {
+        frexpf(b, &e);  // b = m 2^e, m in [0.5, 1)
+        e = min(max(e - 14, -126), 127);
+      }
+      pscale[itr] = ldexpf(1.0f, e);
+    }
   }
 }
 
@@ -421,42 +425,100 @@ __device__ __forceinline__ void store_sample<__nv_bfloat16>(__nv_bfloat16 *d, fl
 template <>
 __device__ __forceinline__ void store_sample<__half>(__half *d, float v) { *d = __float2half_rn(v); }
 
-// One CTA per (trace, t* bin): filtered, zero-padded spectrum -> c2r nffti.
+// Four output samples (two complex points) of a panel row.
 template <typename T>
-__global__ void __launch_bounds__(256) k_phys_panels(const int *__restrict__ status, int sstride,
-                                                     const float2 *__restrict__ spec, int nk,
-                                                     const float2 *__restrict__ filt, FftPlan p,
-                                                     int nbins, T *__restrict__ panels,
+__device__ __forceinline__ void store_quad(T *dst, float mul, float2 z0, float2 z1);
+template <>
+__device__ __forceinline__ void store_quad<float>(float *d, float mul, float2 z0, float2 z1) {
+  *reinterpret_cast<float4 *>(d) = make_float4(mul * z0.x, mul * z0.y, mul * z1.x, mul * z1.y);
+}
+template <>
+__device__ __forceinline__ void store_quad<__half>(__half *d, float mul, float2 z0, float2 z1) {
+  const __half2 a = __halves2half2(__float2half_rn(mul * z0.x), __float2half_rn(mul * z0.y));
+  const __half2 c = __halves2half2(__float2half_rn(mul * z1.x), __float2half_rn(mul * z1.y));
+  uint2 u;
+  u.x = *reinterpret_cast<const unsigned *>(&a);
+  u.y = *reinterpret_cast<const unsigned *>(&c);
+  *reinterpret_cast<uint2 *>(d) = u;
+}
+template <>
+__device__ __forceinline__ void store_quad<__nv_bfloat16>(__nv_bfloat16 *d, float mul, float2 z0,
+                                                         float2 z1) {
+  const __nv_bfloat162 a =
+      __halves2bfloat162(__float2bfloat16_rn(mul * z0.x), __float2bfloat16_rn(mul * z0.y));
+  const __nv_bfloat162 c =
+      __halves2bfloat162(__float2bfloat16_rn(mul * z1.x), __float2bfloat16_rn(mul * z1.y));
+  uint2 u;
+  u.x = *reinterpret_cast<const unsigned *>(&a);
+  u.y = *reinterpret_cast<const unsigned *>(&c);
+  *reinterpret_cast<uint2 *>(d) = u;
+}
+
+// Z[k] of the c2r split from a = Y[k], c = Y[m-k] (irfft_pre with the two
+// spectrum values already at hand).
+__device__ __forceinline__ float2 irfft_split(float2 a, float2 c, float2 tw) {
+  const float2 bb = cconj(c);
+  const float2 e = make_float2(0.5f * (a.x + bb.x), 0.5f * (a.y + bb.y));
+  const float2 d = make_float2(0.5f * (a.x - bb.x), 0.5f * (a.y - bb.y));
+  const float2 o = cmul(d, cconj(tw));
+  return make_float2(e.x - o.y, e.y + o.x);
+}
+
+// t*-binned panels: for every accepted trace and bin b, the filtered,
+// zero-padded spectrum X F_b -> c2r of length nffti.  A persistent CTA loads
+// the twiddles into shared memory once, then takes every gridDim.x-th trace,
+// keeps its spectrum in shared memory and runs all bins of it back to back.
+// Shared memory: two FFT buffers, the m + (m+1) twiddles, the nk-point
+// spectrum.  Each bin's input goes to the buffer the previous bin's result
+// is not in, so one barrier per bin covers the previous bin's stores.
+// Rows are stored two complex points (16 / 8 bytes) at a time when m is even.
+template <typename T>
+__global__ void __launch_bounds__(256, 3) k_phys_panels(const int *__restrict__ status, int sstride,
+                                                     int ntr, const float2 *__restrict__ spec,
+                                                     int nk, const float2 *__restrict__ filt,
+                                                     FftPlan p, int nbins, T *__restrict__ panels,
                                                      const float *__restrict__ pscale) {
-  const int itr = blockIdx.x, b = blockIdx.y;
-  if (status[(size_t)itr * sstride] != kAccepted) return;
   extern __shared__ float2 sm[];
-  float2 *b0 = sm, *b1 = sm + p.m, *twm = sm + 2 * p.m, *twn = sm + 3 * p.m;
+  float2 *twm = sm + 2 * p.m, *twn = sm + 3 * p.m, *Xs = sm + 4 * p.m + 1;
   for (int i = threadIdx.x; i < p.m; i += blockDim.x) twm[i] = p.tw_m[i];
   for (int i = threadIdx.x; i <= p.m; i += blockDim.x) twn[i] = p.tw_n[i];
-  __syncthreads();
-  const float2 *X = spec + (size_t)itr * nk;
-  const float2 *F = filt + (size_t)b * nk;
-  for (int k = threadIdx.x; k < p.m; k += blockDim.x) {
-    // Y[k] and Y[m-k] of the zero-padded filtered spectrum
-    const int k2 = p.m - k;
-    const float2 a = k < nk ? cmul(X[k], F[k]) : make_float2(0.f, 0.f);
-    const float2 c = k2 < nk ? cmul(X[k2], F[k2]) : make_float2(0.f, 0.f);
-    const float2 bb = cconj(c);
-    const float2 e = make_float2(0.5f * (a.x + bb.x), 0.5f * (a.y + bb.y));
-    const float2 d = make_float2(0.5f * (a.x - bb.x), 0.5f * (a.y - bb.y));
-    const float2 o = cmul(d, cconj(twn[k]));
-    b0[k] = make_float2(e.x - o.y, e.y + o.x);
-  }
-  __syncthreads();
-  const int cur = fft_complex_smem(b0, b1, p, twm, true);
-  const float2 *z = cur ? b1 : b0;
-  T *out = panels + ((size_t)itr * nbins + b) * p.n;
-  // 2 / 2^e for FP16 (exact), 2 otherwise
-  const float mul = std::is_same<T, __half>::value ? 2.0f / pscale[itr] : 2.0f;
-  for (int j = threadIdx.x; j < p.m; j += blockDim.x) {
-    store_sample<T>(out + 2 * j, mul * z[j].x);
-    store_sample<T>(out + 2 * j + 1, mul * z[j].y);
+  int in = 0;  // buffer the next bin's input goes to
+  for (int itr = blockIdx.x; itr < ntr; itr += gridDim.x) {
+    if (status[(size_t)itr * sstride] != kAccepted) continue;  // uniform in the CTA
+    const float2 *X = spec + (size_t)itr * nk;
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) Xs[k] = X[k];
+    __syncthreads();
+    // 2 / 2^e for FP16 (exact), 2 otherwise
+    const float mul = std::is_same<T, __half>::value ? 2.0f / pscale[itr] : 2.0f;
+    for (int b = 0; b < nbins; ++b) {
+      const float2 *F = filt + (size_t)b * nk;
+      float2 *b0 = sm + in * p.m, *b1 = sm + (in ^ 1) * p.m;
+      for (int k = threadIdx.x; 2 * k <= p.m; k += blockDim.x) {
+        // Y[k] and Y[m-k] of the zero-padded filtered spectrum give both
+        // Z[k] and Z[m-k] of the c2r split
+        const int k2 = p.m - k;
+        const float2 a = k < nk ? cmul(Xs[k], __ldg(F + k)) : make_float2(0.f, 0.f);
+        const float2 c = k2 < nk ? cmul(Xs[k2], __ldg(F + k2)) : make_float2(0.f, 0.f);
+        b0[k] = irfft_split(a, c, twn[k]);
+        if (k > 0 && k < k2) b0[k2] = irfft_split(c, a, twn[k2]);
+      }
+      __syncthreads();
+      const int cur = fft_complex_smem(b0, b1, p, twm, true);
+      const float2 *z = cur ? b1 : b0;
+      T *out = panels + ((size_t)itr * nbins + b) * p.n;
+      if ((p.m & 1) == 0) {  // rows of 4m bytes (FP16) / 8m bytes: 8- / 16-byte aligned
+        for (int j = threadIdx.x; 2 * j < p.m; j += blockDim.x)
+          store_quad<T>(out + 4 * j, mul, z[2 * j], z[2 * j + 1]);
+      } else {
+        for (int j = threadIdx.x; j < p.m; j += blockDim.x) {
+          store_sample<T>(out + 2 * j, mul * z[j].x);
+          store_sample<T>(out + 2 * j + 1, mul * z[j].y);
+        }
+      }
+      in = cur ? in : in ^ 1;
+    }
+    // the last bin's stores read the buffer other than `in`; the next trace
+    // writes Xs (read by this trace's bins, all past a barrier), then `in`
   }
 }
 
@@ -1100,9 +1162,11 @@ struct BatchedVariant {
 static const BatchedVariant kVariants[] = {
     {32, 8, 2, 8, 4}, {32, 4, 4, 8, 4},  {32, 4, 6, 8, 4},  {64, 4, 3, 8, 4},
     {32, 4, 3, 16, 4}, {8, 16, 4, 8, 4}, {4, 32, 4, 8, 4},  {16, 8, 4, 8, 4},
-    {8, 16, 4, 16, 4}, {16, 8, 3, 16, 4},
+    {8, 16, 4, 16, 4}, {16, 8, 3, 16, 4}, {8, 16, 5, 8, 4},  {8, 16, 5, 16, 4},
+    {16, 8, 5, 8, 4},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+static_assert(kNumVariants <= 16, "tune_ms holds 16 timings");
 
 template <int TZ, int TX, int MB, int U, typename T>
 static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
@@ -1140,7 +1204,10 @@ static int launch_variant(int vi, PhysicsState *s, const PhysImageArgs &a, const
     case 6: return launch_batched_tile<4, 32, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 7: return launch_batched_tile<16, 8, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 8: return launch_batched_tile<8, 16, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
-    default: return launch_batched_tile<16, 8, 3, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 9: return launch_batched_tile<16, 8, 3, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 10:
+    case 11: return launch_batched_tile<8, 16, 5, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    default: return launch_batched_tile<16, 8, 5, 4, T>(s, a, b, v, img, comp, npt, sc, st);
   }
 }
 
@@ -1259,32 +1326,47 @@ static int run_panels(PhysicsState *s, const qpsdm_static_params &p, const Physi
   rc = fft_plan(p.nffti, &pi, err);
   if (rc) return rc;
   const int ntr = b.ntr;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  // persistent grids: as many CTAs as fit on the GPU, at most one per trace
+  auto grid_of = [&](const void *kern, size_t smem) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem);
+    return std::max(1, std::min(ntr, std::max(per_sm, 1) * std::max(nsm, 1)));
+  };
   size_t sm = fft_smem_bytes(pf.m);
   if ((rc = fft_set_smem_attr((const void *)k_phys_fwd, sm))) return rc;
   const bool fp16 = s->dtype == QPSDM_PANEL_FP16;
-  k_phys_fwd<<<ntr, 256, sm, st>>>(b.d_rec, b.rec_bytes, b.big_endian, status, sstride, p.ntl,
-                                   p.dt, b.d_taper200, pf, s->d_spec, s->d_fmax,
-                                   fp16 ? s->d_pscale : nullptr);
+  k_phys_fwd<<<grid_of((const void *)k_phys_fwd, sm), 256, sm, st>>>(
+      b.d_rec, b.rec_bytes, b.big_endian, status, sstride, ntr, p.ntl, p.dt, b.d_taper200, pf,
+      s->d_spec, s->d_fmax, fp16 ? s->d_pscale : nullptr);
   const int nk = p.nfft / 2 + 1;
-  sm = fft_smem_bytes(pi.m);
-  dim3 gp(ntr, s->nbins);
+  sm = fft_smem_bytes(pi.m) + sizeof(float2) * (size_t)nk;
   switch (s->dtype) {
-    case QPSDM_PANEL_FP32:
-      if ((rc = fft_set_smem_attr((const void *)k_phys_panels<float>, sm))) return rc;
-      k_phys_panels<float><<<gp, 256, sm, st>>>(status, sstride, s->d_spec, nk, s->d_filter, pi,
-                                                s->nbins, (float *)s->d_panels, nullptr);
+    case QPSDM_PANEL_FP32: {
+      const void *k = (const void *)k_phys_panels<float>;
+      if ((rc = fft_set_smem_attr(k, sm))) return rc;
+      k_phys_panels<float><<<grid_of(k, sm), 256, sm, st>>>(
+          status, sstride, ntr, s->d_spec, nk, s->d_filter, pi, s->nbins,
+          (float *)s->d_panels, nullptr);
       break;
-    case QPSDM_PANEL_BF16:
-      if ((rc = fft_set_smem_attr((const void *)k_phys_panels<__nv_bfloat16>, sm))) return rc;
-      k_phys_panels<__nv_bfloat16><<<gp, 256, sm, st>>>(status, sstride, s->d_spec, nk,
-                                                        s->d_filter, pi, s->nbins,
-                                                        (__nv_bfloat16 *)s->d_panels, nullptr);
+    }
+    case QPSDM_PANEL_BF16: {
+      const void *k = (const void *)k_phys_panels<__nv_bfloat16>;
+      if ((rc = fft_set_smem_attr(k, sm))) return rc;
+      k_phys_panels<__nv_bfloat16><<<grid_of(k, sm), 256, sm, st>>>(
+          status, sstride, ntr, s->d_spec, nk, s->d_filter, pi, s->nbins,
+          (__nv_bfloat16 *)s->d_panels, nullptr);
       break;
-    default:
-      if ((rc = fft_set_smem_attr((const void *)k_phys_panels<__half>, sm))) return rc;
-      k_phys_panels<__half><<<gp, 256, sm, st>>>(status, sstride, s->d_spec, nk, s->d_filter,
-                                                 pi, s->nbins, (__half *)s->d_panels,
-                                                 s->d_pscale);
+    }
+    default: {
+      const void *k = (const void *)k_phys_panels<__half>;
+      if ((rc = fft_set_smem_attr(k, sm))) return rc;
+      k_phys_panels<__half><<<grid_of(k, sm), 256, sm, st>>>(
+          status, sstride, ntr, s->d_spec, nk, s->d_filter, pi, s->nbins,
+          (__half *)s->d_panels, s->d_pscale);
+    }
   }
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }

@@ -182,7 +182,7 @@ def test_fp16_panels_any_amplitude(cuda, case, form, gain):
     assert nrmse(img, case["o_img"]) <= 2.5e-4
 
 
-@pytest.mark.parametrize("variant", list(range(1, 11)))
+@pytest.mark.parametrize("variant", list(range(1, 14)))
 def test_every_batched_variant(cuda, case, variant):
     """Each launch variant the autotuner may pick (tile, blocks per SM, source
     chunk) images the same as the FP64 oracle."""
