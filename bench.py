@@ -91,6 +91,9 @@ def parse():
                     help="image lines per step of the chosen form (default: the form's own)")
     ap.add_argument("--tile", default="",
                     help="batched kernel tile 'Z,X' instead of autotuning (for profiling)")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="batched kernel variant (1-based, the engine's autotuner list) "
+                         "instead of autotuning (for profiling)")
     return ap.parse_args()
 
 
@@ -103,10 +106,11 @@ class Workload:
     LINE0 = 252                      # first image line of the brick
     HALF_CDPS, HALF_LINES = 200, 100  # aperture: +-2 km in x, +-1 km in y
 
-    def __init__(self, rank: int = 0, tile=(0, 0)):
+    def __init__(self, rank: int = 0, tile=(0, 0), variant: int = 0):
         from q_psdm_b200 import synth
         self.synth = synth
         self.tile = tile
+        self.variant = variant
         self.sv = synth.config2(seed=11)
         self.rank = rank
         ly = self.sv.line_y(self.LINE0 + 4)
@@ -152,7 +156,8 @@ class Workload:
         if pform is None:
             return E.static_params(**kw)
         return E.static_params(**kw, mode=1, panel_dtype=dtype, nbins=16, dtstar=0.002,
-                               form=pform, dzii=self.tables().dzii, tile_z=tz, tile_x=tx)
+                               form=pform, dzii=self.tables().dzii, tile_z=tz, tile_x=tx,
+                               variant=self.variant if form == "batched" else 0)
 
     def lines(self, form: str, contract_rad: float):
         sv = self.sv
@@ -368,7 +373,7 @@ def run_ours(args, rank, world, dist):
         ns, nl, dt, pf = FORMS[args.form]
         FORMS[args.form] = (args.shots or ns, args.lines or nl, dt, pf)
     tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else (0, 0)
-    wl = Workload(rank, tile)
+    wl = Workload(rank, tile, args.variant)
     head = run_form(args.form, wl, args, dev, dist, steps=args.steps, warmup=args.warmup,
                     e2e=not args.no_e2e)
     forms = {args.form: {k: head[k] for k in ("value", "ms_per_step", "point_traces_per_step",

@@ -70,6 +70,7 @@ struct PhysicsState {
   int4 *d_mem = nullptr;                       // [max_batch] member info
   int4 *d_grp = nullptr;                       // [max_batch] group records
   float2 *d_grppos = nullptr;                  // [max_batch] receiver positions
+  int *d_memgrp = nullptr;                     // [max_batch] group of each sorted member
   int *d_tile_ctr = nullptr;
   void *d_cub = nullptr;
   size_t cub_bytes = 0;
@@ -196,6 +197,7 @@ void physics_destroy(PhysicsState *s) {
   cudaFree(s->d_mem);
   cudaFree(s->d_grp);
   cudaFree(s->d_grppos);
+  cudaFree(s->d_memgrp);
   cudaFree(s->d_tile_ctr);
   cudaFree(s->d_cub);
   cudaFree(s->d_filter);
@@ -829,16 +831,19 @@ __global__ void k_batch_keys(const uint8_t *__restrict__ rec, int rec_bytes, int
 }
 
 // Group records: [2g] = (first sorted position, end, min ixi1, max ixi2),
-// [2g+1] = (min source, max source); receiver position per group.
+// [2g+1] = (min source, max source); receiver position per group; the group
+// of every sorted position.
 __global__ void k_batch_groups(const unsigned long long *__restrict__ ukey,
                                const int *__restrict__ count, const int *__restrict__ off,
                                const int *__restrict__ nruns, const int *__restrict__ sval,
                                const int *__restrict__ ints, const int *__restrict__ sid,
-                               int4 *__restrict__ grp, float2 *__restrict__ grppos, int ntr) {
+                               int4 *__restrict__ grp, float2 *__restrict__ grppos,
+                               int *__restrict__ memgrp, int ntr) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ntr || g >= *nruns) return;
   const unsigned long long k = ukey[g];
   const int start = off[g], n = count[g];
+  for (int p = start; p < start + n; ++p) memgrp[p] = g;
   if (k == kNoKey) {
     grp[2 * g] = make_int4(start, start, 1, 0);
     grp[2 * g + 1] = make_int4(1, 0, 0, 0);
@@ -895,24 +900,97 @@ __global__ void k_batch_members(const uint8_t *__restrict__ rec, int rec_bytes, 
 // PX2 > AXg - tanx2c AZg (the receiver's thresholds, once per receiver).
 enum { kMapTQ = 0, kMapCZ, kMapPX, kMapPY, kMapN };
 
+// Tile-level dip test.  A member (source S, receiver G) contributes to an
+// image point P only if the bisector u = A_S + A_G of the unit vectors from
+// P passes the four division-free dip tests
+//   fx1 = ux - tanx1c uz > 0,  fx2 = tanx2c uz - ux > 0   (y likewise),
+// so it can be dropped for a whole image tile when an upper bound of one of
+// them over the tile is negative.  The bounds come from interval arithmetic
+// over the tile's box (x in [x0, x1], y = 0 on the line, z in [z0, z1]) and
+// the tile's ranges of the four dip limits; the margin 1e-4 covers the FP32
+// rounding of the per-point test, so no member that passes at some point of
+// the tile is dropped (the kernel's sums are unchanged).
+struct TileBox {
+  float x0, x1, z0, z1;
+  float t1lo, t1hi, t2lo, t2hi, u1lo, u1hi, u2lo, u2hi;  // tanx1c, tanx2c, tany1c, tany2c
+};
+struct UnitBounds {
+  float axl, axh, ayl, ayh, azl, azh;
+  bool ok;
+};
+__device__ __forceinline__ UnitBounds unit_bounds(float px, float py, const TileBox &b) {
+  UnitBounds u;
+  const float dxl = px - b.x1, dxh = px - b.x0;
+  const float adxmin = (dxl <= 0.0f && dxh >= 0.0f) ? 0.0f : fminf(fabsf(dxl), fabsf(dxh));
+  const float adxmax = fmaxf(fabsf(dxl), fabsf(dxh));
+  const float rmin = sqrtf(adxmin * adxmin + py * py + b.z0 * b.z0);
+  const float rmax = sqrtf(adxmax * adxmax + py * py + b.z1 * b.z1);
+  u.ok = rmin > 1e-3f;  // a point of the box (nearly) at the surface position: no bound
+  const float irmin = 1.0f / fmaxf(rmin, 1e-3f), irmax = 1.0f / rmax;
+  u.axl = dxl >= 0.0f ? dxl * irmax : dxl * irmin;
+  u.axh = dxh >= 0.0f ? dxh * irmin : dxh * irmax;
+  u.ayl = py >= 0.0f ? py * irmax : py * irmin;
+  u.ayh = py >= 0.0f ? py * irmin : py * irmax;
+  u.azl = b.z0 * irmax;
+  u.azh = b.z1 * irmin;
+  return u;
+}
+// max of t * v over t in [tlo, thi], v in [vlo, vhi] (a corner of the box)
+__device__ __forceinline__ float corner_max(float tlo, float thi, float vlo, float vhi) {
+  return fmaxf(fmaxf(tlo * vlo, tlo * vhi), fmaxf(thi * vlo, thi * vhi));
+}
+__device__ __forceinline__ bool tile_keep(float2 sp, float2 gp, const TileBox &b) {
+  const UnitBounds s = unit_bounds(sp.x, sp.y, b), g = unit_bounds(gp.x, gp.y, b);
+  if (!s.ok || !g.ok) return true;
+  const float uxl = s.axl + g.axl, uxh = s.axh + g.axh;
+  const float uyl = s.ayl + g.ayl, uyh = s.ayh + g.ayh;
+  const float uzl = s.azl + g.azl, uzh = s.azh + g.azh;
+  const float fx1 = uxh + corner_max(-b.t1hi, -b.t1lo, uzl, uzh);
+  const float fx2 = corner_max(b.t2lo, b.t2hi, uzl, uzh) - uxl;
+  const float fy1 = uyh + corner_max(-b.u1hi, -b.u1lo, uzl, uzh);
+  const float fy2 = corner_max(b.u2lo, b.u2hi, uzl, uzh) - uyl;
+  constexpr float m = -1e-4f;
+  return !(fx1 < m || fx2 < m || fy1 < m || fy2 < m);  // NaN keeps the member
+}
+
+template <int NW>
+__device__ __forceinline__ float block_min(float v, float (*red)[NW], int k) {
+  for (int off = 16; off > 0; off >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, off));
+  if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+  return v;
+}
+
+// Batched imaging.  A persistent CTA takes image tiles of TZ depths x TX
+// cdps (one thread per point) from a counter.  Per tile and per chunk of sc
+// sources: the source terms of every point in shared memory; then the
+// members (traces in receiver order) in chunks of 32 x NT: the CTA keeps the
+// members that pass the tile-level dip test (a bit mask), and every point
+// runs over the kept members in order -- receiver terms once per receiver
+// group, the members in blocks of U (the per-point aperture and dip tests,
+// then the time/t* pick, weight and panel gathers).  Members dropped for the
+// tile fail every point's dip test, so the image is that of running every
+// member; their in-aperture point count still goes to npt.
 template <int TZ, int TX, int MB, int U, typename T>
 __global__ void __launch_bounds__(TZ *TX, MB)
     k_image_batched(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
-                    const float *__restrict__ dips, const int4 *__restrict__ grp,
-                    const float2 *__restrict__ grppos, const int *__restrict__ nruns,
-                    const int4 *__restrict__ mem, const float2 *__restrict__ srcpos,
-                    const int *__restrict__ nsrc_ptr, const qpsdm_ttt_desc *__restrict__ dt,
-                    const float *__restrict__ ttt, const qpsdm_ttt_desc *__restrict__ dq,
-                    const float *__restrict__ qqq, const T *__restrict__ panels,
-                    int *__restrict__ tile_ctr, int ntz, int ntx, int sc,
-                    unsigned long long *npt) {
-  constexpr int NT = TZ * TX;
+                    const float *__restrict__ dips, const int *__restrict__ memgrp,
+                    const float2 *__restrict__ grppos, const int4 *__restrict__ mem, int nmem,
+                    const float2 *__restrict__ srcpos, const int *__restrict__ nsrc_ptr,
+                    const qpsdm_ttt_desc *__restrict__ dt, const float *__restrict__ ttt,
+                    const qpsdm_ttt_desc *__restrict__ dq, const float *__restrict__ qqq,
+                    const T *__restrict__ panels, int *__restrict__ tile_ctr, int ntz, int ntx,
+                    int sc, unsigned long long *npt) {
+  constexpr int NT = TZ * TX, NW = NT / 32, MC = 32 * NT;
+  static_assert(NT % 32 == 0, "whole warps");
   extern __shared__ float2 smap[];  // [kMapN][sc][NT]
+  __shared__ unsigned s_mask[NT];   // kept members of the chunk, one bit each
+  __shared__ int s_col[TX + 1];     // active points of the tile's columns (prefix sums)
+  __shared__ float s_red[8][NW];
   __shared__ int s_tile;
   __shared__ unsigned long long s_cnt;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int lz = tid % TZ, lx = tid / TZ;
-  const int ngroups = *nruns, nsrc = *nsrc_ptr;
+  const int nsrc = *nsrc_ptr;
   const float inv_dt1 = 1.0f / a.dt1, inv_dts = 1.0f / a.dtstar;
   const size_t pstride = (size_t)a.nbins * a.nt;
   if (tid == 0) s_cnt = 0;
@@ -920,11 +998,13 @@ __global__ void __launch_bounds__(TZ *TX, MB)
   for (;;) {
     __syncthreads();
     if (tid == 0) s_tile = atomicAdd(tile_ctr, 1);
+    if (tid <= TX) s_col[tid] = 0;
     __syncthreads();
     const int tile = s_tile;
     if (tile >= ntz * ntx) break;
-    const int izi = (tile % ntz) * TZ + lz;
-    const int ixb = (tile / ntz) * TX + lx;
+    const int iz0 = (tile % ntz) * TZ, ixb0 = (tile / ntz) * TX;
+    const int izi = iz0 + lz;
+    const int ixb = ixb0 + lx;
     const bool live = izi < a.nzi && ixb < a.nxb;
     const int ixi = ixb + a.ixstart;
     PointCells pc;
@@ -949,11 +1029,47 @@ __global__ void __launch_bounds__(TZ *TX, MB)
     const float tany2c = tany2 + tz * (1.0f + tany2 * tany2);
     const float z2 = z * z;
     const float x = ixi * a.dxi;
+    // the tile's box and dip-limit ranges over its active points
+    {
+      const float big = 3.0e38f;
+      block_min<NW>(act ? tanx1c : big, s_red, 0);
+      block_min<NW>(act ? -tanx1c : big, s_red, 1);
+      block_min<NW>(act ? tanx2c : big, s_red, 2);
+      block_min<NW>(act ? -tanx2c : big, s_red, 3);
+      block_min<NW>(act ? tany1c : big, s_red, 4);
+      block_min<NW>(act ? -tany1c : big, s_red, 5);
+      block_min<NW>(act ? tany2c : big, s_red, 6);
+      block_min<NW>(act ? -tany2c : big, s_red, 7);
+      if (act) atomicAdd(&s_col[lx + 1], 1);
+    }
+    __syncthreads();
+    if (tid == 0)
+      for (int c = 1; c <= TX; ++c) s_col[c] += s_col[c - 1];
+    TileBox box;
+    {
+      float r[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        r[k] = s_red[k][0];
+#pragma unroll
+        for (int w = 1; w < NW; ++w) r[k] = fminf(r[k], s_red[k][w]);
+      }
+      box.t1lo = r[0], box.t1hi = -r[1], box.t2lo = r[2], box.t2hi = -r[3];
+      box.u1lo = r[4], box.u1hi = -r[5], box.u2lo = r[6], box.u2hi = -r[7];
+      const int ncol = min(TX, a.nxb - ixb0), nrow = min(TZ, a.nzi - iz0);
+      box.x0 = (ixb0 + a.ixstart) * a.dxi;
+      box.x1 = (ixb0 + a.ixstart + ncol - 1) * a.dxi;
+      box.z0 = iz0 * a.dzi;
+      box.z1 = (iz0 + nrow - 1) * a.dzi;
+    }
+    __syncthreads();  // s_col complete
+    if (s_col[TX] == 0) continue;  // no active point in the tile
+    const int ixi_lo = ixb0 + a.ixstart, ixi_hi = ixi_lo + min(TX, a.nxb - ixb0) - 1;
 
-    for (int s0 = 0; s0 < nsrc && act; s0 += sc) {
+    for (int s0 = 0; s0 < nsrc; s0 += sc) {
       const int ns = min(sc, nsrc - s0);
       // source terms of this chunk for this thread's point
-      for (int s = 0; s < ns; ++s) {
+      for (int s = 0; s < ns && act; ++s) {
         const float2 sp = srcpos[s0 + s];
         float ts, qs;
         float2 *m = smap + (size_t)s * NT + tid;
@@ -975,116 +1091,173 @@ __global__ void __launch_bounds__(TZ *TX, MB)
         m[kMapPX * sc * NT] = make_float2(fmaf(-tanx1c, az, ax), fmaf(tanx2c, az, -ax));
         m[kMapPY * sc * NT] = make_float2(fmaf(-tany1c, az, ay), fmaf(tany2c, az, -ay));
       }
-      for (int g = 0; g < ngroups; ++g) {
-        const int4 gr = __ldg(grp + 2 * g);
-        if (gr.x >= gr.y || ixi < gr.z || ixi > gr.w) continue;
-        const int4 gs = __ldg(grp + 2 * g + 1);
-        if (gs.y < s0 || gs.x >= s0 + ns) continue;
-        // receiver terms, once per receiver position
-        const float2 gp = __ldg(grppos + g);
-        float tg, qg;
-        const bool rok = lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
-        const float dgx = gp.x - x;
-        const float dg = sqrtf(dgx * dgx + gp.y * gp.y + z2);
-        const float rdg = __fdividef(1.0f, dg);
-        const float agx = dgx * rdg, agy = gp.y * rdg, agz = z * rdg;
-        // dip-test thresholds of this receiver (NaN: no table value, every
-        // member fails)
-        const float qx1 = rok ? fmaf(tanx1c, agz, -agx) : NAN, qx2 = fmaf(-tanx2c, agz, agx);
-        const float qy1 = fmaf(tany1c, agz, -agy), qy2 = fmaf(-tany2c, agz, agy);
-        const float gfac = tg * rdg * rdg * rdg;  // receiver factor of (ds/dg)^3 tg/ts
-        // Members in blocks of U.  Phase 1, without branches, for all U: the
-        // member record, the aperture check (counted), the source direction
-        // and the dip test -- about 70 % of the members end here.  Phase 2:
-        // time/t* pick and weight of the members that passed.  Then all panel
-        // gathers, then the sums (in member order), so that U members' loads
-        // are in flight together.
-        for (int p0 = gr.x; p0 < gr.y; p0 += U) {
-          int4 mi[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u)
-            mi[u] = p0 + u < gr.y ? __ldg(mem + p0 + u) : make_int4(0, -1, 1, 0);
-          bool on[U];
-          int slv[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int sl = (mi[u].y & 0xFFFFFF) - s0;
-            const bool inr = sl >= 0 && sl < ns && ixi >= mi[u].z && ixi <= mi[u].w;
-            cnt += inr ? 1u : 0u;
-            slv[u] = inr ? sl : 0;
-            const float2 *m = smap + (size_t)slv[u] * NT + tid;
-            const float2 px = m[kMapPX * sc * NT], py = m[kMapPY * sc * NT];
-            on[u] = inr && px.x > qx1 && px.y > qx2 && py.x > qy1 && py.y > qy2;
-          }
-          const T *pp[U];
-          float fwt[U], fwb[U], fac[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            pp[u] = panels;
-            fwt[u] = fwb[u] = fac[u] = 0.0f;
-            if (!on[u]) continue;
-            on[u] = false;
-            const float2 *m = smap + (size_t)slv[u] * NT + tid;
-            const float2 tq = m[kMapTQ * sc * NT], cz = m[kMapCZ * sc * NT];
-            const float ts = tq.x;
-            // the pair's dip tangents (for the taper) from the stored terms
-            const float azs = cz.y;
-            const float uz = azs + agz;
-            const float ux = fmaf(tanx1c, azs, m[kMapPX * sc * NT].x) + agx;
-            const float uy = fmaf(tany1c, azs, m[kMapPY * sc * NT].x) + agy;
-            const float ruz = __fdividef(1.0f, uz);
-            const float tanx = ux * ruz, tany = uy * ruz;
-            // dip taper (most passing pairs lie in a taper zone: approximate
-            // divisions, ~2 ulp)
-            float w = 1.0f;
-            if (tanx < tanx1) w *= __fdividef(tanx - tanx1c, tanx1 - tanx1c);
-            if (tanx > tanx2) w *= __fdividef(tanx2c - tanx, tanx2c - tanx2);
-            if (tany < tany1) w *= __fdividef(tany - tany1c, tany1 - tany1c);
-            if (tany > tany2) w *= __fdividef(tany2c - tany, tany2c - tany2);
-            const float t = ts + tg;
-            const float ft = t * inv_dt1;
-            const int it1 = (int)ft;
-            if (!(it1 > 0 && it1 + 1 < a.nt)) continue;
-            const float fb = fminf(fmaxf((tq.y + qg) * inv_dts, 0.0f), (float)(a.nbins - 1));
-            const int b0 = min((int)fb, a.nbins - 2);
-            fwt[u] = ft - (float)it1;
-            fwb[u] = fb - (float)b0;
-            pp[u] = panels + (size_t)mi[u].x * pstride + (unsigned)(b0 * a.nt + it1);
-            // w v (r + 1/r), v = 100 / t^2 (10^4 below 0.1 s), with one reciprocal:
-            // w (r^2 + 1) * 100 / (r t^2)
-            const float r = cz.x * gfac;
-            const bool far = t > 0.1f;
-            fac[u] = w * fmaf(r, r, 1.0f) * __fdividef(far ? 100.0f : 10000.0f, far ? r * t * t : r);
-            if (std::is_same<T, __half>::value)  // 2^e from the record's exponent bits
-              fac[u] *= __int_as_float((int)((((unsigned)mi[u].y >> 24) - 1u) << 23));
-            on[u] = true;
-          }
-          float smp[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            smp[u] = 0.0f;
-            if (on[u]) {
-              const T *q = pp[u];
-              const float p00 = ld_sample<T>(q), p01 = ld_sample<T>(q + 1);
-              const float p10 = ld_sample<T>(q + a.nt), p11 = ld_sample<T>(q + a.nt + 1);
-              const float s0v = p00 + fwt[u] * (p01 - p00), s1v = p10 + fwt[u] * (p11 - p10);
-              smp[u] = s0v + fwb[u] * (s1v - s0v);
+      for (int pc0 = 0; pc0 < nmem; pc0 += MC) {
+        // the chunk's members kept for this tile (warp w, round k: word k NW + w)
+#pragma unroll 4
+        for (int k = 0; k < MC / NT; ++k) {
+          const int wi = k * NW + warp;
+          const int p = pc0 + 32 * wi + lane;
+          bool keep = false;
+          if (p < nmem) {
+            const int4 mi = __ldg(mem + p);
+            const int sl = (mi.y & 0xFFFFFF) - s0;
+            const int lo = max(mi.z, ixi_lo), hi = min(mi.w, ixi_hi);
+            if (sl >= 0 && sl < ns && lo <= hi) {
+              keep = tile_keep(__ldg(srcpos + s0 + sl), __ldg(grppos + __ldg(memgrp + p)), box);
+              // dropped: its in-aperture points still count
+              if (!keep) cnt += s_col[hi - ixi_lo + 1] - s_col[lo - ixi_lo];
             }
           }
+          const unsigned bits = __ballot_sync(0xffffffffu, keep);
+          if (lane == 0) s_mask[wi] = bits;
+        }
+        __syncthreads();
+        if (act) {
+          // kept members in order: word w of the mask, remaining bits mw
+          int w = 0;
+          unsigned mw = s_mask[0];
+          auto next = [&]() -> int {
+            while (mw == 0) {
+              if (++w >= NT) return -1;
+              mw = s_mask[w];
+            }
+            const int b = __ffs(mw) - 1;
+            mw &= mw - 1;
+            return pc0 + 32 * w + b;
+          };
+          int nxt = next();
+          int gn = nxt >= 0 ? __ldg(memgrp + nxt) : -1;
+          int cur = -1;
+          float agx = 0.f, agy = 0.f, agz = 0.f, qx1 = 0.f, qx2 = 0.f, qy1 = 0.f, qy2 = 0.f;
+          float tg = 0.f, qg = 0.f, gfac = 0.f;
+          while (nxt >= 0) {
+            const int g = gn;
+            if (g != cur) {
+              cur = g;
+              // receiver terms, once per receiver position
+              const float2 gp = __ldg(grppos + g);
+              const bool rok =
+                  lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
+              const float dgx = gp.x - x;
+              const float dg = sqrtf(dgx * dgx + gp.y * gp.y + z2);
+              const float rdg = __fdividef(1.0f, dg);
+              agx = dgx * rdg, agy = gp.y * rdg, agz = z * rdg;
+              // dip-test thresholds of this receiver (NaN: no table value,
+              // every member fails)
+              qx1 = rok ? fmaf(tanx1c, agz, -agx) : NAN;
+              qx2 = fmaf(-tanx2c, agz, agx);
+              qy1 = fmaf(tany1c, agz, -agy);
+              qy2 = fmaf(-tany2c, agz, agy);
+              gfac = tg * rdg * rdg * rdg;  // receiver factor of (ds/dg)^3 tg/ts
+            }
+            // up to U kept members of this receiver group
+            int pm[U];
+            pm[0] = nxt;
+            nxt = next();
+            gn = nxt >= 0 ? __ldg(memgrp + nxt) : -1;
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            if (!on[u]) continue;
-            const float val = fac[u] * smp[u];
-            if (comp) {
-              const float y = val - cmp;
-              const float tt = acc + y;
-              cmp = (tt - acc) - y;
-              acc = tt;
-            } else {
-              acc += val;
+            for (int u = 1; u < U; ++u) {
+              if (gn == g) {
+                pm[u] = nxt;
+                nxt = next();
+                gn = nxt >= 0 ? __ldg(memgrp + nxt) : -1;
+              } else {
+                pm[u] = -1;
+              }
+            }
+            // Phase 1, without branches, for all U: the member record, the
+            // aperture check (counted), the source direction and the dip
+            // test.  Phase 2: time/t* pick and weight of the members that
+            // passed.  Then all panel gathers, then the sums (in member
+            // order), so that U members' loads are in flight together.
+            int4 mi[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              mi[u] = pm[u] >= 0 ? __ldg(mem + pm[u]) : make_int4(0, -1, 1, 0);
+            bool on[U];
+            int slv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int sl = (mi[u].y & 0xFFFFFF) - s0;
+              const bool inr = sl >= 0 && sl < ns && ixi >= mi[u].z && ixi <= mi[u].w;
+              cnt += inr ? 1u : 0u;
+              slv[u] = inr ? sl : 0;
+              const float2 *m = smap + (size_t)slv[u] * NT + tid;
+              const float2 px = m[kMapPX * sc * NT], py = m[kMapPY * sc * NT];
+              on[u] = inr && px.x > qx1 && px.y > qx2 && py.x > qy1 && py.y > qy2;
+            }
+            const T *pp[U];
+            float fwt[U], fwb[U], fac[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              pp[u] = panels;
+              fwt[u] = fwb[u] = fac[u] = 0.0f;
+              if (!on[u]) continue;
+              on[u] = false;
+              const float2 *m = smap + (size_t)slv[u] * NT + tid;
+              const float2 tq = m[kMapTQ * sc * NT], cz = m[kMapCZ * sc * NT];
+              const float ts = tq.x;
+              // the pair's dip tangents (for the taper) from the stored terms
+              const float azs = cz.y;
+              const float uz = azs + agz;
+              const float ux = fmaf(tanx1c, azs, m[kMapPX * sc * NT].x) + agx;
+              const float uy = fmaf(tany1c, azs, m[kMapPY * sc * NT].x) + agy;
+              const float ruz = __fdividef(1.0f, uz);
+              const float tanx = ux * ruz, tany = uy * ruz;
+              // dip taper (most passing pairs lie in a taper zone: approximate
+              // divisions, ~2 ulp)
+              float wt = 1.0f;
+              if (tanx < tanx1) wt *= __fdividef(tanx - tanx1c, tanx1 - tanx1c);
+              if (tanx > tanx2) wt *= __fdividef(tanx2c - tanx, tanx2c - tanx2);
+              if (tany < tany1) wt *= __fdividef(tany - tany1c, tany1 - tany1c);
+              if (tany > tany2) wt *= __fdividef(tany2c - tany, tany2c - tany2);
+              const float t = ts + tg;
+              const float ft = t * inv_dt1;
+              const int it1 = (int)ft;
+              if (!(it1 > 0 && it1 + 1 < a.nt)) continue;
+              const float fb = fminf(fmaxf((tq.y + qg) * inv_dts, 0.0f), (float)(a.nbins - 1));
+              const int b0 = min((int)fb, a.nbins - 2);
+              fwt[u] = ft - (float)it1;
+              fwb[u] = fb - (float)b0;
+              pp[u] = panels + (size_t)mi[u].x * pstride + (unsigned)(b0 * a.nt + it1);
+              // w v (r + 1/r), v = 100 / t^2 (10^4 below 0.1 s), with one
+              // reciprocal: w (r^2 + 1) * 100 / (r t^2)
+              const float r = cz.x * gfac;
+              const bool far = t > 0.1f;
+              fac[u] = wt * fmaf(r, r, 1.0f) *
+                       __fdividef(far ? 100.0f : 10000.0f, far ? r * t * t : r);
+              if (std::is_same<T, __half>::value)  // 2^e from the record's exponent bits
+                fac[u] *= __int_as_float((int)((((unsigned)mi[u].y >> 24) - 1u) << 23));
+              on[u] = true;
+            }
+            float smp[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              smp[u] = 0.0f;
+              if (on[u]) {
+                const T *q = pp[u];
+                const float p00 = ld_sample<T>(q), p01 = ld_sample<T>(q + 1);
+                const float p10 = ld_sample<T>(q + a.nt), p11 = ld_sample<T>(q + a.nt + 1);
+                const float s0v = p00 + fwt[u] * (p01 - p00), s1v = p10 + fwt[u] * (p11 - p10);
+                smp[u] = s0v + fwb[u] * (s1v - s0v);
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              if (!on[u]) continue;
+              const float val = fac[u] * smp[u];
+              if (comp) {
+                const float y = val - cmp;
+                const float tt = acc + y;
+                cmp = (tt - acc) - y;
+                acc = tt;
+              } else {
+                acc += val;
+              }
             }
           }
         }
+        __syncthreads();  // the mask is rewritten by the next chunk
       }
     }
     if (live) {
@@ -1117,6 +1290,7 @@ static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p) {
   ok &= cudaMalloc(&s->d_mem, sizeof(int4) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_grp, sizeof(int4) * 2 * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_grppos, sizeof(float2) * n) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_memgrp, sizeof(int) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_tile_ctr, sizeof(int)) == cudaSuccess;
   if (!ok) return QPSDM_ENOMEM;
   size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
@@ -1182,8 +1356,8 @@ static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const Ph
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TZ * TX, smem);
   const int grid = std::max(1, std::min(ntz * ntx, std::max(per_sm, 1) * s->num_sms));
   cudaMemsetAsync(s->d_tile_ctr, 0, sizeof(int), st);
-  kern<<<grid, TZ * TX, smem, st>>>(img, comp, a, v.dips, s->d_grp, s->d_grppos, s->d_nruns,
-                                    s->d_mem, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
+  kern<<<grid, TZ * TX, smem, st>>>(img, comp, a, v.dips, s->d_memgrp, s->d_grppos, s->d_mem,
+                                    b.ntr, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
                                     v.tab->ttt, v.tab->dq, v.tab->qqq, (const T *)s->d_panels,
                                     s->d_tile_ctr, ntz, ntx, sc, npt);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
@@ -1297,7 +1471,7 @@ static int batched_group(PhysicsState *s, const qpsdm_static_params &p, const Li
   if (cub::DeviceScan::ExclusiveSum(s->d_cub, tb, s->d_count, s->d_off, n, st) != cudaSuccess)
     return QPSDM_ECUDA;
   k_batch_groups<<<grd, blk, 0, st>>>(s->d_ukey, s->d_count, s->d_off, s->d_nruns, s->d_val[1],
-                                      v.ints, s->d_sid, s->d_grp, s->d_grppos, n);
+                                      v.ints, s->d_sid, s->d_grp, s->d_grppos, s->d_memgrp, n);
   k_batch_members<<<grd, blk, 0, st>>>(b.d_rec, b.rec_bytes, b.big_endian, n, s->d_val[1],
                                        v.ints, s->d_sid, s->d_srcflag, p.scaled, l.fxi, l.cyi,
                                        s->dtype == QPSDM_PANEL_FP16 ? s->d_pscale : nullptr,
