@@ -114,6 +114,50 @@ def test_batched_many_shots_and_splits(cuda):
     assert nrmse(img, ref) <= 5e-5
 
 
+def _varied_dips(case, seed=5):
+    """The case with dip limits that change from point to point (random in
+    [-0.35, -0.05] and [0.05, 0.35]), so that a tile's dip ranges matter."""
+    c = dict(case)
+    rng = np.random.default_rng(seed)
+    n = case["dips"].shape[1]
+    lo = -rng.uniform(0.05, 0.35, size=(2, n)).astype(np.float32)
+    hi = rng.uniform(0.05, 0.35, size=(2, n)).astype(np.float32)
+    c["dips"] = np.stack([lo[0], hi[0], lo[1], hi[1]])
+    return c
+
+
+def _image(c, **kw):
+    eng, p, o = engine(c, **kw)
+    try:
+        eng.submit(records(c))
+        img = eng.get_image(False)
+        _, npt = eng.counters()
+    finally:
+        eng.close()
+    return img, npt
+
+
+@pytest.mark.parametrize("dips", ["reference", "varied"])
+def test_batched_pointwise_equals_plain(cuda, case, dips):
+    """The batched kernel drops, per image tile, the members whose dip test
+    fails at every point of the tile (a conservative bound).  With FP32
+    panels its image must then equal the plain form's point by point up to
+    the order of the FP32 sums, for every tile shape, with the same
+    point-trace count.  Varied dip limits also against the FP64 oracle."""
+    c = case if dips == "reference" else _varied_dips(case)
+    plain, n0 = _image(c, panel_dtype=0, form=0)
+    amp = np.abs(plain).max()
+    assert amp > 0
+    for tile in [(32, 8), (64, 4), (16, 8), (8, 16), (4, 32)]:
+        img, n = _image(c, panel_dtype=0, form=1, tile=tile)
+        assert n == n0, tile
+        assert np.abs(img - plain).max() <= 2e-5 * amp, tile
+    if dips == "varied":
+        ref, npt, _ = oracle_run(c)
+        assert n0 == npt
+        assert nrmse(plain, ref) <= 5e-5
+
+
 # ---- image bricks (several lines per submit) ------------------------------
 @pytest.mark.parametrize("form,dtype,tol", [(0, 0, 5e-5), (1, 0, 5e-5), (1, 1, 1e-3)])
 def test_brick_equals_single_lines(cuda, form, dtype, tol):
