@@ -831,19 +831,16 @@ __global__ void k_batch_keys(const uint8_t *__restrict__ rec, int rec_bytes, int
 }
 
 // Group records: [2g] = (first sorted position, end, min ixi1, max ixi2),
-// [2g+1] = (min source, max source); receiver position per group; the group
-// of every sorted position.
+// [2g+1] = (min source, max source); receiver position per group.
 __global__ void k_batch_groups(const unsigned long long *__restrict__ ukey,
                                const int *__restrict__ count, const int *__restrict__ off,
                                const int *__restrict__ nruns, const int *__restrict__ sval,
                                const int *__restrict__ ints, const int *__restrict__ sid,
-                               int4 *__restrict__ grp, float2 *__restrict__ grppos,
-                               int *__restrict__ memgrp, int ntr) {
+                               int4 *__restrict__ grp, float2 *__restrict__ grppos, int ntr) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ntr || g >= *nruns) return;
   const unsigned long long k = ukey[g];
   const int start = off[g], n = count[g];
-  for (int p = start; p < start + n; ++p) memgrp[p] = g;
   if (k == kNoKey) {
     grp[2 * g] = make_int4(start, start, 1, 0);
     grp[2 * g + 1] = make_int4(1, 0, 0, 0);
@@ -862,6 +859,20 @@ __global__ void k_batch_groups(const unsigned long long *__restrict__ ukey,
   grp[2 * g + 1] = make_int4(s0, s1, 0, 0);
   grppos[g] = make_float2(__uint_as_float((unsigned)(k & 0xffffffffu)),
                           __uint_as_float((unsigned)(k >> 32)));
+}
+
+// The group of every sorted position: the last run whose first position is
+// at or before it (off: exclusive prefix sums of the run lengths).
+__global__ void k_batch_memgrp(const int *__restrict__ off, const int *__restrict__ nruns,
+                               int *__restrict__ memgrp, int ntr) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ntr) return;
+  int lo = 0, hi = *nruns;  // off[lo] <= p < off[hi] (off[nruns] taken as ntr)
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= p) lo = mid; else hi = mid;
+  }
+  memgrp[p] = lo;
 }
 
 // Member info per sorted position (trace, source, column range) and the
@@ -1471,7 +1482,8 @@ static int batched_group(PhysicsState *s, const qpsdm_static_params &p, const Li
   if (cub::DeviceScan::ExclusiveSum(s->d_cub, tb, s->d_count, s->d_off, n, st) != cudaSuccess)
     return QPSDM_ECUDA;
   k_batch_groups<<<grd, blk, 0, st>>>(s->d_ukey, s->d_count, s->d_off, s->d_nruns, s->d_val[1],
-                                      v.ints, s->d_sid, s->d_grp, s->d_grppos, s->d_memgrp, n);
+                                      v.ints, s->d_sid, s->d_grp, s->d_grppos, n);
+  k_batch_memgrp<<<grd, blk, 0, st>>>(s->d_off, s->d_nruns, s->d_memgrp, n);
   k_batch_members<<<grd, blk, 0, st>>>(b.d_rec, b.rec_bytes, b.big_endian, n, s->d_val[1],
                                        v.ints, s->d_sid, s->d_srcflag, p.scaled, l.fxi, l.cyi,
                                        s->dtype == QPSDM_PANEL_FP16 ? s->d_pscale : nullptr,
