@@ -1038,6 +1038,10 @@ __global__ void __launch_bounds__(TZ *TX, MB)
     const float tanx2c = tanx2 + tz * (1.0f + tanx2 * tanx2);
     const float tany1c = tany1 - tz * (1.0f + tany1 * tany1);
     const float tany2c = tany2 + tz * (1.0f + tany2 * tany2);
+    // inverse taper-zone widths: the taper factor at a passing pair is
+    // min(1, f / (w uz)) for the test function f of each limit, w = |tan - tanc|
+    const float iwx1 = 1.0f / (tanx1 - tanx1c), iwx2 = 1.0f / (tanx2c - tanx2);
+    const float iwy1 = 1.0f / (tany1 - tany1c), iwy2 = 1.0f / (tany2c - tany2);
     const float z2 = z * z;
     const float x = ixi * a.dxi;
     // the tile's box and dip-limit ranges over its active points
@@ -1207,21 +1211,17 @@ __global__ void __launch_bounds__(TZ *TX, MB)
               on[u] = false;
               const float2 *m = smap + (size_t)slv[u] * NT + tid;
               const float2 tq = m[kMapTQ * sc * NT], cz = m[kMapCZ * sc * NT];
+              const float2 px = m[kMapPX * sc * NT], py = m[kMapPY * sc * NT];
               const float ts = tq.x;
-              // the pair's dip tangents (for the taper) from the stored terms
-              const float azs = cz.y;
-              const float uz = azs + agz;
-              const float ux = fmaf(tanx1c, azs, m[kMapPX * sc * NT].x) + agx;
-              const float uy = fmaf(tany1c, azs, m[kMapPY * sc * NT].x) + agy;
-              const float ruz = __fdividef(1.0f, uz);
-              const float tanx = ux * ruz, tany = uy * ruz;
-              // dip taper (most passing pairs lie in a taper zone: approximate
-              // divisions, ~2 ulp)
-              float wt = 1.0f;
-              if (tanx < tanx1) wt *= __fdividef(tanx - tanx1c, tanx1 - tanx1c);
-              if (tanx > tanx2) wt *= __fdividef(tanx2c - tanx, tanx2c - tanx2);
-              if (tany < tany1) wt *= __fdividef(tany - tany1c, tany1 - tany1c);
-              if (tany > tany2) wt *= __fdividef(tany2c - tany, tany2c - tany2);
+              // dip taper from the pair's test functions (ux - tanx1c uz and
+              // the like, all > 0 here): (tanx - tanx1c) / (tanx1 - tanx1c) =
+              // (ux - tanx1c uz) / ((tanx1 - tanx1c) uz) below tanx1, likewise
+              // at the other three limits; of the two limits of an axis at
+              // most one taper is active, so each axis takes the smaller ratio
+              const float ruz = __fdividef(1.0f, cz.y + agz);
+              const float ex = fminf((px.x - qx1) * iwx1, (px.y - qx2) * iwx2);
+              const float ey = fminf((py.x - qy1) * iwy1, (py.y - qy2) * iwy2);
+              const float wt = fminf(1.0f, ex * ruz) * fminf(1.0f, ey * ruz);
               const float t = ts + tg;
               const float ft = t * inv_dt1;
               const int it1 = (int)ft;
