@@ -1100,7 +1100,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
         const float ds = sqrtf(dsx * dsx + sp.y * sp.y + z2);
         const float rds = __fdividef(1.0f, ds);
         const float ax = dsx * rds, ay = sp.y * rds, az = z * rds;
-        m[kMapTQ * sc * NT] = make_float2(ts, qs);
+        m[kMapTQ * sc * NT] = make_float2(ts, qs * inv_dts);  // t* in bins
         // source factor of (ds/dg)^3 tg/ts
         m[kMapCZ * sc * NT] = make_float2(__fdividef(ds * ds * ds, ts), az);
         m[kMapPX * sc * NT] = make_float2(fmaf(-tanx1c, az, ax), fmaf(tanx2c, az, -ax));
@@ -1164,6 +1164,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
               qy1 = fmaf(tany1c, agz, -agy);
               qy2 = fmaf(-tany2c, agz, agy);
               gfac = tg * rdg * rdg * rdg;  // receiver factor of (ds/dg)^3 tg/ts
+              qg *= inv_dts;                // t* in bins
             }
             // up to U kept members of this receiver group
             int pm[U];
@@ -1194,7 +1195,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               const int sl = (mi[u].y & 0xFFFFFF) - s0;
-              const bool inr = sl >= 0 && sl < ns && ixi >= mi[u].z && ixi <= mi[u].w;
+              const bool inr = (unsigned)sl < (unsigned)ns && ixi >= mi[u].z && ixi <= mi[u].w;
               cnt += inr ? 1u : 0u;
               slv[u] = inr ? sl : 0;
               const float2 *m = smap + (size_t)slv[u] * NT + tid;
@@ -1226,7 +1227,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
               const float ft = t * inv_dt1;
               const int it1 = (int)ft;
               if (!(it1 > 0 && it1 + 1 < a.nt)) continue;
-              const float fb = fminf(fmaxf((tq.y + qg) * inv_dts, 0.0f), (float)(a.nbins - 1));
+              const float fb = fminf(fmaxf(tq.y + qg, 0.0f), (float)(a.nbins - 1));
               const int b0 = min((int)fb, a.nbins - 2);
               fwt[u] = ft - (float)it1;
               fwb[u] = fb - (float)b0;
