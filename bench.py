@@ -57,7 +57,7 @@ F_PT = {"batched": 64, "plain": 64, "compat": 35}
 # DRAM bytes (read + write) per point-trace of the image kernel, from one ncu
 # capture each (profiles/): scaled to a launch by its point-traces.
 TRAFFIC_B_PER_PT = {
-    "batched": (194.8e6 + 4.1e6) / 1.943e9,   # 2 gathers x 1 line capture
+    "batched": (190.7e6 + 6.6e6) / 1.943e9,   # 2 gathers x 1 line capture
     "plain": (229.7e6 + 4.9e6) / 9.58e8,      # the plain form's own step
     "compat": 4.55e6 / 9.83e8,                # the compat form's own step
 }

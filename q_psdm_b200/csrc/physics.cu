@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -53,6 +54,10 @@ struct PhysicsState {
     qpsdm_ttt_desc *dt = nullptr, *dq = nullptr;
     float *ttt = nullptr, *qqq = nullptr;
     size_t dt_cap = 0, dq_cap = 0, ttt_cap = 0, qqq_cap = 0;
+    // batched form, t and t* tables with identical descriptors: (t, t*) pairs
+    float2 *tq = nullptr;
+    size_t tq_cap = 0;
+    bool paired = false;
   };
   std::vector<LineTab> tabs;  // one per line of the brick
   float *d_tab_tmp = nullptr;  // batched form: table upload before the re-layout
@@ -211,6 +216,7 @@ void physics_destroy(PhysicsState *s) {
     cudaFree(t.dq);
     cudaFree(t.ttt);
     cudaFree(t.qqq);
+    cudaFree(t.tq);
   }
   cudaFree(s->d_any);
   cudaFree(s->d_tune);
@@ -261,6 +267,14 @@ static int check_tables(const qpsdm_line_params &l, std::string *err) {
 // fastest), so that image points of neighbouring cdps, which a warp of the
 // batched kernel holds, read neighbouring table words.  Out of place:
 // descriptors may share a block.
+// (t, t*) pairs of two tables with identical descriptors.
+__global__ void k_tab_pair(const float *__restrict__ t, const float *__restrict__ q,
+                           float2 *__restrict__ tq, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    tq[i] = make_float2(t[i], q[i]);
+}
+
 __global__ void k_tab_xfast(const float *__restrict__ in, float *__restrict__ out,
                             const qpsdm_ttt_desc *__restrict__ desc, int nxi1, int nzi1) {
   const qpsdm_ttt_desc d = desc[blockIdx.y];
@@ -306,6 +320,17 @@ int physics_set_lines(PhysicsState *s, const qpsdm_static_params &p,
       k_tab_xfast<<<g, 256, 0, st>>>(s->d_tab_tmp, t.ttt, t.dt, l.nxi1, l.nzi1);
       cudaMemcpyAsync(s->d_tab_tmp, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyHostToDevice, st);
       k_tab_xfast<<<g, 256, 0, st>>>(s->d_tab_tmp, t.qqq, t.dq, l.nxi1, l.nzi1);
+      // identical descriptors (the reference writes both tables alike): the
+      // image kernel reads t and t* of a node with one 8-byte load
+      t.paired = l.ttt_len == l.qqq_len &&
+                 std::memcmp(l.ttt_desc, l.qqq_desc, sizeof(qpsdm_ttt_desc) * ncell) == 0;
+      if (t.paired) {
+        if (!grow_dev(&t.tq, &t.tq_cap, (size_t)l.ttt_len)) {
+          if (err) *err = "paired table allocation failed";
+          return QPSDM_ENOMEM;
+        }
+        k_tab_pair<<<148 * 8, 256, 0, st>>>(t.ttt, t.qqq, t.tq, l.ttt_len);
+      }
     } else {
       cudaMemcpyAsync(t.ttt, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(t.qqq, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyHostToDevice, st);
@@ -675,6 +700,42 @@ __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
   return true;
 }
 
+// lookup_tq for a line whose t and t* tables have identical descriptors,
+// read as (t, t*) pairs (tq): same values, same arithmetic, half the loads.
+__device__ __forceinline__ float2 bilin2(const float2 *__restrict__ tab, int64_t base, int64_t sx,
+                                         int64_t sy, float wx, float wy) {
+  const float2 v00 = __ldg(tab + base), v01 = __ldg(tab + base + sx);
+  const float2 v10 = __ldg(tab + base + sy), v11 = __ldg(tab + base + sy + sx);
+  const float at = v00.x + wx * (v01.x - v00.x), bt = v10.x + wx * (v11.x - v10.x);
+  const float aq = v00.y + wx * (v01.y - v00.y), bq = v10.y + wx * (v11.y - v10.y);
+  return make_float2(at + wy * (bt - at), aq + wy * (bq - aq));
+}
+__device__ __forceinline__ bool lookup_tq(const PointCells &pc,
+                                          const qpsdm_ttt_desc *__restrict__ dt,
+                                          const float *__restrict__ ttt,
+                                          const qpsdm_ttt_desc *__restrict__ dq,
+                                          const float *__restrict__ qqq,
+                                          const float2 *__restrict__ tq, int nxi1, int nzi1,
+                                          float px, float py, float &t, float &q) {
+  if (!tq || !pc.same) return lookup_tq(pc, dt, ttt, dq, qqq, nxi1, nzi1, px, py, t, q);
+  const int nxs = pc.nxs, nys = pc.nys;
+  const float fx = (px - pc.xc) * pc.rdx + pc.hx;
+  const float fy = py * pc.rdy + pc.hy;
+  if (!(fx >= 0.0f && fx <= (float)(nxs - 1) && fy >= 0.0f && fy <= (float)(nys - 1)))
+    return false;
+  const int ix = min((int)fx, max(nxs - 2, 0));
+  const int iy = min((int)fy, max(nys - 2, 0));
+  const float wx = nxs > 1 ? fx - ix : 0.0f, wy = nys > 1 ? fy - iy : 0.0f;
+  const int64_t plane = (int64_t)nxi1 * nzi1;
+  const int64_t sx = nxs > 1 ? plane : 0, sy = nys > 1 ? (int64_t)nxs * plane : 0;
+  const int64_t off = (int64_t)(iy * nxs + ix) * plane;
+  const float2 a = bilin2(tq, pc.tA + off + pc.offA, sx, sy, wx, wy);
+  const float2 b = bilin2(tq, pc.tB + off + pc.offB, sx, sy, wx, wy);
+  t = a.x + pc.c2 * (b.x - a.x);
+  q = a.y + pc.c2 * (b.y - a.y);
+  return true;
+}
+
 constexpr int kPhysBz = 32, kPhysBx = 8, kPhysChunk = 256;
 
 template <typename T>
@@ -989,8 +1050,9 @@ __global__ void __launch_bounds__(TZ *TX, MB)
                     const float2 *__restrict__ srcpos, const int *__restrict__ nsrc_ptr,
                     const qpsdm_ttt_desc *__restrict__ dt, const float *__restrict__ ttt,
                     const qpsdm_ttt_desc *__restrict__ dq, const float *__restrict__ qqq,
-                    const T *__restrict__ panels, int *__restrict__ tile_ctr, int ntz, int ntx,
-                    int sc, unsigned long long *npt) {
+                    const float2 *__restrict__ tqp, const T *__restrict__ panels,
+                    int *__restrict__ tile_ctr, int ntz, int ntx, int sc,
+                    unsigned long long *npt) {
   constexpr int NT = TZ * TX, NW = NT / 32, MC = 32 * NT;
   static_assert(NT % 32 == 0, "whole warps");
   extern __shared__ float2 smap[];  // [kMapN][sc][NT]
@@ -1088,7 +1150,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
         const float2 sp = srcpos[s0 + s];
         float ts, qs;
         float2 *m = smap + (size_t)s * NT + tid;
-        if (!lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, sp.x, sp.y, ts, qs)) {
+        if (!lookup_tq(pc, dt, ttt, dq, qqq, tqp, a.nxi1, a.nzi1, sp.x, sp.y, ts, qs)) {
           // no table value: NaN fails every member's dip test
           m[kMapTQ * sc * NT] = make_float2(NAN, 0.0f);
           m[kMapCZ * sc * NT] = make_float2(0.0f, NAN);
@@ -1152,7 +1214,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
               // receiver terms, once per receiver position
               const float2 gp = __ldg(grppos + g);
               const bool rok =
-                  lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
+                  lookup_tq(pc, dt, ttt, dq, qqq, tqp, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
               const float dgx = gp.x - x;
               const float dg = sqrtf(dgx * dgx + gp.y * gp.y + z2);
               const float rdg = __fdividef(1.0f, dg);
@@ -1370,7 +1432,8 @@ static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const Ph
   cudaMemsetAsync(s->d_tile_ctr, 0, sizeof(int), st);
   kern<<<grid, TZ * TX, smem, st>>>(img, comp, a, v.dips, s->d_memgrp, s->d_grppos, s->d_mem,
                                     b.ntr, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
-                                    v.tab->ttt, v.tab->dq, v.tab->qqq, (const T *)s->d_panels,
+                                    v.tab->ttt, v.tab->dq, v.tab->qqq,
+                                    v.tab->paired ? v.tab->tq : nullptr, (const T *)s->d_panels,
                                     s->d_tile_ctr, ntz, ntx, sc, npt);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }

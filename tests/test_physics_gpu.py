@@ -158,6 +158,33 @@ def test_batched_pointwise_equals_plain(cuda, case, dips):
         assert nrmse(plain, ref) <= 5e-5
 
 
+class _ShiftedQ:
+    """Tables whose t* data sit behind a padding block, so that the t and t*
+    descriptors differ (idx) while every value is the same."""
+
+    def __init__(self, tab, pad=1000):
+        self.tab, self.pad, self.dzii = tab, pad, tab.dzii
+
+    def as_engine_dict(self):
+        d = self.tab.as_engine_dict()
+        dq = d["qqq_desc"].copy()
+        dq[:, :8].view(np.int64)[:, 0] += self.pad
+        d["qqq_desc"] = dq
+        d["qqq"] = np.concatenate([np.full(self.pad, 7.0, np.float32), d["qqq"]])
+        return d
+
+
+def test_batched_unpaired_tables(cuda, case):
+    """t and t* tables with different descriptors take the two-table lookup
+    (identical descriptors are read as (t, t*) pairs): same image."""
+    paired, n0 = _image(case, panel_dtype=0, form=1)
+    c = dict(case)
+    c["tab"] = _ShiftedQ(case["tab"])
+    img, n = _image(c, panel_dtype=0, form=1)
+    assert n == n0
+    assert np.abs(img - paired).max() <= 1e-6 * np.abs(paired).max()
+
+
 # ---- image bricks (several lines per submit) ------------------------------
 @pytest.mark.parametrize("form,dtype,tol", [(0, 0, 5e-5), (1, 0, 5e-5), (1, 1, 1e-3)])
 def test_brick_equals_single_lines(cuda, form, dtype, tol):
