@@ -10,7 +10,7 @@ A point-trace is one (image point, trace) pair inside the trace's aperture;
 the engine counts them on the device.
 
 Forms (a step = one pass over one batch):
-  batched  8 shot gathers (73728 traces) into a brick of 8 image lines; FP16
+  batched  8 shot gathers (73728 traces) into a brick of 16 image lines; FP16
            t* panels (each trace scaled by a power of two into FP16's range)
            computed once per trace and shared by the brick;
            receiver-grouped persistent kernel.  The headline.
@@ -62,7 +62,7 @@ TRAFFIC_B_PER_PT = {
     "compat": 4.55e6 / 9.83e8,                # the compat form's own step
 }
 FORMS = {  # shots per step, lines per step, panel dtype, physics form
-    "batched": (8, 8, 2, 1),
+    "batched": (8, 16, 2, 1),
     "plain": (1, 1, 0, 0),
     "compat": (1, 1, 0, None),
 }
