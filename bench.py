@@ -724,7 +724,11 @@ def run_reference(args, rank, world):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": wl.config("compat"), "cpu_baseline": info,
+            "config": dict(wl.config("batched"), reference_path=(
+                "the reference's own CPU path of the same workload: its preprocessing "
+                "compiled from its sources (oracle/_ref) and the C restatement of its "
+                "imaging kernel, per shot gather and line, all host threads")),
+            "cpu_baseline": info,
             "e2e": {"value": v, "unit": "Gpoint-traces/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
