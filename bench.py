@@ -705,6 +705,70 @@ def accuracy_vs_fp64(wl, dev, ntr=1536, seed=2):
     return out
 
 
+def accuracy_config(name, dev, ntr=1200):
+    """Image NRMSE of the batched (FP16 panels) and plain (FP32 panels) forms
+    against the FP64 oracle on a seeded sample of configuration `name`
+    (`synth.accuracy_sample`: its own geometry, trace length, Q model, gain
+    limit and image size), one line."""
+    from oracle import oracle as O
+    from q_psdm_b200 import engine as E
+    from q_psdm_b200 import synth
+    smp = synth.accuracy_sample(name, ntr=ntr)
+    sv, tab = smp["sv"], smp["tab"]
+    st = O.derive_static(sv.ntl, np.float32(sv.dt), sv.threshold, 3.0, 8.0)
+    az = np.stack(smp["az"]).astype(np.int32)
+    keep = [O.iaztab()] + [np.ascontiguousarray(az[i]) for i in range(4)]
+    ip = lambda x: x.ctypes.data_as(C.POINTER(C.c_int))
+    gp = O.GateParams(scaled=sv.scaled, fxv1=np.float32(sv.fxv - 2000.0),
+                      fyv1=np.float32(sv.fyv - 1000.0),
+                      exv1=np.float32(sv.fxv + sv.nxi * sv.dxi + 2000.0),
+                      eyv1=np.float32(sv.fyv + sv.nyi * sv.dyi + 1000.0), fxi=sv.fxv,
+                      cyi=smp["cyi"], dxi=sv.dxi, dyi=sv.dyi, eps=0.001, nzi=sv.nzi,
+                      ixstart=0, ixend=sv.nxi, iaztab=ip(keep[0]), aznx1=ip(keep[1]),
+                      aznx2=ip(keep[2]), azny1=ip(keep[3]), azny2=ip(keep[4]))
+    ints, geom = O.gate_traces(gp, smp["hdr"])
+    ok = ints[:, 0] == 3
+    dts = float(np.float32(smp["dtstar"]))
+    filt = O.physics_filter(st["nfft"], np.float32(sv.dt), 130.0, 140.0, sv.fpeak,
+                            sv.threshold, 16, smp["dtstar"])
+    pan = O.physics_panels(smp["traces"][ok], np.float32(sv.dt), st["nfft"], st["nffti"], filt)
+    pp = O.PhysParams(nzi=sv.nzi, nxb=sv.nxi, ixstart=0, nt=st["nffti"], nbins=16,
+                      dt1=float(st["dt1"]), dxi=sv.dxi, dzi=sv.dzi,
+                      taperzone=float(st["taperzone"]), dtstar=dts, dzii=tab.dzii,
+                      tcdp1=tab.cdp1 - sv.fci, tcdp2=tab.cdp2 - sv.fci, nxg=tab.nxg,
+                      nzg=tab.nzg, nxi1=tab.nxi1, nzi1=tab.nzi1)
+    dips = [d.ravel() for d in synth.dip_fields(sv.nxi, sv.nzi, float(st["contract"]))]
+    ref, npt = O.physics_image(pp, geom[ok], ints[ok][:, [4, 5, 7]], pan, dips,
+                               tab.as_engine_dict())
+    ref = np.asarray(ref, np.float64).reshape(sv.nxi, sv.nzi)
+    out = {"sample": smp["describe"] + f" ({npt} point-traces, nt {sv.ntl}, "
+                                       f"nffti {st['nffti']}, gain limit {sv.threshold:g})"}
+    for form, dtype in (("batched", 2), ("plain", 0)):
+        p = E.static_params(nxi=sv.nxi, nzi=sv.nzi, ntl=sv.ntl, dt=float(sv.dt), dxi=sv.dxi,
+                            dyi=sv.dyi, dzi=sv.dzi, fci=sv.fci, scaled=sv.scaled, fxv=sv.fxv,
+                            fyv=sv.fyv, nxv=sv.nxi, nyv=sv.nyi, fc=sv.fpeak,
+                            threshold=sv.threshold, mode=1, panel_dtype=dtype, nbins=16,
+                            dtstar=smp["dtstar"], form=1 if form == "batched" else 0,
+                            dzii=tab.dzii, max_batch=len(smp["hdr"]))
+        eng = E.Engine(p, device=dev)
+        try:
+            eng.set_lines([dict(fxi=sv.fxv, cyi=smp["cyi"],
+                                dips=synth.dip_fields(sv.nxi, sv.nzi, p.contract),
+                                tables=tab.as_engine_dict())])
+            eng.begin_offset(E.offset_params(p, 0, sv.nxi, aznx1=az[0], aznx2=az[1],
+                                             azny1=az[2], azny2=az[3]))
+            eng.submit(smp["records"])
+            img = np.asarray(eng.get_image(False), np.float64).reshape(sv.nxi, sv.nzi)
+            _, n = eng.counters()
+        finally:
+            eng.close()
+        if n != npt:
+            raise RuntimeError(f"{name} {form}: point-traces {n} != oracle {npt}")
+        e = float(np.sqrt(np.mean((img - ref) ** 2)) / np.sqrt(np.mean(ref ** 2)))
+        out[f"nrmse_{form}_{'fp16' if dtype == 2 else 'fp32'}_panels_vs_fp64"] = e
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -753,14 +817,20 @@ def main():
         res = run_reference(args, rank, world)
     else:
         res, wl = run_ours(args, rank, world, dist)
-        if res is not None and not args.no_accuracy:
-            res["accuracy"] = accuracy_vs_fp64(wl, int(os.environ.get("LOCAL_RANK", "0")))
+        dev = int(os.environ.get("LOCAL_RANK", "0"))
         if res is not None and not args.no_surrogate:
-            res["surrogate"] = run_surrogate(int(os.environ.get("LOCAL_RANK", "0")),
-                                             args.steps, args.warmup)
+            res["surrogate"] = run_surrogate(dev, args.steps, args.warmup)
         if res is not None and not args.no_cpu:
+            # the CPU leg: the oracle timed on a host sample and, unless
+            # --no-accuracy, the oracle's FP64 images of seeded samples (this
+            # workload's and one of configurations 1, 3 and 5 each) against
+            # the engine's images of the same traces
             res["cpu_baseline"] = (cpu_compat_rate(wl) if args.form == "compat"
                                    else cpu_physics_rate(wl))
+            if not args.no_accuracy:
+                res["accuracy"] = accuracy_vs_fp64(wl, dev)
+                res["accuracy"]["configs"] = {n: accuracy_config(n, dev)
+                                              for n in ("c1", "c3", "c5")}
     if res is not None:
         print(json.dumps(res), flush=True)
     if dist:

@@ -41,6 +41,14 @@ class Survey:
     scalco: int = -100         # coordinates stored in cm
     fci: int = 1
     seed: int = 0
+    # per-shot receiver indices (gathers of uneven size); None: every shot
+    # records the whole spread
+    gathers: list | None = None
+    # Q model: None (constant q), ("layers", z_nodes, q_nodes) with Q linear
+    # between the nodes, or ("cloud", x, y, z, radius, q_cloud) inside a
+    # background of constant q
+    q_model: tuple | None = None
+    threshold: float = 600.0   # gain limit of the inverse-Q filter
 
     @property
     def fxv(self) -> float:     # x of image cdp fci (velocity grid = image grid)
@@ -60,7 +68,12 @@ class Survey:
 
     @property
     def ntraces(self) -> int:
+        if self.gathers is not None:
+            return int(sum(len(g) for g in self.gathers))
         return len(self.shots) * len(self.receivers)
+
+    def receivers_of(self, shot: int) -> np.ndarray:
+        return self.receivers if self.gathers is None else self.receivers[self.gathers[shot]]
 
 
 def config1(seed: int = 0) -> Survey:
@@ -95,6 +108,52 @@ def config2(seed: int = 0) -> Survey:
                   80.0, 30.0, shots, receivers, 2000.0, diff, 20.0, seed=seed)
 
 
+def config3(seed: int = 0) -> Survey:
+    """Batching stress case: image 768x768x500 at 10 m, v(z)=1800+0.5z,
+    nt=2500, dt=2 ms, 25 Hz; 1024 shots on a 32x32 grid, each recording the
+    n nearest receivers of a 128x128 spread at 60 m, n seeded uniform in
+    [500, 12000] (gathers of uneven size); smooth random Q: linear between
+    seeded values in [25, 150] every 700 m of depth."""
+    rng = np.random.default_rng([seed, 3])
+    g = X0 + 120.0 + 240.0 * np.arange(32)
+    shots = np.array([(x, Y0 + (y - X0)) for y in g for x in g])
+    r1 = 30.0 + 60.0 * np.arange(128)
+    receivers = np.array([(X0 + x, Y0 + y) for y in r1 for x in r1])
+    counts = rng.integers(500, 12001, size=len(shots))
+    gathers = []
+    for (sx, sy), n in zip(shots, counts):
+        d2 = (receivers[:, 0] - sx) ** 2 + (receivers[:, 1] - sy) ** 2
+        gathers.append(np.sort(np.argsort(d2, kind="stable")[:n]))
+    zn = np.arange(0.0, 5600.0, 700.0)
+    qn = rng.uniform(25.0, 150.0, size=len(zn))
+    diff = np.array([[X0 + 2000.0, Y0 + 3840.0, 1500.0],
+                     [X0 + 3840.0, Y0 + 3840.0, 2600.0],
+                     [X0 + 5600.0, Y0 + 3000.0, 3800.0]])
+    return Survey("c3", 768, 768, 500, 10.0, 10.0, 10.0, 2500, 0.002, 1800.0, 0.5,
+                  80.0, 25.0, shots, receivers, 2500.0, diff, 20.0, seed=seed,
+                  gathers=gathers, q_model=("layers", zn, qn))
+
+
+def config5(seed: int = 0) -> Survey:
+    """Large, strongly attenuating case: image 1024x1024x600 at 10 m,
+    v(z)=1800+0.5z, nt=3000, dt=2 ms, 25 Hz; 350 shots (14 x 25) x 100x100
+    receivers at 102.4 m = 3.5 M traces; Q = 100 with a gas cloud of Q = 20
+    (radius 800 m, centre 1500 m deep under the middle of the image); 40 dB
+    gain limit of the inverse-Q filter (threshold 100)."""
+    sxg = X0 + 366.0 + 731.0 * np.arange(14)
+    syg = Y0 + 205.0 + 410.0 * np.arange(25)
+    shots = np.array([(x, y) for y in syg for x in sxg])
+    r1 = 51.2 + 102.4 * np.arange(100)
+    receivers = np.array([(X0 + x, Y0 + y) for y in r1 for x in r1])
+    diff = np.array([[X0 + 5120.0, Y0 + 5120.0, 2500.0],
+                     [X0 + 3000.0, Y0 + 5120.0, 3500.0],
+                     [X0 + 7000.0, Y0 + 4500.0, 4500.0]])
+    return Survey("c5", 1024, 1024, 600, 10.0, 10.0, 10.0, 3000, 0.002, 1800.0, 0.5,
+                  100.0, 25.0, shots, receivers, 3000.0, diff, 20.0, seed=seed,
+                  q_model=("cloud", X0 + 5120.0, Y0 + 5120.0, 1500.0, 800.0, 20.0),
+                  threshold=100.0)
+
+
 def traveltime(sv: Survey, r, z):
     """Linear-gradient traveltime from the surface (z=0)."""
     r = np.asarray(r, np.float64)
@@ -112,13 +171,62 @@ def ricker_spectrum(f, fpeak):
 def trace_geometry(sv: Survey, shot_ids=None):
     """(sx, sy, gx, gy) as SU integers (scalco units) for the given shots."""
     shot_ids = np.arange(len(sv.shots)) if shot_ids is None else np.asarray(shot_ids)
-    s = sv.shots[shot_ids]
-    nr = len(sv.receivers)
-    sxy = np.repeat(s, nr, axis=0)
-    gxy = np.tile(sv.receivers, (len(shot_ids), 1))
+    rec = [sv.receivers_of(int(i)) for i in shot_ids]
+    sxy = np.concatenate([np.repeat(sv.shots[i][None], len(r), axis=0)
+                          for i, r in zip(shot_ids, rec)]) if len(rec) else np.zeros((0, 2))
+    gxy = np.concatenate(rec) if len(rec) else np.zeros((0, 2))
     scale = 1.0 / sv.scaled
     to_i = lambda a: np.rint(a * scale).astype(np.int64).astype(np.int32)
     return to_i(sxy[:, 0]), to_i(sxy[:, 1]), to_i(gxy[:, 0]), to_i(gxy[:, 1])
+
+
+def vertical_time(sv: Survey, z):
+    """One-way vertical time to depth z in v(z) = v0 + k z."""
+    z = np.asarray(z, np.float64)
+    return np.log1p(sv.k * z / sv.v0) / sv.k if sv.k > 1e-9 else z / sv.v0
+
+
+def tstar(sv: Survey, px, py, x, y, z, t):
+    """t* of the straight path from the surface point (px, py, 0) to (x, y, z)
+    with traveltime t (absolute coordinates, m).
+
+    Constant Q: t / q.  Layers: t times the vertical-time average of 1/Q over
+    [0, z] (Q linear between the model's nodes; the integral by 64-point
+    midpoint rule).  Cloud: t / q plus (1/q_cloud - 1/q) times the time spent
+    inside the sphere, the chord length over v at the sphere's centre."""
+    t = np.asarray(t, np.float64)
+    if sv.q_model is None:
+        return t / sv.q
+    kind = sv.q_model[0]
+    if kind == "layers":
+        zn, qn = np.asarray(sv.q_model[1], float), np.asarray(sv.q_model[2], float)
+        z = np.asarray(z, np.float64)
+        zu, inv = np.unique(z, return_inverse=True)  # the ratio depends on z only
+        u = (np.arange(64) + 0.5) / 64.0
+        zz = zu[:, None] * u
+        w = 1.0 / (sv.v0 + sv.k * zz)
+        num = (w / np.interp(zz, zn, qn)).sum(-1)
+        den = w.sum(-1)
+        ratio = np.where(zu > 0, num / np.maximum(den, 1e-30), 1.0 / np.interp(0.0, zn, qn))
+        return t * ratio[inv].reshape(z.shape)
+    _, cx, cy, cz, rad, qc = sv.q_model
+    a = np.stack(np.broadcast_arrays(np.asarray(px, float), np.asarray(py, float),
+                                     np.zeros_like(np.asarray(px, float))), -1)
+    b = np.stack(np.broadcast_arrays(np.asarray(x, float), np.asarray(y, float),
+                                     np.asarray(z, float)), -1)
+    d = b - a
+    L = np.linalg.norm(d, axis=-1)
+    c = np.array([cx, cy, cz])
+    # chord of the segment a + s d (s in [0, 1]) inside the sphere
+    dd = np.maximum((d * d).sum(-1), 1e-30)
+    s0 = ((c - a) * d).sum(-1) / dd
+    m = a + s0[..., None] * d
+    h2 = rad * rad - ((m - c) ** 2).sum(-1)
+    half = np.sqrt(np.maximum(h2, 0.0) / dd)
+    s1, s2 = np.clip(s0 - half, 0.0, 1.0), np.clip(s0 + half, 0.0, 1.0)
+    chord = np.where(h2 > 0, (s2 - s1) * L, 0.0)
+    tin = chord / (sv.v0 + sv.k * cz)
+    return t / sv.q + tin * (1.0 / qc - 1.0 / sv.q)
 
 
 def make_traces(sv: Survey, shot_ids=None, noise: bool = True) -> np.ndarray:
@@ -126,10 +234,21 @@ def make_traces(sv: Survey, shot_ids=None, noise: bool = True) -> np.ndarray:
 
     Events: the flat reflector (reflection time through the midpoint at the
     reflector depth) and the point diffractors.  Each event is the Ricker
-    spectrum delayed by its traveltime, attenuated by exp(-pi f t*) with
-    t* = t / Q and phase-shifted by the Kjartansson dispersion term
+    spectrum delayed by its traveltime, attenuated by exp(-pi f t*) with t*
+    of the survey's Q model summed over the two legs (`tstar`) and
+    phase-shifted by the Kjartansson dispersion term
     exp(+2 i f t* ln(f / fpeak)).  Gaussian noise at snr_db (seeded)."""
     sx, sy, gx, gy = (a.astype(np.float64) * sv.scaled for a in trace_geometry(sv, shot_ids))
+    return pair_traces(sv, np.stack([sx, sy], 1), np.stack([gx, gy], 1), noise)
+
+
+def pair_traces(sv: Survey, spos: np.ndarray, gpos: np.ndarray,
+                noise: bool = True) -> np.ndarray:
+    """Trace samples [ntr, ntl] float32 of the (source, receiver) position
+    pairs spos[i], gpos[i] (absolute x, y in m), as make_traces synthesises
+    them."""
+    sx, sy = spos[:, 0].astype(np.float64), spos[:, 1].astype(np.float64)
+    gx, gy = gpos[:, 0].astype(np.float64), gpos[:, 1].astype(np.float64)
     ntr = sx.size
     n = sv.ntl
     nf = n // 2 + 1
@@ -138,25 +257,30 @@ def make_traces(sv: Survey, shot_ids=None, noise: bool = True) -> np.ndarray:
     W = ricker_spectrum(f, sv.fpeak)
     times = []
     amps = []
+    qstar = []
     mx, my = 0.5 * (sx + gx), 0.5 * (sy + gy)
     h = 0.5 * np.hypot(gx - sx, gy - sy)
-    times.append(2.0 * traveltime(sv, h, sv.reflector_z))
+    tr1 = traveltime(sv, h, sv.reflector_z)
+    times.append(2.0 * tr1)
     amps.append(np.full(ntr, 1.0))
+    qstar.append(tstar(sv, sx, sy, mx, my, sv.reflector_z, tr1)
+                 + tstar(sv, gx, gy, mx, my, sv.reflector_z, tr1))
     for (dx, dy, dz) in sv.diffractors:
         ts = traveltime(sv, np.hypot(sx - dx, sy - dy), dz)
         tg = traveltime(sv, np.hypot(gx - dx, gy - dy), dz)
         times.append(ts + tg)
         amps.append(np.full(ntr, 0.5))
+        qstar.append(tstar(sv, sx, sy, dx, dy, dz, ts) + tstar(sv, gx, gy, dx, dy, dz, tg))
     out = np.zeros((ntr, n), np.float32)
     chunk = 4096
     for c0 in range(0, ntr, chunk):
         c1 = min(ntr, c0 + chunk)
         spec = np.zeros((c1 - c0, nf), np.complex128)
-        for t, a in zip(times, amps):
+        for t, a, q in zip(times, amps, qstar):
             tt = t[c0:c1, None]
-            tstar = tt / sv.q
-            spec += (a[c0:c1, None] * W[None, :] * np.exp(-np.pi * f * tstar)
-                     * np.exp(2j * fpos * tstar * np.log(fpos / sv.fpeak))
+            ts_ = q[c0:c1, None]
+            spec += (a[c0:c1, None] * W[None, :] * np.exp(-np.pi * f * ts_)
+                     * np.exp(2j * fpos * ts_ * np.log(fpos / sv.fpeak))
                      * np.exp(-2j * np.pi * f * tt))
         tr = np.fft.irfft(spec, n=n, axis=1) / sv.dt
         if noise:
@@ -225,3 +349,53 @@ def config2_model(h: float = 40.0, seed: int = 0, anomalies: bool = True,
             iq[Z >= ztop] = 1.0 / qv
     return GridModel(v.astype(np.float32), iq.astype(np.float32), h, float(xs[0]),
                      float(ys[0]), v0, kz)
+
+
+# ---------------------------------------------------------------------------
+# seeded accuracy samples of every configuration
+# ---------------------------------------------------------------------------
+SAMPLES = {
+    # name: (survey, line, shots near the line, dtstar (s), aperture half-width
+    # (m) or None for a seeded value in [1, 4] km, table half-widths (m))
+    "c1": (config1, 64, 4, 0.0015, 400.0, (900.0, 900.0)),
+    "c3": (config3, 384, 3, 0.0025, None, (2500.0, 1500.0)),
+    "c5": (config5, 512, 2, 0.005, 2000.0, (2500.0, 1500.0)),
+}
+
+
+def accuracy_sample(name: str, ntr: int = 1200, seed: int = 7) -> dict:
+    """A seeded sample of a configuration for image accuracy against the FP64
+    oracle: `ntr` traces drawn from the shots nearest to one image line (their
+    gathers as the configuration records them), the line's analytic tables
+    (depth and surface nodes every 160 m; t* from the configuration's Q model)
+    and the aperture tables.  Configuration 2's sample is the benchmark's own
+    (two of its step's gathers)."""
+    from . import tables as T
+    from .engine import encode_su
+    make, line, nsh, dtstar, ap, (hx, hy) = SAMPLES[name]
+    sv = make(seed)
+    rng = np.random.default_rng([seed, 11])
+    if ap is None:
+        ap = float(rng.uniform(1000.0, 4000.0))
+    ly = sv.line_y(line)
+    near = np.argsort(np.abs(sv.shots[:, 1] - ly) + 1e-3 * np.abs(sv.shots[:, 0] - X0
+                                                                   - 0.5 * sv.nxi * sv.dxi),
+                      kind="stable")[:nsh]
+    sx, sy, gx, gy = trace_geometry(sv, near)
+    pick = np.sort(rng.choice(sx.size, min(ntr, sx.size), replace=False))
+    spos = np.stack([sx[pick], sy[pick]], 1).astype(np.float64) * sv.scaled
+    gpos = np.stack([gx[pick], gy[pick]], 1).astype(np.float64) * sv.scaled
+    traces = pair_traces(sv, spos, gpos)
+    hdr = np.stack([sx[pick], sy[pick], gx[pick], gy[pick]], 1).astype(np.int32)
+    rec = encode_su(hdr[:, 0], hdr[:, 1], hdr[:, 2], hdr[:, 3], traces,
+                    dt_us=int(round(sv.dt * 1e6)), scalco=sv.scalco)
+    sub_n = 16  # 160 m nodes
+    tab = T.linear_gradient_tables(sv, fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi,
+                                   zmax=(sv.nzi - 1) * sv.dzi, sub=sub_n, nxi1=16,
+                                   half_x=hx, half_y=hy, line_y=ly)
+    half_cdps, half_lines = int(round(ap / sv.dxi)), int(round(0.5 * ap / sv.dyi))
+    return dict(name=name, sv=sv, line=line, cyi=ly, hdr=hdr, traces=traces, records=rec,
+                tab=tab, az=aperture_tables(half_cdps, half_lines), dtstar=dtstar,
+                aperture_m=ap,
+                describe=f"{len(pick)} seeded traces of the {nsh} shot gathers nearest to "
+                         f"line {line} of configuration {name[1:]}, aperture +-{ap:.0f} m")

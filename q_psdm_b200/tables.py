@@ -108,16 +108,23 @@ def build_line_tables(time_fn, tstar_fn, *, fci: int, nxi: int, dxi: float, zmax
 
 def linear_gradient_tables(sv, *, fci: int, nxi: int, dxi: float, zmax: float,
                            sub: int = 4, nxi1: int = 16, half_x: float = 900.0,
-                           half_y: float = 900.0) -> LineTables:
-    """Analytic v(z) = v0 + k z tables (constant Q: t* = t / Q), subsampled
-    `sub` times in depth and surface position relative to the 10 m grid."""
-    from .synth import traveltime
+                           half_y: float = 900.0, line_y: float | None = None) -> LineTables:
+    """Analytic v(z) = v0 + k z tables, subsampled `sub` times in depth and
+    surface position relative to the 10 m grid; t* of the survey's Q model
+    along the straight path (`synth.tstar`: t / Q for constant Q).  line_y:
+    absolute y of the line (needed by a Q model that is not layered)."""
+    from .synth import traveltime, tstar
 
     def tfn(px, py, x, z):
         return traveltime(sv, np.hypot(px - x, py), z)
 
+    ly = sv.fyv if line_y is None else line_y
+
     def qfn(px, py, x, z):
-        return traveltime(sv, np.hypot(px - x, py), z) / sv.q
+        t = traveltime(sv, np.hypot(px - x, py), z)
+        if sv.q_model is None:
+            return t / sv.q
+        return tstar(sv, sv.fxv + px, ly + py, sv.fxv + x, ly, z, t)
 
     dzii = sub * sv.dzi
     nnodes = int(np.floor(zmax / dzii)) + 2
