@@ -1216,8 +1216,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
               const bool rok =
                   lookup_tq(pc, dt, ttt, dq, qqq, tqp, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
               const float dgx = gp.x - x;
-              const float dg = sqrtf(dgx * dgx + gp.y * gp.y + z2);
-              const float rdg = __fdividef(1.0f, dg);
+              const float rdg = rsqrtf(dgx * dgx + gp.y * gp.y + z2);  // 1 / dg
               agx = dgx * rdg, agy = gp.y * rdg, agz = z * rdg;
               // dip-test thresholds of this receiver (NaN: no table value,
               // every member fails)
