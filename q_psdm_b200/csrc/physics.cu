@@ -995,10 +995,12 @@ __device__ __forceinline__ UnitBounds unit_bounds(float px, float py, const Tile
   const float dxl = px - b.x1, dxh = px - b.x0;
   const float adxmin = (dxl <= 0.0f && dxh >= 0.0f) ? 0.0f : fminf(fabsf(dxl), fabsf(dxh));
   const float adxmax = fmaxf(fabsf(dxl), fabsf(dxh));
-  const float rmin = sqrtf(adxmin * adxmin + py * py + b.z0 * b.z0);
-  const float rmax = sqrtf(adxmax * adxmax + py * py + b.z1 * b.z1);
-  u.ok = rmin > 1e-3f;  // a point of the box (nearly) at the surface position: no bound
-  const float irmin = 1.0f / fmaxf(rmin, 1e-3f), irmax = 1.0f / rmax;
+  const float rmin2 = adxmin * adxmin + py * py + b.z0 * b.z0;
+  const float rmax2 = adxmax * adxmax + py * py + b.z1 * b.z1;
+  u.ok = rmin2 > 1e-6f;  // a point of the box (nearly) at the surface position: no bound
+  // 1/rmin, 1/rmax (approximate reciprocal square roots: ~1e-7 relative,
+  // far inside the test's margin)
+  const float irmin = rsqrtf(fmaxf(rmin2, 1e-6f)), irmax = rsqrtf(fmaxf(rmax2, 1e-6f));
   u.axl = dxl >= 0.0f ? dxl * irmax : dxl * irmin;
   u.axh = dxh >= 0.0f ? dxh * irmin : dxh * irmax;
   u.ayl = py >= 0.0f ? py * irmax : py * irmin;
