@@ -99,8 +99,10 @@ typedef struct {
 /* Physics forms.  PLAIN: one pass per trace in submission order with table
  * lookups per point-trace (source terms reused while consecutive traces share
  * a source).  BATCHED: traces of a batch grouped by receiver position and
- * source; source terms built once per shot and image tile, receiver terms
- * once per receiver position, a persistent kernel over image tiles; t*
+ * source; a persistent kernel over image tiles builds the source terms once
+ * per shot and tile, drops for the tile every trace whose dip test fails at
+ * all its points (a conservative bound; the image and point-trace counts
+ * are unchanged), and computes receiver terms once per receiver position; t*
  * panels computed once per trace and shared by every line of a brick
  * (qpsdm_set_lines).  FP16 panels are scaled per trace by a power of two
  * from a bound on the trace's filtered amplitude, so any data amplitude

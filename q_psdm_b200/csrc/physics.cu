@@ -22,7 +22,6 @@
 #include <math.h>
 
 #include <algorithm>
-#include <climits>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -73,7 +72,6 @@ struct PhysicsState {
   int *d_srcflag = nullptr, *d_sid = nullptr;  // source run flags / ids (1-based)
   float2 *d_srcpos = nullptr;                  // [max_batch] source positions
   int4 *d_mem = nullptr;                       // [max_batch] member info
-  int4 *d_grp = nullptr;                       // [max_batch] group records
   float2 *d_grppos = nullptr;                  // [max_batch] receiver positions
   int *d_memgrp = nullptr;                     // [max_batch] group of each sorted member
   int *d_tile_ctr = nullptr;
@@ -200,7 +198,6 @@ void physics_destroy(PhysicsState *s) {
   cudaFree(s->d_sid);
   cudaFree(s->d_srcpos);
   cudaFree(s->d_mem);
-  cudaFree(s->d_grp);
   cudaFree(s->d_grppos);
   cudaFree(s->d_memgrp);
   cudaFree(s->d_tile_ctr);
@@ -891,33 +888,13 @@ __global__ void k_batch_keys(const uint8_t *__restrict__ rec, int rec_bytes, int
   val[i] = i;
 }
 
-// Group records: [2g] = (first sorted position, end, min ixi1, max ixi2),
-// [2g+1] = (min source, max source); receiver position per group.
+// Receiver position of every receiver group (run of equal keys).
 __global__ void k_batch_groups(const unsigned long long *__restrict__ ukey,
-                               const int *__restrict__ count, const int *__restrict__ off,
-                               const int *__restrict__ nruns, const int *__restrict__ sval,
-                               const int *__restrict__ ints, const int *__restrict__ sid,
-                               int4 *__restrict__ grp, float2 *__restrict__ grppos, int ntr) {
+                               const int *__restrict__ nruns, float2 *__restrict__ grppos,
+                               int ntr) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ntr || g >= *nruns) return;
-  const unsigned long long k = ukey[g];
-  const int start = off[g], n = count[g];
-  if (k == kNoKey) {
-    grp[2 * g] = make_int4(start, start, 1, 0);
-    grp[2 * g + 1] = make_int4(1, 0, 0, 0);
-    return;
-  }
-  int c0 = INT_MAX, c1 = INT_MIN, s0 = INT_MAX, s1 = INT_MIN;
-  for (int p = start; p < start + n; ++p) {
-    const int j = sval[p];
-    c0 = min(c0, ints[(size_t)j * kGateInts + 4]);
-    c1 = max(c1, ints[(size_t)j * kGateInts + 5]);
-    const int sj = sid[j] - 1;
-    s0 = min(s0, sj);
-    s1 = max(s1, sj);
-  }
-  grp[2 * g] = make_int4(start, start + n, c0, c1);
-  grp[2 * g + 1] = make_int4(s0, s1, 0, 0);
+  const unsigned long long k = ukey[g];  // rejected traces (kNoKey) are never imaged
   grppos[g] = make_float2(__uint_as_float((unsigned)(k & 0xffffffffu)),
                           __uint_as_float((unsigned)(k >> 32)));
 }
@@ -1363,7 +1340,6 @@ static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p) {
   ok &= cudaMalloc(&s->d_sid, sizeof(int) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_srcpos, sizeof(float2) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_mem, sizeof(int4) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_grp, sizeof(int4) * 2 * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_grppos, sizeof(float2) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_memgrp, sizeof(int) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_tile_ctr, sizeof(int)) == cudaSuccess;
@@ -1546,8 +1522,7 @@ static int batched_group(PhysicsState *s, const qpsdm_static_params &p, const Li
   tb = s->cub_bytes;
   if (cub::DeviceScan::ExclusiveSum(s->d_cub, tb, s->d_count, s->d_off, n, st) != cudaSuccess)
     return QPSDM_ECUDA;
-  k_batch_groups<<<grd, blk, 0, st>>>(s->d_ukey, s->d_count, s->d_off, s->d_nruns, s->d_val[1],
-                                      v.ints, s->d_sid, s->d_grp, s->d_grppos, n);
+  k_batch_groups<<<grd, blk, 0, st>>>(s->d_ukey, s->d_nruns, s->d_grppos, n);
   k_batch_memgrp<<<grd, blk, 0, st>>>(s->d_off, s->d_nruns, s->d_memgrp, n);
   k_batch_members<<<grd, blk, 0, st>>>(b.d_rec, b.rec_bytes, b.big_endian, n, s->d_val[1],
                                        v.ints, s->d_sid, s->d_srcflag, p.scaled, l.fxi, l.cyi,
