@@ -145,7 +145,7 @@ class Workload:
                 nxi1=16, half_x=2500.0, half_y=1200.0)
         return self._tab
 
-    def static(self, form: str, max_batch: int):
+    def static(self, form: str, max_batch: int, use_graph: int = 0):
         from q_psdm_b200 import engine as E
         sv = self.sv
         _, _, dtype, pform = FORMS[form]
@@ -157,7 +157,8 @@ class Workload:
             return E.static_params(**kw)
         return E.static_params(**kw, mode=1, panel_dtype=dtype, nbins=16, dtstar=0.002,
                                form=pform, dzii=self.tables().dzii, tile_z=tz, tile_x=tx,
-                               variant=self.variant if form == "batched" else 0)
+                               variant=self.variant if form == "batched" else 0,
+                               use_graph=use_graph)
 
     def lines(self, form: str, contract_rad: float):
         sv = self.sv
@@ -263,13 +264,52 @@ def fp32_peak_tflops(torch):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def _kernel_times(eng, _lib):
+    return {name: eng.kernel_time(c) for name, c in
+            (("gate", _lib.K_GATE), ("panels", _lib.K_PRE), ("image", _lib.K_IMAGE),
+             ("grouping", _lib.K_OTHER))}
+
+
+def _eager_kernel_times(form, wl, dev, stream, drecs, ntr, flush, nsteps=2):
+    """Per-kernel CUDA-event times of `nsteps` steps of a second engine that
+    runs the batches eagerly (an engine replaying CUDA graphs records no
+    events inside them): the per-kernel breakdown and the image kernel's time
+    per launch of a graph-timed run."""
+    from q_psdm_b200 import _lib
+    from q_psdm_b200 import engine as E
+    import torch
+    ns = FORMS[form][0]
+    p = wl.static(form, max_batch=ns * wl.ntr_shot)
+    eng = E.Engine(p, device=dev)
+    try:
+        eng.set_stream(stream.cuda_stream)
+        eng.set_lines(wl.lines(form, p.contract))
+        az = wl.aperture()
+        eng.begin_offset(E.offset_params(p, 0, p.nxi, aznx1=az[0], aznx2=az[1], azny1=az[2],
+                                         azny2=az[3]))
+        eng.submit_device(drecs[0].data_ptr(), ntr)
+        torch.cuda.synchronize()
+        eng.profile(True)
+        for k in range(nsteps):
+            flush.zero_()
+            eng.submit_device(drecs[k % len(drecs)].data_ptr(), ntr)
+        torch.cuda.synchronize()
+        kt = _kernel_times(eng, _lib)
+        eng.profile(False)
+    finally:
+        eng.close()
+    return kt, nsteps
+
+
 def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True):
     import torch
     from q_psdm_b200 import _lib
     from q_psdm_b200 import engine as E
 
     ns, nl, _, _ = FORMS[form]
-    p = wl.static(form, max_batch=ns * wl.ntr_shot)
+    # the batched form replays each batch from a captured CUDA graph
+    graph = form == "batched"
+    p = wl.static(form, max_batch=ns * wl.ntr_shot, use_graph=int(graph))
     eng = E.Engine(p, device=dev)
     stream = torch.cuda.Stream()  # non-default: its handle is never 0
     torch.cuda.set_stream(stream)
@@ -308,10 +348,14 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     ms = sum(a.elapsed_time(b) for a, b in ev)
     _, npt1 = eng.counters()
     npt = npt1 - npt0
-    kt = {name: eng.kernel_time(c) for name, c in
-          (("gate", _lib.K_GATE), ("panels", _lib.K_PRE), ("image", _lib.K_IMAGE),
-           ("grouping", _lib.K_OTHER))}
+    kt = _kernel_times(eng, _lib)  # launch counts (graph replays included)
     eng.profile(False)
+    kms = {k: v[0] / steps for k, v in kt.items()}
+    img_launch = kt["image"][0] / max(kt["image"][1], 1)
+    if graph:  # kernel times from eager steps of the same batches
+        kte, nst = _eager_kernel_times(form, wl, dev, stream, drecs, ntr, flush)
+        kms = {k: v[0] / nst for k, v in kte.items()}
+        img_launch = kte["image"][0] / max(kte["image"][1], 1)
     t = torch.tensor([ms, float(npt)], dtype=torch.float64, device="cuda")
     if dist:
         tm, tn = t[0:1].clone(), t[1:2].clone()
@@ -322,9 +366,9 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
         ms_max, npt_all = ms, float(npt)
     out = {"value": npt_all / (ms_max * 1e-3) / 1e9, "ms_per_step": ms_max / steps,
            "point_traces_per_step": npt_all / steps, "clocks": ck,
-           "kernel_ms_per_step": {k: v[0] / steps for k, v in kt.items()},
+           "kernel_ms_per_step": kms,
            "launches": int(sum(v[1] for v in kt.values())),
-           "image_ms_per_launch": kt["image"][0] / max(kt["image"][1], 1),
+           "image_ms_per_launch": img_launch,
            "image_launches": kt["image"][1], "npt": npt}
     if form == "batched":
         tu = eng.tuning()
@@ -417,6 +461,9 @@ def run_ours(args, rank, world, dist):
            "kernel_ms_per_step": head["kernel_ms_per_step"], "forms": forms}
     if "tuning" in head:
         res["config"]["autotuned"] = head["tuning"]
+    if args.form == "batched":
+        res["config"]["cuda_graph"] = ("each batch replayed from a captured CUDA graph (captured "
+                                       "in the warm-up steps); per-kernel times from eager steps")
     return res, wl
 
 
