@@ -941,12 +941,15 @@ __global__ void k_batch_members(const uint8_t *__restrict__ rec, int rec_bytes, 
 }
 
 // Source terms kept per (source, point) in shared memory, as four float2
-// planes [plane][source][point]: (T, t*), (CS = ds^3 / ts, AZ), (PX1, PX2),
-// (PY1, PY2), with A the unit vector from the point to the source and
+// planes [plane][source][point]: (T, t* / dtstar), (CS = ds^3 / ts, AZ),
+// (PX1, PX2), (PY1, PY2), with A the unit vector from the point to the source
+// and
 //   PX1 = AX - tanx1c AZ, PX2 = tanx2c AZ - AX   (PY likewise with tany)
 // so that the dip test of a (source, receiver) pair needs no division: for
 // uz = AZ + AZg > 0, tanx1c < ux / uz < tanx2c is PX1 > tanx1c AZg - AXg and
 // PX2 > AXg - tanx2c AZg (the receiver's thresholds, once per receiver).
+// The differences PX1 - (tanx1c AZg - AXg) etc. are the pair's dip-test
+// functions, which also give the dip taper.
 enum { kMapTQ = 0, kMapCZ, kMapPX, kMapPY, kMapN };
 
 // Tile-level dip test.  A member (source S, receiver G) contributes to an
