@@ -243,7 +243,9 @@ int qpsdm_profile_get(qpsdm_engine *e, int kernel_class, double *total_ms,
 int qpsdm_tuning_info(qpsdm_engine *e, int *variant, int *tile_z, int *tile_x,
                       int *min_blocks, float *ms, int nms);
 
-/* Counters since begin_offset: traces accepted by the gate and point-traces
+/* Counters since begin_offset: traces accepted by the gate (summed over the
+ * lines of the brick: a trace accepted by two lines counts twice; counted on
+ * the device, so batches replayed from CUDA graphs count too) and point-traces
  * evaluated (one per image point inside a trace's aperture). */
 int qpsdm_get_counters(qpsdm_engine *e, int64_t *traces_accepted,
                        int64_t *point_traces);

@@ -27,13 +27,20 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 
 
+def ref_src() -> str:
+    """Directory of the reference's sources: $QPSDM_REF_SRC, else the
+    checkout's usual place."""
+    return os.environ.get("QPSDM_REF_SRC", "/root/reference/src")
+
+
 def build(ref: bool | None = None) -> None:
     """Compile liboracle.so (and oracle/_ref when the reference is present)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+    src = ref_src()
     if ref is None:
-        ref = os.path.isdir("/root/reference/src")
+        ref = os.path.isdir(src)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "ref-gpu"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, f"REF={src}", "ref", "ref-gpu"], check=True)
 
 
 class GateParams(C.Structure):

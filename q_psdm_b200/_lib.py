@@ -133,6 +133,7 @@ SYMBOLS = [
     ("qpsdm_mlp_status", _I, [_P]),
 ]
 FFT_NOALLOC_MAX_N = 8192
+ETIMEOUT = 5
 ESIZE = 8
 
 _lib = None

@@ -19,11 +19,10 @@ namespace qpsdm {
 // ---------------------------------------------------------------------------
 // Gate: one thread per trace.
 // ---------------------------------------------------------------------------
-__global__ void k_gate(const uint8_t *__restrict__ rec, int rec_bytes, int ntr,
-                       int be, GateArgs g, int *__restrict__ ints,
-                       float *__restrict__ geom, unsigned *err) {
-  const int itr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (itr >= ntr) return;
+__device__ __forceinline__ bool gate_trace(const uint8_t *__restrict__ rec, int rec_bytes,
+                                           int itr, int be, const GateArgs &g,
+                                           int *__restrict__ ints, float *__restrict__ geom,
+                                           unsigned *err) {
   const uint8_t *r = rec + (size_t)itr * rec_bytes;
   int *o = ints + (size_t)itr * kGateInts;
   float *f = geom + (size_t)itr * kGateF;
@@ -39,7 +38,7 @@ __global__ void k_gate(const uint8_t *__restrict__ rec, int rec_bytes, int ntr,
   if (sx < g.fxv1 || sx > g.exv1 || gx < g.fxv1 || gx > g.exv1 ||
       sy < g.fyv1 || sy > g.eyv1 || gy < g.fyv1 || gy > g.eyv1) {
     o[0] = kRejBbox;
-    return;
+    return false;
   }
   const double ddx = __dsub_rn(gx, sx), ddy = __dsub_rn(gy, sy);
   const double offset = (double)__fsqrt_rn(
@@ -67,7 +66,7 @@ __global__ void k_gate(const uint8_t *__restrict__ rec, int rec_bytes, int ntr,
   const int ny1 = g.az[2][iaz], ny2 = g.az[3][iaz];
   if (cdpy > ny1 || cdpy < -ny2) {
     o[0] = kRejY;
-    return;
+    return false;
   }
   // Columns cdpx-nx1 .. cdpx+nx2-1 clipped to the block; every column starts
   // at depth 0 and columns exist only when nzi > 10 (src/q-psdm.cu:2155-2171).
@@ -77,7 +76,7 @@ __global__ void k_gate(const uint8_t *__restrict__ rec, int rec_bytes, int ntr,
   const int ntibeg = (g.nzi > 10 && last >= first) ? last - first + 1 : 0;
   if (ntibeg == 0) {
     o[0] = kRejCols;
-    return;
+    return false;
   }
   o[0] = kAccepted;
   o[4] = first;
@@ -88,14 +87,27 @@ __global__ void k_gate(const uint8_t *__restrict__ rec, int rec_bytes, int ntr,
   f[1] = __double2float_rn(__dsub_rn(sy, g.cyi));
   f[2] = __double2float_rn(__dsub_rn(gx, g.fxi));
   f[3] = __double2float_rn(__dsub_rn(gy, g.cyi));
+  return true;
+}
+
+__global__ void k_gate(const uint8_t *__restrict__ rec, int rec_bytes, int ntr,
+                       int be, GateArgs g, int *__restrict__ ints,
+                       float *__restrict__ geom, unsigned *err,
+                       unsigned long long *__restrict__ nacc) {
+  const int itr = blockIdx.x * blockDim.x + threadIdx.x;
+  // accepted traces of the block, one atomic per warp (graph replays count too)
+  const bool accepted = itr < ntr && gate_trace(rec, rec_bytes, itr, be, g, ints, geom, err);
+  const unsigned ballot = __ballot_sync(0xffffffffu, accepted);
+  if (nacc && (threadIdx.x & 31) == 0 && ballot)
+    atomicAdd(nacc, (unsigned long long)__popc(ballot));
 }
 
 int launch_gate(const uint8_t *d_rec, int rec_bytes, int ntr, int be,
                 const GateArgs &g, int *d_ints, float *d_geom, unsigned *d_err,
-                cudaStream_t s) {
+                unsigned long long *d_nacc, cudaStream_t s) {
   if (ntr <= 0) return QPSDM_OK;
   k_gate<<<(ntr + 127) / 128, 128, 0, s>>>(d_rec, rec_bytes, ntr, be, g, d_ints,
-                                           d_geom, d_err);
+                                           d_geom, d_err, d_nacc);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
 

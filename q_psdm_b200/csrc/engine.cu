@@ -48,6 +48,7 @@ struct qpsdm_engine {
   float *d_geom = nullptr;
   unsigned *d_err = nullptr;
   unsigned long long *d_npt = nullptr;
+  unsigned long long *d_nacc = nullptr;  // (trace, line) pairs the gate accepted
   // lines of the image brick
   bool line_set = false;
   std::vector<qpsdm_line_params> lines;
@@ -63,7 +64,6 @@ struct qpsdm_engine {
   size_t spec_cap = 0;
   float *d_img = nullptr;
   size_t img_cap = 0;
-  int64_t traces_accepted = 0;
   // physics state (physics.cu)
   PhysicsState *phys = nullptr;
   KernelProfiler prof;
@@ -189,6 +189,8 @@ extern "C" int qpsdm_engine_create(const qpsdm_static_params *p,
   CKC(cudaMemset(e->d_err, 0, sizeof(unsigned)));
   CKC(cudaMalloc(&e->d_npt, sizeof(unsigned long long)));
   CKC(cudaMemset(e->d_npt, 0, sizeof(unsigned long long)));
+  CKC(cudaMalloc(&e->d_nacc, sizeof(unsigned long long)));
+  CKC(cudaMemset(e->d_nacc, 0, sizeof(unsigned long long)));
   if (e->p.mode == QPSDM_MODE_PHYSICS) {
     int rc = physics_create(&e->phys, e->p, &e->err);
     if (rc) return bail(rc);
@@ -220,6 +222,7 @@ extern "C" int qpsdm_engine_destroy(qpsdm_engine *e) {
   cudaFree(e->d_geom);
   cudaFree(e->d_err);
   cudaFree(e->d_npt);
+  cudaFree(e->d_nacc);
   cudaFree(e->d_dips);
   cudaFree(e->d_omega);
   cudaFree(e->d_re);
@@ -301,6 +304,7 @@ extern "C" int qpsdm_begin_offset(qpsdm_engine *e, const qpsdm_offset_params *o)
   if (o->zero_image || realloc_img || !e->offset_set)
     CK(cudaMemsetAsync(e->d_img, 0, sizeof(float) * nimg, e->s_comp));
   CK(cudaMemsetAsync(e->d_npt, 0, sizeof(unsigned long long), e->s_comp));
+  CK(cudaMemsetAsync(e->d_nacc, 0, sizeof(unsigned long long), e->s_comp));
   if (e->p.mode == QPSDM_MODE_PHYSICS) {
     rc = physics_begin_offset(e->phys, e->p, *o, (int)e->lines.size(), e->s_comp, &e->err);
     if (rc) return rc;
@@ -308,7 +312,6 @@ extern "C" int qpsdm_begin_offset(qpsdm_engine *e, const qpsdm_offset_params *o)
   e->off = *o;
   clear_graphs(e);
   e->offset_set = true;
-  e->traces_accepted = 0;
   return QPSDM_OK;
 }
 
@@ -348,7 +351,7 @@ int process_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
     memcpy(g.az[3], e->off.azny2, sizeof(int) * QPSDM_NAZ);
     e->prof.begin(QPSDM_K_GATE, e->s_comp);
     int rc = launch_gate(d_rec, (int)e->rec_bytes, ntr, be, g, e->d_ints + il * ints_ls,
-                         e->d_geom + il * geom_ls, e->d_err, e->s_comp);
+                         e->d_geom + il * geom_ls, e->d_err, e->d_nacc, e->s_comp);
     e->prof.end(e->s_comp);
     if (rc) return fail(e, rc, "gate launch failed");
   }
@@ -598,10 +601,11 @@ extern "C" int qpsdm_get_counters(qpsdm_engine *e, int64_t *acc, int64_t *npt) {
   if (!e) return QPSDM_EINVAL;
   DeviceGuard g(e->device);
   CK(cudaStreamSynchronize(e->s_comp));
-  unsigned long long v = 0;
+  unsigned long long v = 0, na = 0;
   CK(cudaMemcpy(&v, e->d_npt, sizeof(v), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&na, e->d_nacc, sizeof(na), cudaMemcpyDeviceToHost));
   if (npt) *npt = (int64_t)v;
-  if (acc) *acc = e->traces_accepted;
+  if (acc) *acc = (int64_t)na;
   return QPSDM_OK;
 }
 

@@ -166,11 +166,13 @@ extern "C" int qpsdm_fft_c2r(const float *d_in, int n, int batch, float *d_out,
 // that loads the library holds until the process exits.
 //
 // The array is shared by every call on a device and keeps the last call's
-// twiddles; each call rewrites the part it uses before its kernel runs, so
-// nothing needs clearing.  Calls that overlap on the GPU (concurrent streams)
-// race on the array and must be serialised by the caller.  The first call on
-// a device looks up the array's device address (cudaGetSymbolAddress); make
-// that first call before any stream capture.
+// twiddles; each call first rewrites the part it uses with a small kernel on
+// its own stream (cos and sin of the angles in double precision, rounded once
+// to float), so nothing needs clearing and no host buffer is involved.  Calls
+// that overlap on the GPU (concurrent streams) race on the array and must be
+// serialised by the caller.  The first call on a device looks up the array's
+// device address (cudaGetSymbolAddress); make that first call before any
+// stream capture.
 // ---------------------------------------------------------------------------
 namespace qpsdm {
 
@@ -198,6 +200,17 @@ static int noalloc_twiddle_ptr(float2 **out) {
   return QPSDM_OK;
 }
 
+// Twiddles of length n = 2m into tw: exp(-2 pi i e / m) for e < m, then
+// exp(-2 pi i k / n) for k <= m (the layout of FftPlan's tw_m, tw_n).
+__global__ void k_noalloc_twiddles(float2 *__restrict__ tw, int m) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 2 * m + 1) return;
+  const double turns = i < m ? -2.0 * (double)i / (double)m : -(double)(i - m) / (double)m;
+  double sn, cs;
+  sincospi(turns, &sn, &cs);
+  tw[i] = make_float2((float)cs, (float)sn);
+}
+
 }  // namespace qpsdm
 
 extern "C" int qpsdm_fft_r2c_noalloc(const float *d_in, int n, int batch,
@@ -213,20 +226,9 @@ extern "C" int qpsdm_fft_r2c_noalloc(const float *d_in, int n, int batch,
   float2 *tw = nullptr;
   int rc = noalloc_twiddle_ptr(&tw);
   if (rc) return rc;
-  // the same double-precision twiddles, rounded once, that qpsdm_fft_r2c uses
-  static thread_local float2 h[QPSDM_FFT_NOALLOC_MAX_N + 1];
-  for (int e = 0; e < p.m; ++e) {
-    double a = -2.0 * M_PI * (double)e / (double)p.m;
-    h[e] = make_float2((float)std::cos(a), (float)std::sin(a));
-  }
-  for (int k = 0; k <= p.m; ++k) {
-    double a = -2.0 * M_PI * (double)k / (double)n;
-    h[p.m + k] = make_float2((float)std::cos(a), (float)std::sin(a));
-  }
-  // pageable source: returns once h has been staged, so h may be reused
-  if (cudaMemcpyAsync(tw, h, sizeof(float2) * (2 * (size_t)p.m + 1), cudaMemcpyHostToDevice,
-                      (cudaStream_t)stream) != cudaSuccess)
-    return QPSDM_ECUDA;
+  // this length's twiddles into the shared array, on the caller's stream
+  const int ntw = 2 * p.m + 1;
+  k_noalloc_twiddles<<<(ntw + 255) / 256, 256, 0, (cudaStream_t)stream>>>(tw, p.m);
   p.tw_m = tw;
   p.tw_n = tw + p.m;
   const size_t sm = fft_smem_bytes(p.m);

@@ -86,7 +86,7 @@ struct GateArgs {
 
 int launch_gate(const uint8_t *d_rec, int rec_bytes, int ntr, int big_endian,
                 const GateArgs &g, int *d_ints, float *d_geom,
-                unsigned *d_err, cudaStream_t s);
+                unsigned *d_err, unsigned long long *d_nacc, cudaStream_t s);
 
 // Two-window spectra of accepted traces (src/q-psdm.cu:2174-2219).
 struct SpectraArgs {

@@ -959,12 +959,15 @@ enum { kMapTQ = 0, kMapCZ, kMapPX, kMapPY, kMapN };
 // so it can be dropped for a whole image tile when an upper bound of one of
 // them over the tile is negative.  The bounds come from interval arithmetic
 // over the tile's box (x in [x0, x1], y = 0 on the line, z in [z0, z1]) and
-// the tile's ranges of the four dip limits; the margin 1e-4 covers the FP32
-// rounding of the per-point test, so no member that passes at some point of
-// the tile is dropped (the kernel's sums are unchanged).
+// the tile's ranges of the four dip limits; the margin 1e-4 max(1, |tan|)
+// (|tan| the largest dip-limit tangent of the tile: the test functions'
+// rounding grows with tan uz) covers the FP32 rounding of the per-point test,
+// so no member that passes at some point of the tile is dropped (the kernel's
+// sums are unchanged).
 struct TileBox {
   float x0, x1, z0, z1;
   float t1lo, t1hi, t2lo, t2hi, u1lo, u1hi, u2lo, u2hi;  // tanx1c, tanx2c, tany1c, tany2c
+  float margin;  // -1e-4 max(1, largest |tan| of the tile)
 };
 struct UnitBounds {
   float axl, axh, ayl, ayh, azl, azh;
@@ -1003,7 +1006,7 @@ __device__ __forceinline__ bool tile_keep(float2 sp, float2 gp, const TileBox &b
   const float fx2 = corner_max(b.t2lo, b.t2hi, uzl, uzh) - uxl;
   const float fy1 = uyh + corner_max(-b.u1hi, -b.u1lo, uzl, uzh);
   const float fy2 = corner_max(b.u2lo, b.u2hi, uzl, uzh) - uyl;
-  constexpr float m = -1e-4f;
+  const float m = b.margin;
   return !(fx1 < m || fx2 < m || fy1 < m || fy2 < m);  // NaN keeps the member
 }
 
@@ -1115,6 +1118,10 @@ __global__ void __launch_bounds__(TZ *TX, MB)
       }
       box.t1lo = r[0], box.t1hi = -r[1], box.t2lo = r[2], box.t2hi = -r[3];
       box.u1lo = r[4], box.u1hi = -r[5], box.u2lo = r[6], box.u2hi = -r[7];
+      float tmax = 1.0f;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) tmax = fmaxf(tmax, fabsf(r[k]));
+      box.margin = -1e-4f * tmax;
       const int ncol = min(TX, a.nxb - ixb0), nrow = min(TZ, a.nzi - iz0);
       box.x0 = (ixb0 + a.ixstart) * a.dxi;
       box.x1 = (ixb0 + a.ixstart + ncol - 1) * a.dxi;

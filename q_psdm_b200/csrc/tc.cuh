@@ -81,12 +81,13 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 }
 
 // Bounded wait for phase `parity` to complete: gives up after max_iter polls
-// or 2 s of wall time, whichever comes first; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t max_iter) {
+// or limit_ns of wall time, whichever comes first; returns false on timeout.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, uint32_t parity, uint32_t max_iter,
+                                              uint64_t limit_ns) {
   const uint32_t a = smem_u32(bar);
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 0; i < max_iter; ++i) {
-    if ((i & 1023u) == 1023u && globaltimer_ns() - t0 > 2000000000ull) return false;
+    if ((i & 1023u) == 1023u && globaltimer_ns() - t0 > limit_ns) return false;
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -98,6 +99,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
     if (done) return true;
   }
   return false;
+}
+// the kernels' waits: 2 s
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t max_iter) {
+  return mbar_wait_for(bar, parity, max_iter, 2000000000ull);
 }
 
 // --- MMA ---------------------------------------------------------------------

@@ -70,7 +70,47 @@ __global__ void __launch_bounds__(128) k_tc_gemm_test(const __nv_bfloat16 *__res
   if (warp == 0) tc::tmem_free(tmem, ncols);
 }
 
+// The failure path of the tensor-core kernels' bounded waits: a CTA holding
+// TMEM waits on an mbarrier that nothing will arrive on (no MMA is issued, so
+// nothing is in flight), gives up after limit_ns, records the timeout and
+// still frees its TMEM and returns normally -- the context stays usable.
+__global__ void __launch_bounds__(128) k_tc_wait_test(int *err, unsigned long long limit_ns) {
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) tc::tmem_alloc(&tslot, 32);
+  if (tid == 0) {
+    tc::mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tslot;
+  const bool ok = tc::mbar_wait_for(&bar, 0, 1u << 30, limit_ns);
+  if (!ok && lane == 0) atomicExch(err, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_free(tmem, 32);
+}
+
 }  // namespace qpsdm
+
+// Test entry: runs k_tc_wait_test with a limit of limit_us microseconds,
+// synchronises the stream and returns QPSDM_ETIMEOUT when the wait gave up.
+extern "C" int qpsdm_internal_tc_wait_timeout(int limit_us, int *d_err, void *stream) {
+  using namespace qpsdm;
+  if (!d_err || limit_us <= 0 || limit_us > 1000000) return QPSDM_EINVAL;
+  if (cudaMemsetAsync(d_err, 0, sizeof(int), (cudaStream_t)stream) != cudaSuccess)
+    return QPSDM_ECUDA;
+  k_tc_wait_test<<<1, 128, 0, (cudaStream_t)stream>>>(d_err, 1000ull * (unsigned)limit_us);
+  if (cudaGetLastError() != cudaSuccess) return QPSDM_ECUDA;
+  int h = 0;
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess ||
+      cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return QPSDM_ECUDA;
+  return h ? QPSDM_ETIMEOUT : QPSDM_OK;
+}
 
 extern "C" int qpsdm_internal_tc_gemm(const void *d_a, const void *d_b, float *d_out, int N,
                                       int K, int a_mn, int b_mn, int *d_err, void *stream) {

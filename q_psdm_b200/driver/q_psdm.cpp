@@ -34,6 +34,8 @@
 //                           within +-extxline of it)
 //   resume=1                skip the lines up to <offspath>/break_point.txt
 //   check=1                 resolve and print the parameters, image nothing
+//   check=2                 also load every line's tables and list the data files
+//                           (whole traces, trailing partial bytes), image nothing
 // Errors print a message and exit 1, as the reference does; the library
 // itself never exits.
 #include <cuda_runtime.h>
@@ -326,9 +328,17 @@ bool load_tables(const std::string &ttpath, bool q, int line, int line1, int lin
     t.nxg = g[1];
     t.nzi1 = g[2];
     t.nxi1 = g[3];
-    t.desc.resize((size_t)t.nxg * t.nzg);
-    ok = t.nxg > 0 && t.nzg > 0 &&
-         std::fread(t.desc.data(), sizeof(qpsdm_ttt_desc), t.desc.size(), fp) == t.desc.size();
+    // a header whose grid does not fit the file is an index size error
+    // before anything is allocated for it
+    struct stat st;
+    const long long ncell = (long long)t.nxg * t.nzg;
+    ok = t.nxg > 0 && t.nzg > 0 && t.nzi1 > 0 && t.nxi1 > 0 &&
+         fstat(fileno(fp), &st) == 0 &&
+         (long long)st.st_size >= 32 + ncell * (long long)sizeof(qpsdm_ttt_desc);
+    if (ok) {
+      t.desc.resize((size_t)ncell);
+      ok = std::fread(t.desc.data(), sizeof(qpsdm_ttt_desc), t.desc.size(), fp) == t.desc.size();
+    }
   }
   std::fclose(fp);
   if (!ok) die("travel time table or qfield index size error %s", idx.c_str());
@@ -421,7 +431,11 @@ class Producer {
       if (!fp) continue;  // a missing data line contributes nothing
       struct stat st;
       fstat(fileno(fp), &st);
+      // whole records only, as the reference's producer (src/q-psdm.cu:1909)
       long left = (long)(st.st_size / (long)rec_bytes_);
+      if (st.st_size % (long)rec_bytes_)
+        logf("Warn: %s ends in a partial trace (%ld bytes), ignored\n", f.c_str(),
+             (long)(st.st_size % (long)rec_bytes_));
       while (left > 0) {
         int b;
         {
@@ -675,8 +689,35 @@ int main(int argc, char **argv) {
                 (int)offmin[0].size(), offmin[0].empty() ? 0.0 : offmin[0][0],
                 offmax[0].empty() ? 0.0 : offmax[0][0], sp.nfft, sp.nffti);
     for (size_t i = 0; i < lines.size(); ++i) std::printf("%s%d", i ? "," : "", lines[i]);
-    std::printf("],\"mute_depth_off0\":%.6g}\n",
+    std::printf("],\"mute_depth_off0\":%.6g",
                 offmin[0].empty() ? 0.0 : (double)mute_depth(mute, offmin[0][0]));
+    if (check_only >= 2) {
+      // dry run of the inputs: every line's tables as a run loads them, and
+      // every data file the lines read (whole traces, trailing partial bytes)
+      std::printf(",\"tables\":[");
+      for (size_t i = 0; i < lines.size(); ++i) {
+        Tables tt, tq;
+        const bool ht = load_tables(ttpath, false, lines[i], line1, line2, tt);
+        const bool hq = ht && load_tables(ttpath, true, lines[i], line1, line2, tq);
+        std::printf("%s{\"line\":%d,\"ttt\":%lld,\"qqq\":%lld,\"nxg\":%d,\"nzg\":%d}",
+                    i ? "," : "", lines[i], ht ? (long long)tt.data.size() : -1LL,
+                    hq ? (long long)tq.data.size() : -1LL, tt.nxg, tt.nzg);
+      }
+      std::printf("],\"data\":[");
+      const size_t rb = kHdr + 4 * (size_t)ntl;
+      int nf = 0;
+      for (size_t k = 0; k < offmin[0].size(); ++k)
+        for (int l = line1; l <= line2; ++l) {
+          const std::string f = offspath + "/off" + std::to_string(k) + "/line" + std::to_string(l);
+          struct stat st;
+          if (stat(f.c_str(), &st) != 0) continue;
+          std::printf("%s{\"file\":\"%s\",\"traces\":%lld,\"partial_bytes\":%lld}",
+                      nf++ ? "," : "", f.c_str(), (long long)(st.st_size / (long long)rb),
+                      (long long)(st.st_size % (long long)rb));
+        }
+      std::printf("]");
+    }
+    std::printf("}\n");
     return 0;
   }
   int ngpu = 0;

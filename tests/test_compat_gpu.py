@@ -41,8 +41,10 @@ def test_image_bit_exact(cuda, case):
         assert img.shape == case["o_img"].shape
         assert np.array_equal(img, case["o_img"], equal_nan=True)
         assert np.isfinite(img).all()
-        _, npt = eng.counters()
+        nacc, npt = eng.counters()
         assert npt == case["o_npt"]
+        # traces the gate accepted, counted on the device
+        assert nacc == int((case["o_ints"][:, 0] == 3).sum())
     finally:
         eng.close()
 
@@ -64,8 +66,10 @@ def test_batching_preserves_bits(cuda):
     _, _, ref, _ = oracle_run(c)
     n = c["hdr"].shape[0]
     eng, img, *_ = engine_run(c, batches=[700, 1, 600, n - 1301], max_batch=1024)
+    nacc, _ = eng.counters()
     eng.close()
     assert np.array_equal(img, ref)
+    assert nacc == int((oracle_run(c)[0][:, 0] == 3).sum())
     # host path splitting a submit larger than max_batch
     eng, img2, *_ = engine_run(c, batches=[n], max_batch=500)
     eng.close()

@@ -114,14 +114,15 @@ def test_batched_many_shots_and_splits(cuda):
     assert nrmse(img, ref) <= 5e-5
 
 
-def _varied_dips(case, seed=5):
-    """The case with dip limits that change from point to point (random in
-    [-0.35, -0.05] and [0.05, 0.35]), so that a tile's dip ranges matter."""
+def _varied_dips(case, seed=5, lo_hi=(0.05, 0.35)):
+    """The case with dip limits that change from point to point (random
+    tangents in [-0.35, -0.05] and [0.05, 0.35] by default, [-3, -2] and
+    [2, 3] for steep limits), so that a tile's dip ranges matter."""
     c = dict(case)
     rng = np.random.default_rng(seed)
     n = case["dips"].shape[1]
-    lo = -rng.uniform(0.05, 0.35, size=(2, n)).astype(np.float32)
-    hi = rng.uniform(0.05, 0.35, size=(2, n)).astype(np.float32)
+    lo = -rng.uniform(*lo_hi, size=(2, n)).astype(np.float32)
+    hi = rng.uniform(*lo_hi, size=(2, n)).astype(np.float32)
     c["dips"] = np.stack([lo[0], hi[0], lo[1], hi[1]])
     return c
 
@@ -137,14 +138,17 @@ def _image(c, **kw):
     return img, npt
 
 
-@pytest.mark.parametrize("dips", ["reference", "varied"])
+@pytest.mark.parametrize("dips", ["reference", "varied", "steep"])
 def test_batched_pointwise_equals_plain(cuda, case, dips):
     """The batched kernel drops, per image tile, the members whose dip test
     fails at every point of the tile (a conservative bound).  With FP32
     panels its image must then equal the plain form's point by point up to
     the order of the FP32 sums, for every tile shape, with the same
-    point-trace count.  Varied dip limits also against the FP64 oracle."""
-    c = case if dips == "reference" else _varied_dips(case)
+    point-trace count.  Varied dip limits also against the FP64 oracle;
+    steep limits (tangents 2 to 3) exercise the bound's margin, which grows
+    with the tangent."""
+    c = {"reference": lambda: case, "varied": lambda: _varied_dips(case),
+         "steep": lambda: _varied_dips(case, seed=6, lo_hi=(2.0, 3.0))}[dips]()
     plain, n0 = _image(c, panel_dtype=0, form=0)
     amp = np.abs(plain).max()
     assert amp > 0
@@ -152,7 +156,7 @@ def test_batched_pointwise_equals_plain(cuda, case, dips):
         img, n = _image(c, panel_dtype=0, form=1, tile=tile)
         assert n == n0, tile
         assert np.abs(img - plain).max() <= 2e-5 * amp, tile
-    if dips == "varied":
+    if dips != "reference":
         ref, npt, _ = oracle_run(c)
         assert n0 == npt
         assert nrmse(plain, ref) <= 5e-5
@@ -220,7 +224,7 @@ def test_graph_replay_matches_eager(cuda):
     c = make_case(nshots=2, rstep=2)
     rec = records(c)
     half = rec.shape[0] // 2
-    imgs = []
+    imgs, counts = [], []
     for g in (0, 1):
         eng, p, o = engine(c, form=1, panel_dtype=1, use_graph=g, max_batch=half)
         try:
@@ -230,10 +234,15 @@ def test_graph_replay_matches_eager(cuda):
                     eng.submit(rec[:half])
                     eng.submit(rec[half:2 * half])
             imgs.append(eng.get_image(False))
-            _, npt = eng.counters()
+            counts.append(eng.counters())
         finally:
             eng.close()
     assert np.array_equal(imgs[0], imgs[1])
+    # both counters are kept on the device: replays count like eager batches
+    assert counts[0] == counts[1]
+    ints = oracle_run(c)[2]
+    acc = int((ints[:2 * half, 0] == 3).sum())
+    assert counts[0][0] == 3 * acc
 
 
 @pytest.mark.parametrize("form", [0, 1])

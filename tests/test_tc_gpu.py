@@ -40,3 +40,27 @@ def test_tc_gemm(cuda, N, K, a_mn, b_mn):
     got, ref = _run(a, b, a_mn, b_mn)
     # bf16 inputs are exact in the reference; only FP32 accumulation differs
     assert np.abs(got - ref).max() <= 1e-4 * np.abs(ref).max()
+
+
+def test_bounded_wait_times_out_and_context_survives(cuda):
+    """A tensor-core CTA waiting on an mbarrier that nothing arrives on (no
+    MMA issued, nothing in flight) gives up after its limit, frees its tensor
+    memory and returns: the entry point reports QPSDM_ETIMEOUT, and the next
+    normal tensor-core call on the same context succeeds."""
+    import time
+
+    import torch
+    L = _lib.lib()
+    f = L.qpsdm_internal_tc_wait_timeout
+    f.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    t0 = time.perf_counter()
+    assert f(2000, err.data_ptr(), None) == _lib.ETIMEOUT     # 2 ms limit
+    assert time.perf_counter() - t0 < 5.0
+    assert int(err.item()) == 1
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((128, 64)).astype(np.float32)
+    b = rng.standard_normal((64, 64)).astype(np.float32)
+    got, ref = _run(a, b, 0, 0)
+    assert np.abs(got - ref).max() <= 1e-3 * np.abs(ref).max()

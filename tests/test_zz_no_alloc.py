@@ -44,6 +44,44 @@ def test_noalloc_matches_allocating_entry_point(cuda):
         assert np.abs(got - want).max() <= tol, n
 
 
+def test_noalloc_allocates_nothing(cuda):
+    """Free device memory is unchanged around a first call at a new length
+    (after one earlier call has loaded the kernels and looked up the array)."""
+    import torch
+    L = _lib.lib()
+    x = torch.randn((4, 3080), device="cuda")
+    y = torch.empty((4, 3080 // 2 + 1, 2), dtype=torch.float32, device="cuda")
+    assert L.qpsdm_fft_r2c_noalloc(x.data_ptr(), 720, 4, y.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert L.qpsdm_fft_r2c_noalloc(x.data_ptr(), 3080, 4, y.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
+def test_noalloc_on_a_stream(cuda):
+    """Two calls in a row on a non-default stream, each checked against the
+    allocating entry point on the same stream."""
+    import torch
+    L = _lib.lib()
+    st = torch.cuda.Stream()
+    g = torch.Generator(device="cuda").manual_seed(9)
+    for n, batch in [(2002, 7), (6006, 2)]:
+        x = torch.randn((batch, n), device="cuda", generator=g)
+        want = torch.empty((batch, n // 2 + 1, 2), dtype=torch.float32, device="cuda")
+        got = torch.empty_like(want)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(st):
+            assert L.qpsdm_fft_r2c(x.data_ptr(), n, batch, want.data_ptr(), st.cuda_stream) == 0
+            assert L.qpsdm_fft_r2c_noalloc(x.data_ptr(), n, batch, got.data_ptr(),
+                                           st.cuda_stream) == 0
+        st.synchronize()
+        w, o = want.cpu().numpy(), got.cpu().numpy()
+        tol = 3e-7 * max(1.0, np.log2(n)) * np.abs(w).max()
+        assert np.abs(o - w).max() <= tol, n
+
+
 def test_noalloc_rejects_sizes_beyond_its_array(cuda):
     import torch
     L = _lib.lib()
