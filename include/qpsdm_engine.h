@@ -113,7 +113,9 @@ enum { QPSDM_FORM_PLAIN = 0, QPSDM_FORM_BATCHED = 1 };
  * (src/q-psdm.cu:149-179) and the line buffers of GPUParamsWithLine
  * (src/q-psdm.cu:195-213).  Replaces the per-line H2D block of qpsdm()
  * (src/q-psdm.cu:1463-1515) and get_ttt_all() (src/q-psdm.cu:2382-2622).
- * All pointers are host memory, copied during qpsdm_set_line. */
+ * All pointers are host memory, copied during qpsdm_set_line, except the
+ * table data ttt and qqq, which may also be memory of the engine's device
+ * (tables built on the GPU, e.g. by qpsdm_surrogate_tables). */
 typedef struct {
   double fxi, cyi;       /* x of the first image cdp, y of this line */
   const float *dipx1, *dipx2, *dipy1, *dipy2; /* [nxi][nzi] dip tangents */
@@ -280,11 +282,13 @@ typedef struct {
 /* Traveltime T and t* of nsrc surface sources on their local grids
  * (d_T, d_tstar: [nsrc][nz][ny][nx]).  d_src: nsrc x (sx, sy, ox, oy) floats,
  * source position and local-grid origin in model coordinates.  d_work:
- * 2 * nsrc * nx*ny*nz + 1 floats of scratch.  First-order Godunov upwind
- * updates relaxed until nothing changes (at most max_iter sweeps), the
- * analytic background held inside init_radius of the source.  The
+ * QPSDM_EIK_WORK_FLOATS(nsrc * nx*ny*nz) floats of scratch, 8-byte aligned.
+ * First-order Godunov upwind updates relaxed until nothing changes (at most
+ * max_iter sweeps), the analytic background held inside init_radius of the
+ * source; t* is transported in FP64 and stored as float.  The
  * generator of the L<line>.ttt / .qqq data read by get_ttt_all
  * (src/q-psdm.cu:2382-2627); no counterpart of its own in the reference. */
+#define QPSDM_EIK_WORK_FLOATS(n) (4 * (size_t)(n) + 4)
 int qpsdm_eikonal_solve(const float *d_vel, const float *d_invq,
                         const qpsdm_eik_model *model, const float *d_src, int nsrc,
                         const qpsdm_eik_grid *grid, float init_radius, int max_iter,
@@ -377,6 +381,74 @@ int qpsdm_mlp_forward(qpsdm_mlp *h, const float *d_x, int n, float *d_y,
 /* Synchronise; QPSDM_ETIMEOUT if a tensor-core wait gave up in any kernel
  * since the handle was created. */
 int qpsdm_mlp_status(qpsdm_mlp *h);
+
+/* ---- the surrogate and the tables ------------------------------------------
+ * Outputs of the network are corrections (ms) to the linear-gradient
+ * background: T = T_bg + y0 / 1000, t* = T_bg / q_ref + y1 / 1000, with T_bg
+ * the exact traveltime of v = v0 + kz z from the surface point.  Coordinates
+ * are model coordinates (x from the first image cdp, y of the eikonal model). */
+typedef struct {
+  float v0, kz;  /* background velocity law */
+  float q_ref;   /* background t* = T_bg / q_ref of the network's targets */
+  float q_bg;    /* constant Q of the background solves (d_T_bg, d_tstar_bg) */
+} qpsdm_sur_background;
+
+/* Training samples drawn from solved grids (qpsdm_eikonal_solve of ns
+ * sources, d_src as there): nsamples uniform (source, node) pairs from the
+ * hash of seed; d_x [n][5] = (sx, sy, x, y, z), d_t [n][2] = the corrections
+ * (ms) of T and t*.  With the background's own solves on the same grids
+ * (d_T_bg, d_tstar_bg, both or neither) the values are corrected as the
+ * tables are: T = T_bg + T - T_bgsolve, t* = t* (T_bg / q_bg) / t*_bgsolve.
+ * A set of sources x volume points is never materialised: each batch of
+ * sources yields its samples while its grids are on the device.  No
+ * counterpart in the reference (it reads precomputed tables). */
+int qpsdm_eikonal_samples(const float *d_T, const float *d_tstar, const float *d_T_bg,
+                          const float *d_tstar_bg, const qpsdm_eik_grid *grid,
+                          const float *d_src, int ns, const qpsdm_sur_background *bg,
+                          uint64_t seed, int nsamples, float *d_x, float *d_t, void *stream);
+
+/* One image line's tables as the surrogate sees them (reference layout,
+ * surface grid of a cell centred on its middle cdp and on the line). */
+typedef struct {
+  int nxg, nzg, nxi1, nzi1;
+  int tcdp1;       /* first table cdp relative to the first image cdp */
+  float dxi, dzii; /* cdp spacing, depth-node spacing (m) */
+  float line_y;    /* model y of the line */
+  float v0, kz, q_ref; /* the network's background */
+} qpsdm_sur_line;
+
+/* Background correction of a line's eikonal tables in place: with d_ttt_bg,
+ * d_qqq_bg the same line's tables from solves of the linear-gradient
+ * background (v0, kz of ln, constant Q = q_bg) on the same grids,
+ * T = T_bg + T - T_bgsolve and t* = t* (T_bg / q_bg) / t*_bgsolve, T_bg exact:
+ * the first-order scheme's systematic error cancels.  Synchronises. */
+int qpsdm_eikonal_correct(const qpsdm_sur_line *ln, const qpsdm_ttt_desc *desc, float *d_ttt,
+                          float *d_qqq, const float *d_ttt_bg, const float *d_qqq_bg,
+                          int64_t len, float q_bg, void *stream);
+
+/* The network's traveltime error (ms) against the line's tables at every
+ * surface node of every cell, the maximum over the node's points,
+ * max-accumulated into d_node_err (float per node, cells in descriptor
+ * order, nodes [iys][ixs]; clear it first: calls for several lines give the
+ * maximum over them).  desc: host descriptors; d_ttt: len floats (device).
+ * Synchronises the stream. */
+int qpsdm_surrogate_gate(qpsdm_mlp *net, const qpsdm_sur_line *ln, const qpsdm_ttt_desc *desc,
+                         const float *d_ttt, int64_t len, float *d_node_err, void *stream);
+
+/* Tables of the line on the surface grids of fine_desc (same cells as
+ * coarse_desc) from the network; in every coarse patch whose corner nodes
+ * the network missed by more than gate_ms (d_node_err as written by
+ * qpsdm_surrogate_gate) the fine values are the bilinear interpolation of
+ * the coarse tables instead (the plain method keeps the last word on the
+ * network's error).  gated_nodes (may be NULL): fine surface nodes of all
+ * cells that kept the tables.  Replaces, for this line, the table lookup the
+ * reference stages for its kernel (src/q-psdm.cu:2343-2357) with denser
+ * tables.  Synchronises the stream. */
+int qpsdm_surrogate_tables(qpsdm_mlp *net, const qpsdm_sur_line *ln,
+                           const qpsdm_ttt_desc *coarse_desc, const float *d_cttt,
+                           const float *d_cqqq, int64_t coarse_len, const float *d_node_err,
+                           float gate_ms, const qpsdm_ttt_desc *fine_desc, float *d_fttt,
+                           float *d_fqqq, int64_t fine_len, int64_t *gated_nodes, void *stream);
 
 #ifdef __cplusplus
 }

@@ -10,7 +10,8 @@
  * against this double-precision restatement of the method:
  *
  *   for every image point (x, z) of the block and every accepted trace whose
- *   column range holds x:
+ *   column range holds x and whose source and receiver both lie inside the
+ *   surface grid of the point's table cells (a point-trace):
  *     ts, t*s, tg, t*g  from the tables: cell (ixg, izg) of the point, the
  *                       cell's surface grid centred on the cell (bilinear in
  *                       surface position), linear between depth nodes
@@ -38,14 +39,30 @@ typedef struct {
   int nxg, nzg, nxi1, nzi1;
 } orc_phys_params;
 
+/* The surface-grid test of a lookup, in the engine's FP32 arithmetic (one
+ * rounding per operation, the fused multiply-add as fmaf), so that a pair is
+ * evaluated -- and counted -- exactly when the engine evaluates it:
+ * fx = fma(px - xc, 1/dxs, (nxs-1)/2) inside [0, nxs-1], fy likewise. */
+static int in_grid(const orc_desc *d, float px, float py, float xc) {
+  const float rdx = 1.0f / (float)d->dxs, rdy = 1.0f / (float)d->dys;
+  const float fx = fmaf(px - xc, rdx, 0.5f * (float)(d->nxs - 1));
+  const float fy = fmaf(py, rdy, 0.5f * (float)(d->nys - 1));
+  return fx >= 0.0f && fx <= (float)(d->nxs - 1) && fy >= 0.0f && fy <= (float)(d->nys - 1);
+}
+
 /* value at one depth node of one cell for surface point (px, py) */
-static int tab_node(const orc_desc *d, const float *tab, double px, double py,
-                    double xc, int ixl, int izl, int nxi1, int nzi1,
+static int tab_node(const orc_desc *d, const float *tab, float pxf, float pyf,
+                    float xcf, int ixl, int izl, int nxi1, int nzi1,
                     double *v) {
+  if (!in_grid(d, pxf, pyf, xcf)) return 0;
+  const double px = pxf, py = pyf, xc = xcf;
   int nxs = d->nxs, nys = d->nys;
   double fx = (px - xc) / d->dxs + 0.5 * (nxs - 1);
   double fy = py / d->dys + 0.5 * (nys - 1);
-  if (!(fx >= 0.0 && fx <= nxs - 1 && fy >= 0.0 && fy <= nys - 1)) return 0;
+  if (fx < 0.0) fx = 0.0;
+  if (fx > nxs - 1) fx = nxs - 1;
+  if (fy < 0.0) fy = 0.0;
+  if (fy > nys - 1) fy = nys - 1;
   int ix = (int)fx, iy = (int)fy;
   if (ix > nxs - 2) ix = nxs - 2 < 0 ? 0 : nxs - 2;
   if (iy > nys - 2) iy = nys - 2 < 0 ? 0 : nys - 2;
@@ -60,12 +77,13 @@ static int tab_node(const orc_desc *d, const float *tab, double px, double py,
 
 typedef struct {
   int ok, ixl, izlA, izlB;
-  double c2, xc;
+  double c2;
+  float xc; /* the cell's centre x in the engine's FP32 arithmetic */
   const orc_desc *tA, *tB, *qA, *qB;
 } cells_t;
 
 static int lookup(const cells_t *c, const float *ttt, const float *qqq, int nxi1,
-                  int nzi1, double px, double py, double *t, double *q) {
+                  int nzi1, float px, float py, double *t, double *q) {
   double ta, tb, qa, qb;
   if (!tab_node(c->tA, ttt, px, py, c->xc, c->ixl, c->izlA, nxi1, nzi1, &ta)) return 0;
   if (!tab_node(c->tB, ttt, px, py, c->xc, c->ixl, c->izlB, nxi1, nzi1, &tb)) return 0;
@@ -117,7 +135,8 @@ void orc_physics_image(const orc_phys_params *p, int ntr, const float *geom,
           c.tB = dt + ixg * p->nzg + izgB;
           c.qA = dq + ixg * p->nzg + izgA;
           c.qB = dq + ixg * p->nzg + izgB;
-          c.xc = (p->tcdp1 + ixg * p->nxi1 + 0.5 * (p->nxi1 - 1)) * p->dxi;
+          c.xc = ((float)(p->tcdp1 + ixg * p->nxi1) + 0.5f * (float)(p->nxi1 - 1)) *
+                 (float)p->dxi;
         }
       }
       if (!c.ok) continue;
@@ -125,12 +144,14 @@ void orc_physics_image(const orc_phys_params *p, int ntr, const float *geom,
       for (int itr = 0; itr < ntr; ++itr) {
         const int *q3 = ints3 + 3 * itr;
         if (ixi < q3[0] || ixi > q3[1] || izi < q3[2]) continue;
-        ++npt;
         const float *g = geom + 4 * itr;
         double sx = g[0], sy = g[1], gx = g[2], gy = g[3];
         double ts, qs, tg, qg;
-        if (!lookup(&c, ttt, qqq, p->nxi1, p->nzi1, sx, sy, &ts, &qs)) continue;
-        if (!lookup(&c, ttt, qqq, p->nxi1, p->nzi1, gx, gy, &tg, &qg)) continue;
+        /* a point-trace: inside the trace's aperture, with table values for
+         * both its source and its receiver (the pairs the kernel evaluates) */
+        if (!lookup(&c, ttt, qqq, p->nxi1, p->nzi1, g[0], g[1], &ts, &qs)) continue;
+        if (!lookup(&c, ttt, qqq, p->nxi1, p->nzi1, g[2], g[3], &tg, &qg)) continue;
+        ++npt;
         double dsx = sx - x, dgx = gx - x;
         double ds = sqrt(dsx * dsx + sy * sy + z * z);
         double dg = sqrt(dgx * dgx + gy * gy + z * z);

@@ -87,6 +87,17 @@ class EikFillGeom(C.Structure):
                 ("dzii", C.c_float), ("x_cdp1", C.c_float), ("line_y", C.c_float)]
 
 
+class SurBackground(C.Structure):
+    _fields_ = [("v0", C.c_float), ("kz", C.c_float), ("q_ref", C.c_float), ("q_bg", C.c_float)]
+
+
+class SurLine(C.Structure):
+    _fields_ = [("nxg", C.c_int), ("nzg", C.c_int), ("nxi1", C.c_int), ("nzi1", C.c_int),
+                ("tcdp1", C.c_int), ("dxi", C.c_float), ("dzii", C.c_float),
+                ("line_y", C.c_float), ("v0", C.c_float), ("kz", C.c_float),
+                ("q_ref", C.c_float)]
+
+
 # (name, restype, argtypes) of every symbol include/qpsdm_engine.h declares.
 _P, _I, _F, _V = C.c_void_p, C.c_int, C.c_float, C.c_void_p
 SYMBOLS = [
@@ -131,6 +142,12 @@ SYMBOLS = [
     ("qpsdm_mlp_train_step", _I, [_P, _P, _P, _I, _F, C.POINTER(C.c_float), _P]),
     ("qpsdm_mlp_forward", _I, [_P, _P, _I, _P, _P]),
     ("qpsdm_mlp_status", _I, [_P]),
+    ("qpsdm_eikonal_samples", _I, [_P, _P, _P, _P, C.POINTER(EikGrid), _P, _I,
+                                   C.POINTER(SurBackground), C.c_uint64, _I, _P, _P, _P]),
+    ("qpsdm_eikonal_correct", _I, [C.POINTER(SurLine), _P, _P, _P, _P, _P, C.c_int64, _F, _P]),
+    ("qpsdm_surrogate_gate", _I, [_P, C.POINTER(SurLine), _P, _P, C.c_int64, _P, _P]),
+    ("qpsdm_surrogate_tables", _I, [_P, C.POINTER(SurLine), _P, _P, _P, C.c_int64, _P, _F, _P,
+                                    _P, _P, C.c_int64, C.POINTER(C.c_int64), _P]),
 ]
 FFT_NOALLOC_MAX_N = 8192
 ETIMEOUT = 5

@@ -11,7 +11,9 @@
 // the linear-gradient analytic traveltime inside a radius around the source,
 // which is held fixed.  t* then follows from grad T . grad t* = 1/(v^2 Q)
 // with the same upwind neighbours:
-//   t*_i = (f_i + sum_d w_d t*_d) / sum_d w_d,  w_d = (T_i - T_d)/h^2.
+//   t*_i = (f_i + sum_d w_d t*_d) / sum_d w_d,  w_d = (T_i - T_d)/h^2,
+// accumulated in double precision (t* is a cumulative integral along the
+// ray; the float result is written once, at the end).
 #include <math.h>
 
 #include "common.cuh"
@@ -80,7 +82,7 @@ __global__ void k_eik_setup(const float *__restrict__ vel, const float *__restri
                             qpsdm_eik_model m, const float4 *__restrict__ src, int nsrc,
                             qpsdm_eik_grid g, float r0, float *__restrict__ F,
                             float *__restrict__ QF, float *__restrict__ T,
-                            float *__restrict__ TS) {
+                            double *__restrict__ TS) {
   const size_t n = (size_t)g.nx * g.ny * g.nz;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n * nsrc;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -94,10 +96,10 @@ __global__ void k_eik_setup(const float *__restrict__ vel, const float *__restri
       const float r = sqrtf((e.x - sp.x) * (e.x - sp.x) + (e.y - sp.y) * (e.y - sp.y));
       const float t = lin_grad_time(r, e.z, m.v0, m.kz);
       T[i] = t;
-      TS[i] = t * model_at(invq, m, sp.x, sp.y, 0.0f);  // near-surface Q along the path
+      TS[i] = (double)t * model_at(invq, m, sp.x, sp.y, 0.0f);  // near-surface Q on the path
     } else {
       T[i] = kInf;
-      TS[i] = 0.0f;
+      TS[i] = 0.0;
     }
   }
 }
@@ -142,19 +144,19 @@ __global__ void k_eik_relax(const float *__restrict__ F, float *__restrict__ T,
   if (ch) atomicOr(changed, 1u);
 }
 
-// One in-place relaxation of t* along the upwind directions of T.
+// One in-place relaxation of t* along the upwind directions of T (FP64).
 __global__ void k_tstar_relax(const float *__restrict__ T, const float *__restrict__ QF,
-                              float *__restrict__ TS, const float4 *__restrict__ src, int nsrc,
+                              double *__restrict__ TS, const float4 *__restrict__ src, int nsrc,
                               qpsdm_eik_grid g, float r0) {
   const size_t n = (size_t)g.nx * g.ny * g.nz;
   const size_t sxy = (size_t)g.nx * g.ny;
-  const float ih2 = 1.0f / (g.h * g.h);
+  const double ih2 = 1.0 / ((double)g.h * g.h);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n * nsrc;
        i += (size_t)gridDim.x * blockDim.x) {
     const EikNode e = eik_node(i, n, g, src);
     const float ti = T[i];
     if (ti >= kInf || in_start(e, src, r0)) continue;
-    float num = QF[i], den = 0.0f;
+    double num = QF[i], den = 0.0;
     const size_t st[3] = {1, (size_t)g.nx, sxy};
     const int id[3] = {e.ix, e.iy, e.iz}, nd[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
@@ -173,13 +175,19 @@ __global__ void k_tstar_relax(const float *__restrict__ T, const float *__restri
         has = true;
       }
       if (has) {
-        const float w = (ti - best) * ih2;
+        const double w = ((double)ti - (double)best) * ih2;
         num += w * TS[nb];
         den += w;
       }
     }
-    if (den > 0.0f) TS[i] = num / den;
+    if (den > 0.0) TS[i] = num / den;
   }
+}
+
+__global__ void k_tstar_store(const double *__restrict__ TS, float *__restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (float)TS[i];
 }
 
 // Table entries (reference layout) whose source is solved in this batch.
@@ -252,12 +260,15 @@ extern "C" int qpsdm_eikonal_solve(const float *d_vel, const float *d_invq,
   cudaStream_t st = (cudaStream_t)stream;
   const qpsdm_eik_grid g = *grid;
   const size_t n = (size_t)g.nx * g.ny * g.nz * nsrc;
+  // work: F, QF (n floats each), t* in FP64 (n doubles, 8-byte aligned), a flag
   float *F = d_work, *QF = d_work + n;
-  unsigned *changed = reinterpret_cast<unsigned *>(d_work + 2 * n);
+  double *TS = reinterpret_cast<double *>(d_work + 2 * n + ((2 * n) & 1));
+  unsigned *changed = reinterpret_cast<unsigned *>(TS + n);
+  if (reinterpret_cast<uintptr_t>(d_work) % 8) return QPSDM_EINVAL;
   const float4 *src = (const float4 *)d_src;
   const int blk = 256, grd = 148 * 8;
   k_eik_setup<<<grd, blk, 0, st>>>(d_vel, d_invq, *model, src, nsrc, g, init_radius, F, QF,
-                                   d_T, d_tstar);
+                                   d_T, TS);
   // relax in rounds of 16 sweeps until a round changes nothing (or max_iter)
   int rounds = 0;
   for (int it = 0; it < max_iter; it += 16, ++rounds) {
@@ -274,7 +285,8 @@ extern "C" int qpsdm_eikonal_solve(const float *d_vel, const float *d_invq,
   // t* needs about as many sweeps as T took to settle
   const int tsweeps = (rounds + 1) * 16;
   for (int it = 0; it < tsweeps; ++it)
-    k_tstar_relax<<<grd, blk, 0, st>>>(d_T, QF, d_tstar, src, nsrc, g, init_radius);
+    k_tstar_relax<<<grd, blk, 0, st>>>(d_T, QF, TS, src, nsrc, g, init_radius);
+  k_tstar_store<<<grd, blk, 0, st>>>(TS, d_tstar, n);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
 

@@ -285,6 +285,8 @@ __global__ void k_tab_xfast(const float *__restrict__ in, float *__restrict__ ou
   }
 }
 
+// Table data may be host or device memory (cudaMemcpyDefault: unified
+// addressing tells them apart); descriptors are host memory.
 int physics_set_lines(PhysicsState *s, const qpsdm_static_params &p,
                       const qpsdm_line_params *lines, int nlines, cudaStream_t st,
                       std::string *err) {
@@ -313,9 +315,9 @@ int physics_set_lines(PhysicsState *s, const qpsdm_static_params &p,
         return QPSDM_ENOMEM;
       }
       const dim3 g(256, (unsigned)ncell);
-      cudaMemcpyAsync(s->d_tab_tmp, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(s->d_tab_tmp, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyDefault, st);
       k_tab_xfast<<<g, 256, 0, st>>>(s->d_tab_tmp, t.ttt, t.dt, l.nxi1, l.nzi1);
-      cudaMemcpyAsync(s->d_tab_tmp, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(s->d_tab_tmp, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyDefault, st);
       k_tab_xfast<<<g, 256, 0, st>>>(s->d_tab_tmp, t.qqq, t.dq, l.nxi1, l.nzi1);
       // identical descriptors (the reference writes both tables alike): the
       // image kernel reads t and t* of a node with one 8-byte load
@@ -329,8 +331,8 @@ int physics_set_lines(PhysicsState *s, const qpsdm_static_params &p,
         k_tab_pair<<<148 * 8, 256, 0, st>>>(t.ttt, t.qqq, t.tq, l.ttt_len);
       }
     } else {
-      cudaMemcpyAsync(t.ttt, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyHostToDevice, st);
-      cudaMemcpyAsync(t.qqq, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(t.ttt, l.ttt, sizeof(float) * l.ttt_len, cudaMemcpyDefault, st);
+      cudaMemcpyAsync(t.qqq, l.qqq, sizeof(float) * l.qqq_len, cudaMemcpyDefault, st);
     }
   }
   if (cudaStreamSynchronize(st) != cudaSuccess) {
@@ -569,15 +571,28 @@ __device__ __forceinline__ float ld_sample<__nv_bfloat16>(const __nv_bfloat16 *p
 template <>
 __device__ __forceinline__ float ld_sample<__half>(const __half *p) { return __half2float(*p); }
 
+// The surface-grid test of every table lookup: fractional node coordinates
+// of (px, py) in a grid of nxs x nys nodes at spacing 1/rdx, 1/rdy centred
+// on (xc, 0), and whether they lie inside it.  Explicit IEEE operations (the
+// oracle repeats them bit for bit), because a pair is evaluated -- and
+// counted as a point-trace -- exactly when both its lookups pass this test.
+__device__ __forceinline__ bool grid_pos(float px, float py, float xc, float rdx, float rdy,
+                                         float hx, float hy, int nxs, int nys, float &fx,
+                                         float &fy) {
+  fx = __fmaf_rn(__fsub_rn(px, xc), rdx, hx);
+  fy = __fmaf_rn(py, rdy, hy);
+  return fx >= 0.0f && fx <= (float)(nxs - 1) && fy >= 0.0f && fy <= (float)(nys - 1);
+}
+
 // Table value at one depth node of a cell for surface point (px, py).
 // Returns false outside the cell's surface grid.
 __device__ __forceinline__ bool table_node(const qpsdm_ttt_desc &d, const float *__restrict__ tab,
                                            float px, float py, float xc, int poff,
                                            int nxi1, int nzi1, float &v) {
   const int nxs = d.nxs, nys = d.nys;
-  const float fx = (px - xc) / (float)d.dxs + 0.5f * (nxs - 1);
-  const float fy = py / (float)d.dys + 0.5f * (nys - 1);
-  if (!(fx >= 0.0f && fx <= (float)(nxs - 1) && fy >= 0.0f && fy <= (float)(nys - 1)))
+  float fx, fy;
+  if (!grid_pos(px, py, xc, __fdiv_rn(1.0f, (float)d.dxs), __fdiv_rn(1.0f, (float)d.dys),
+                0.5f * (nxs - 1), 0.5f * (nys - 1), nxs, nys, fx, fy))
     return false;
   int ix = min((int)fx, max(nxs - 2, 0));
   int iy = min((int)fy, max(nys - 2, 0));
@@ -645,8 +660,8 @@ __device__ __forceinline__ void setup_cells(PointCells &pc, int ixi, float z,
   pc.same = same_grid(tA, tB) && same_grid(tA, qA) && same_grid(tA, qB);
   pc.nxs = tA.nxs;
   pc.nys = tA.nys;
-  pc.rdx = 1.0f / (float)tA.dxs;
-  pc.rdy = 1.0f / (float)tA.dys;
+  pc.rdx = __fdiv_rn(1.0f, (float)tA.dxs);
+  pc.rdy = __fdiv_rn(1.0f, (float)tA.dys);
   pc.hx = 0.5f * (tA.nxs - 1);
   pc.hy = 0.5f * (tA.nys - 1);
 }
@@ -668,10 +683,8 @@ __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
                                           float px, float py, float &t, float &q) {
   if (pc.same) {  // one set of surface weights for t and t*, both depth nodes
     const int nxs = pc.nxs, nys = pc.nys;
-    const float fx = (px - pc.xc) * pc.rdx + pc.hx;
-    const float fy = py * pc.rdy + pc.hy;
-    if (!(fx >= 0.0f && fx <= (float)(nxs - 1) && fy >= 0.0f && fy <= (float)(nys - 1)))
-      return false;
+    float fx, fy;
+    if (!grid_pos(px, py, pc.xc, pc.rdx, pc.rdy, pc.hx, pc.hy, nxs, nys, fx, fy)) return false;
     const int ix = min((int)fx, max(nxs - 2, 0));
     const int iy = min((int)fy, max(nys - 2, 0));
     const float wx = nxs > 1 ? fx - ix : 0.0f, wy = nys > 1 ? fy - iy : 0.0f;
@@ -716,10 +729,8 @@ __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
                                           float px, float py, float &t, float &q) {
   if (!tq || !pc.same) return lookup_tq(pc, dt, ttt, dq, qqq, nxi1, nzi1, px, py, t, q);
   const int nxs = pc.nxs, nys = pc.nys;
-  const float fx = (px - pc.xc) * pc.rdx + pc.hx;
-  const float fy = py * pc.rdy + pc.hy;
-  if (!(fx >= 0.0f && fx <= (float)(nxs - 1) && fy >= 0.0f && fy <= (float)(nys - 1)))
-    return false;
+  float fx, fy;
+  if (!grid_pos(px, py, pc.xc, pc.rdx, pc.rdy, pc.hx, pc.hy, nxs, nys, fx, fy)) return false;
   const int ix = min((int)fx, max(nxs - 2, 0));
   const int iy = min((int)fy, max(nys - 2, 0));
   const float wx = nxs > 1 ? fx - ix : 0.0f, wy = nys > 1 ? fy - iy : 0.0f;
@@ -797,7 +808,6 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
     for (int i = 0; i < nc; ++i) {
       const int4 rg = s_rng[i];
       if (!rg.w || ixi < rg.x || ixi > rg.y || izi < rg.z) continue;
-      ++cnt;
       const float4 gm = s_geom[i];
       if (gm.x != last_sx || gm.y != last_sy) {
         last_sx = gm.x;
@@ -807,6 +817,7 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
       if (!s_ok) continue;
       float tg, qg;
       if (!lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, gm.z, gm.w, tg, qg)) continue;
+      ++cnt;  // a point-trace: in the aperture, table values at both ends
       // ray directions and dip taper (src/q-psdm.cu:2303-2340)
       const float dsx = gm.x - x, dgx = gm.z - x;
       const float ds = sqrtf(dsx * dsx + gm.y * gm.y + z2);
@@ -1010,6 +1021,18 @@ __device__ __forceinline__ bool tile_keep(float2 sp, float2 gp, const TileBox &b
   return !(fx1 < m || fx2 < m || fy1 < m || fy2 < m);  // NaN keeps the member
 }
 
+// The surface grid shared by every active point of a tile whose points all
+// read the same table cells (one test decides a source's coverage for the
+// whole tile).
+struct TileGrid {
+  float xc, rdx, rdy, hx, hy;
+  int nxs, nys;
+};
+__device__ __forceinline__ bool tile_covers(const TileGrid &g, float2 p) {
+  float fx, fy;
+  return grid_pos(p.x, p.y, g.xc, g.rdx, g.rdy, g.hx, g.hy, g.nxs, g.nys, fx, fy);
+}
+
 template <int NW>
 __device__ __forceinline__ float block_min(float v, float (*red)[NW], int k) {
   for (int off = 16; off > 0; off >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, off));
@@ -1026,7 +1049,13 @@ __device__ __forceinline__ float block_min(float v, float (*red)[NW], int k) {
 // group, the members in blocks of U (the per-point aperture and dip tests,
 // then the time/t* pick, weight and panel gathers).  Members dropped for the
 // tile fail every point's dip test, so the image is that of running every
-// member; their in-aperture point count still goes to npt.
+// member.  A point-trace is a pair in the trace's aperture whose source and
+// receiver both have table values at the point: in a tile whose active
+// points all read the same table cells (the usual case) one surface-grid
+// test per member decides that for the whole tile, members outside the grid
+// are dropped too, and a member dropped by the dip bound counts its
+// in-aperture points; in any other tile every member goes to the points,
+// which count for themselves.
 template <int TZ, int TX, int MB, int U, typename T>
 __global__ void __launch_bounds__(TZ *TX, MB)
     k_image_batched(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
@@ -1043,7 +1072,9 @@ __global__ void __launch_bounds__(TZ *TX, MB)
   extern __shared__ float2 smap[];  // [kMapN][sc][NT]
   __shared__ unsigned s_mask[NT];   // kept members of the chunk, one bit each
   __shared__ int s_col[TX + 1];     // active points of the tile's columns (prefix sums)
-  __shared__ float s_red[8][NW];
+  __shared__ float s_red[13][NW];
+  __shared__ TileGrid s_tg;         // the tile's shared surface grid (uniform tiles)
+  __shared__ int s_tgw;             // the thread that writes it
   __shared__ int s_tile;
   __shared__ unsigned long long s_cnt;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1055,7 +1086,10 @@ __global__ void __launch_bounds__(TZ *TX, MB)
   unsigned cnt = 0;
   for (;;) {
     __syncthreads();
-    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1);
+    if (tid == 0) {
+      s_tile = atomicAdd(tile_ctr, 1);
+      s_tgw = -1;
+    }
     if (tid <= TX) s_col[tid] = 0;
     __syncthreads();
     const int tile = s_tile;
@@ -1102,16 +1136,23 @@ __global__ void __launch_bounds__(TZ *TX, MB)
       block_min<NW>(act ? -tany1c : big, s_red, 5);
       block_min<NW>(act ? tany2c : big, s_red, 6);
       block_min<NW>(act ? -tany2c : big, s_red, 7);
+      // the table cells of the tile's points (exact in float: cells < 2^24)
+      block_min<NW>(act ? (float)pc.cA : big, s_red, 8);
+      block_min<NW>(act ? -(float)pc.cA : big, s_red, 9);
+      block_min<NW>(act ? (float)pc.cB : big, s_red, 10);
+      block_min<NW>(act ? -(float)pc.cB : big, s_red, 11);
+      block_min<NW>(act ? (pc.same ? 0.0f : -1.0f) : big, s_red, 12);
       if (act) atomicAdd(&s_col[lx + 1], 1);
     }
     __syncthreads();
     if (tid == 0)
       for (int c = 1; c <= TX; ++c) s_col[c] += s_col[c - 1];
     TileBox box;
+    bool uni;  // every active point reads the same cells on one surface grid
     {
-      float r[8];
+      float r[13];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
+      for (int k = 0; k < 13; ++k) {
         r[k] = s_red[k][0];
 #pragma unroll
         for (int w = 1; w < NW; ++w) r[k] = fminf(r[k], s_red[k][w]);
@@ -1127,8 +1168,11 @@ __global__ void __launch_bounds__(TZ *TX, MB)
       box.x1 = (ixb0 + a.ixstart + ncol - 1) * a.dxi;
       box.z0 = iz0 * a.dzi;
       box.z1 = (iz0 + nrow - 1) * a.dzi;
+      uni = r[8] == -r[9] && r[10] == -r[11] && r[12] == 0.0f;
+      if (uni && act && atomicCAS(&s_tgw, -1, tid) == -1)
+        s_tg = TileGrid{pc.xc, pc.rdx, pc.rdy, pc.hx, pc.hy, pc.nxs, pc.nys};
     }
-    __syncthreads();  // s_col complete
+    __syncthreads();  // s_col and s_tg complete
     if (s_col[TX] == 0) continue;  // no active point in the tile
     const int ixi_lo = ixb0 + a.ixstart, ixi_hi = ixi_lo + min(TX, a.nxb - ixb0) - 1;
 
@@ -1169,9 +1213,15 @@ __global__ void __launch_bounds__(TZ *TX, MB)
             const int sl = (mi.y & 0xFFFFFF) - s0;
             const int lo = max(mi.z, ixi_lo), hi = min(mi.w, ixi_hi);
             if (sl >= 0 && sl < ns && lo <= hi) {
-              keep = tile_keep(__ldg(srcpos + s0 + sl), __ldg(grppos + __ldg(memgrp + p)), box);
-              // dropped: its in-aperture points still count
-              if (!keep) cnt += s_col[hi - ixi_lo + 1] - s_col[lo - ixi_lo];
+              if (uni) {
+                const float2 sp = __ldg(srcpos + s0 + sl), gp = __ldg(grppos + __ldg(memgrp + p));
+                const bool cov = tile_covers(s_tg, sp) && tile_covers(s_tg, gp);
+                keep = cov && tile_keep(sp, gp, box);
+                // dropped by the dip bound: its in-aperture points still count
+                if (cov && !keep) cnt += s_col[hi - ixi_lo + 1] - s_col[lo - ixi_lo];
+              } else {
+                keep = true;  // several cells in the tile: every point decides alone
+              }
             }
           }
           const unsigned bits = __ballot_sync(0xffffffffu, keep);
@@ -1196,14 +1246,14 @@ __global__ void __launch_bounds__(TZ *TX, MB)
           int cur = -1;
           float agx = 0.f, agy = 0.f, agz = 0.f, qx1 = 0.f, qx2 = 0.f, qy1 = 0.f, qy2 = 0.f;
           float tg = 0.f, qg = 0.f, gfac = 0.f;
+          bool rok = false;  // the current receiver has table values at this point
           while (nxt >= 0) {
             const int g = gn;
             if (g != cur) {
               cur = g;
               // receiver terms, once per receiver position
               const float2 gp = __ldg(grppos + g);
-              const bool rok =
-                  lookup_tq(pc, dt, ttt, dq, qqq, tqp, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
+              rok = lookup_tq(pc, dt, ttt, dq, qqq, tqp, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
               const float dgx = gp.x - x;
               const float rdg = rsqrtf(dgx * dgx + gp.y * gp.y + z2);  // 1 / dg
               agx = dgx * rdg, agy = gp.y * rdg, agz = z * rdg;
@@ -1246,10 +1296,11 @@ __global__ void __launch_bounds__(TZ *TX, MB)
             for (int u = 0; u < U; ++u) {
               const int sl = (mi[u].y & 0xFFFFFF) - s0;
               const bool inr = (unsigned)sl < (unsigned)ns && ixi >= mi[u].z && ixi <= mi[u].w;
-              cnt += inr ? 1u : 0u;
               slv[u] = inr ? sl : 0;
               const float2 *m = smap + (size_t)slv[u] * NT + tid;
               const float2 px = m[kMapPX * sc * NT], py = m[kMapPY * sc * NT];
+              // source terms are NaN where the source has no table value
+              cnt += (inr && rok && px.x == px.x) ? 1u : 0u;
               on[u] = inr && px.x > qx1 && px.y > qx2 && py.x > qy1 && py.y > qy2;
             }
             const T *pp[U];

@@ -147,7 +147,8 @@ class Engine:
                  tables=None, ttt_cdp1=None, ttt_cdp2=None) -> None:
         """dips: (dipx1, dipx2, dipy1, dipy2), each [nxi, nzi] float32.
         tables: None or dict(nxg, nzg, nxi1, nzi1, cdp1, cdp2, ttt_desc,
-        ttt, qqq_desc, qqq) in the reference layout."""
+        ttt, qqq_desc, qqq) in the reference layout; ttt and qqq may be numpy
+        arrays or float32 torch tensors on the engine's device."""
         self.set_lines([dict(fxi=fxi, cyi=cyi, dips=dips, nf3=nf3, q=q, tables=tables,
                              ttt_cdp1=ttt_cdp1, ttt_cdp2=ttt_cdp2)])
 
@@ -181,10 +182,16 @@ class Engine:
                 d = np.ascontiguousarray(tables[k])
                 keep.append(d)
                 setattr(lp, k, d.ctypes.data)
-            lp.ttt = fptr(tables["ttt"])
-            lp.qqq = fptr(tables["qqq"])
-            lp.ttt_len = int(np.asarray(tables["ttt"]).size)
-            lp.qqq_len = int(np.asarray(tables["qqq"]).size)
+            for k in ("ttt", "qqq"):
+                a = tables[k]
+                if hasattr(a, "is_cuda") and a.is_cuda:  # table data on the device
+                    assert a.is_contiguous() and str(a.dtype) == "torch.float32"
+                    keep.append(a)
+                    setattr(lp, k, a.data_ptr())
+                    setattr(lp, k + "_len", int(a.numel()))
+                else:
+                    setattr(lp, k, fptr(a))
+                    setattr(lp, k + "_len", int(np.asarray(a).size))
         else:
             lp.ttt_cdp1 = self.p.fci if ttt_cdp1 is None else ttt_cdp1
             lp.ttt_cdp2 = self.p.fci + self.p.nxi - 1 if ttt_cdp2 is None else ttt_cdp2

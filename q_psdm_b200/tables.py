@@ -304,7 +304,7 @@ def eikonal_line_tables(model: GridModel, *, fci: int, nxi: int, dxi: float, zma
     nb = min(batch, nsrc)
     d_T = torch.empty(nb * n, dtype=torch.float32, device=dev)
     d_S = torch.empty(nb * n, dtype=torch.float32, device=dev)
-    d_w = torch.empty(2 * nb * n + 1, dtype=torch.float32, device=dev)
+    d_w = torch.empty(4 * nb * n + 4, dtype=torch.float32, device=dev)  # QPSDM_EIK_WORK_FLOATS
     for s0 in range(0, nsrc, nb):
         ns = min(nb, nsrc - s0)
         sp = np.zeros((ns, 4), np.float32)
