@@ -1,24 +1,39 @@
 """Benchmark of the imaging path: Gpoint-traces/s on one or more B200s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--form batched|plain|compat]
+                    [--config c5|c2] [--form batched|plain|compat]
 
-Workload: configuration 2's geometry (200 shots x 96 x 96 receivers, nt=2000,
-dt=2 ms, image 512 x 512 x 400 at 10 m), seeded synthetic traces, analytic
-v(z) = 1800 + 0.5 z traveltime / t* tables subsampled 8x (constant Q = 80).
-A point-trace is one (image point, trace) pair inside the trace's aperture;
-the engine counts them on the device.
+A point-trace is one (image point, trace) pair inside the trace's aperture
+whose source and receiver both have table values at the point -- the pairs
+the imaging kernel evaluates; the engine counts them on the device, the
+oracle the same way.
+
+Workload (--config c5, the default): configuration 5, the full combined
+form.  Image 1024 x 1024 x 600 at 10 m, 350 shots x 100 x 100 receivers
+(3.5 M traces), nt = 3000, dt = 2 ms, 25 Hz; v(z) = 1800 + 0.5 z with a
+low-velocity gas-cloud ellipsoid of Q = 20 in Q = 100; 40 dB gain limit.
+The brick: 16 image lines 504..519.  Tables: the project's eikonal / t*
+solver on the config-5 model (50 m grid, background-corrected) writes the
+table files of lines 504 and 520 at surface nodes every 320 m (depth nodes
+every 80 m) -- what the reference reads; the plain form interpolates them
+between lines as get_ttt_all does; the batched form images through the
+surrogate's tables: the MLP, trained on samples drawn from those solves,
+evaluated at surface nodes every 160 m for every brick line, gated at 2 ms
+against the eikonal tables.  Data: seeded synthetic gathers of the shots
+whose sources lie within the tables' reach of the brick (|y| <= 1.5 km),
+in a seeded order; each step is 8 whole gathers (80,000 traces).
+--config c2 keeps configuration 2's geometry with analytic v(z) tables.
 
 Forms (a step = one pass over one batch):
-  batched  8 shot gathers (73728 traces) into a brick of 16 image lines; FP16
-           t* panels (each trace scaled by a power of two into FP16's range)
-           computed once per trace and shared by the brick;
-           receiver-grouped persistent kernel.  The headline.
+  batched  8 shot gathers into the brick of 16 image lines; FP16 t* panels
+           (each trace scaled by a power of two into FP16's range), computed
+           once per trace and shared by the brick; receiver-grouped
+           persistent kernel; each batch replayed from a captured CUDA graph.
+           The headline.
   plain    1 shot gather into 1 image line, FP32 panels, launch per shot and
-           per line, as the reference organises its work.
+           per line, as the reference organises its work; timed in the same
+           run, reported under "forms" with the batched-over-plain ratio.
   compat   the reference's own (stub) kernel semantics, 1 shot into 1 line.
-With --form batched the plain form is also timed in the same run and
-reported under "forms" with the batched-over-plain ratio.
 
 `value`: records resident in HBM, CUDA events on the engine's stream around
 each step, L2 flushed (256 MiB write) before each step.  `e2e`: the host API
@@ -66,6 +81,7 @@ FORMS = {  # shots per step, lines per step, panel dtype, physics form
     "plain": (1, 1, 0, 0),
     "compat": (1, 1, 0, None),
 }
+DTYPE_NAME = {0: "fp32", 1: "bf16", 2: "fp16"}
 
 
 def parse():
@@ -74,6 +90,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c5", choices=["c5", "c2"])
     ap.add_argument("--form", default="batched", choices=list(FORMS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -89,62 +106,37 @@ def parse():
                     help="shot gathers per step of the chosen form (default: the form's own)")
     ap.add_argument("--lines", type=int, default=0,
                     help="image lines per step of the chosen form (default: the form's own)")
+    ap.add_argument("--batches", type=int, default=0,
+                    help="distinct batches held in HBM and cycled by the steps")
     ap.add_argument("--tile", default="",
                     help="batched kernel tile 'Z,X' instead of autotuning (for profiling)")
     ap.add_argument("--variant", type=int, default=0,
                     help="batched kernel variant (1-based, the engine's autotuner list) "
                          "instead of autotuning (for profiling)")
+    ap.add_argument("--train-steps", type=int, default=4000,
+                    help="training steps of the surrogate (config 5)")
     return ap.parse_args()
 
 
 # ---------------------------------------------------------------------------
-# workload
+# workloads
 # ---------------------------------------------------------------------------
 class Workload:
-    """Configuration 2 geometry; steps are shot gathers near the image lines."""
+    """Common part: static parameters, image lines, aperture, batches."""
 
-    LINE0 = 252                      # first image line of the brick
     HALF_CDPS, HALF_LINES = 200, 100  # aperture: +-2 km in x, +-1 km in y
+    LINE0 = 0
+    nbatch = 2
 
     def __init__(self, rank: int = 0, tile=(0, 0), variant: int = 0):
         from q_psdm_b200 import synth
         self.synth = synth
         self.tile = tile
         self.variant = variant
-        self.sv = synth.config2(seed=11)
         self.rank = rank
-        ly = self.sv.line_y(self.LINE0 + 4)
-        self.shot_ids = np.argsort(np.abs(self.sv.shots[:, 1] - ly), kind="stable")
-        self.ntr_shot = len(self.sv.receivers)
         self._rec = {}
-        self._tab = None
 
-    def shot(self, k: int) -> int:
-        return int(self.shot_ids[(self.rank * 7 + k) % len(self.shot_ids)])
-
-    def records(self, k: int, nshots: int) -> np.ndarray:
-        """SU records (big-endian) of shots k*nshots .. k*nshots+nshots-1."""
-        from q_psdm_b200 import engine as E
-        out = []
-        for j in range(k * nshots, k * nshots + nshots):
-            sid = self.shot(j)
-            if sid not in self._rec:
-                sx, sy, gx, gy = self.synth.trace_geometry(self.sv, [sid])
-                tr = self.synth.make_traces(self.sv, [sid])
-                self._rec[sid] = E.encode_su(sx, sy, gx, gy, tr, dt_us=2000,
-                                             scalco=self.sv.scalco)
-            out.append(self._rec[sid])
-        return np.concatenate(out)
-
-    def tables(self):
-        if self._tab is None:
-            from q_psdm_b200 import tables as T
-            sv = self.sv
-            self._tab = T.linear_gradient_tables(
-                sv, fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi, zmax=(sv.nzi - 1) * sv.dzi, sub=8,
-                nxi1=16, half_x=2500.0, half_y=1200.0)
-        return self._tab
-
+    # the static parameters of a form
     def static(self, form: str, max_batch: int, use_graph: int = 0):
         from q_psdm_b200 import engine as E
         sv = self.sv
@@ -152,11 +144,12 @@ class Workload:
         tz, tx = self.tile if form == "batched" else (0, 0)
         kw = dict(nxi=sv.nxi, nzi=sv.nzi, ntl=sv.ntl, dt=float(sv.dt), dxi=sv.dxi, dyi=sv.dyi,
                   dzi=sv.dzi, fci=sv.fci, scaled=sv.scaled, fxv=sv.fxv, fyv=sv.fyv,
-                  nxv=sv.nxi, nyv=sv.nyi, fc=30.0, max_batch=max_batch)
+                  nxv=sv.nxi, nyv=sv.nyi, fc=sv.fpeak, threshold=sv.threshold,
+                  max_batch=max_batch)
         if pform is None:
             return E.static_params(**kw)
-        return E.static_params(**kw, mode=1, panel_dtype=dtype, nbins=16, dtstar=0.002,
-                               form=pform, dzii=self.tables().dzii, tile_z=tz, tile_x=tx,
+        return E.static_params(**kw, mode=1, panel_dtype=dtype, nbins=16, dtstar=self.DTSTAR,
+                               form=pform, dzii=self.dzii, tile_z=tz, tile_x=tx,
                                variant=self.variant if form == "batched" else 0,
                                use_graph=use_graph)
 
@@ -164,28 +157,178 @@ class Workload:
         sv = self.sv
         nl = FORMS[form][1]
         dips = self.synth.dip_fields(sv.nxi, sv.nzi, contract_rad)
-        tab = None if FORMS[form][3] is None else self.tables().as_engine_dict()
-        return [dict(fxi=sv.fxv, cyi=sv.line_y(self.LINE0 + i), dips=dips, tables=tab)
-                for i in range(nl)]
+        return [dict(fxi=sv.fxv, cyi=sv.line_y(L), dips=dips,
+                     tables=None if FORMS[form][3] is None else self.tables_for(form, L))
+                for L in self.form_lines(form)[:nl]]
 
     def aperture(self):
         return self.synth.aperture_tables(self.HALF_CDPS, self.HALF_LINES)
 
+    def batch(self, k: int, nshots: int) -> np.ndarray:
+        """SU records (big-endian) of shots k*nshots .. k*nshots+nshots-1."""
+        from q_psdm_b200 import engine as E
+        out = []
+        for j in range(k * nshots, k * nshots + nshots):
+            sid = self.shot(j)
+            if sid not in self._rec:
+                sx, sy, gx, gy = self.synth.trace_geometry(self.sv, [sid])
+                tr = self.traces(sid, sx, sy, gx, gy)
+                self._rec[sid] = E.encode_su(sx, sy, gx, gy, tr, dt_us=2000,
+                                             scalco=self.sv.scalco)
+            out.append(self._rec[sid])
+        return np.concatenate(out)
+
+
+class Config5(Workload):
+    """Configuration 5: the full combined form (batched + panels + surrogate
+    tables against plain FP32 tables)."""
+
+    LINE0 = 504
+    TABLE_LINES = (504, 520)
+    NLINES = 16
+    DTSTAR = 0.005          # t* bins of 5 ms: 16 bins reach 80 ms (Q = 20 below the cloud)
+    COARSE, FINE = 320, 160  # surface-node spacing (m) of the eikonal and surrogate tables
+    HALF_X, HALF_Y = 2500.0, 1500.0  # surface reach of every table cell (m)
+    H = 50.0                # eikonal grid (m)
+    dzii = 80.0
+    nbatch = 6
+
+    def __init__(self, rank=0, tile=(0, 0), variant=0, train_steps=4000):
+        super().__init__(rank, tile, variant)
+        self.sv = self.synth.config5(seed=11)
+        self.train_steps = train_steps
+        sv = self.sv
+        y0, y1 = sv.line_y(self.LINE0), sv.line_y(self.LINE0 + self.NLINES - 1)
+        near = np.nonzero((sv.shots[:, 1] >= y0 - self.HALF_Y)
+                          & (sv.shots[:, 1] <= y1 + self.HALF_Y))[0]
+        rng = np.random.default_rng([11, 5])
+        self.shot_ids = near[rng.permutation(near.size)]
+        self.ntr_shot = len(sv.receivers)
+        self.tabs = None
+        self.device = 0
+
+    def shot(self, k: int) -> int:
+        return int(self.shot_ids[(self.rank * 7 + k) % len(self.shot_ids)])
+
+    def traces(self, sid, sx, sy, gx, gy):
+        sv = self.sv
+        spos = np.stack([sx, sy], 1).astype(np.float64) * sv.scaled
+        gpos = np.stack([gx, gy], 1).astype(np.float64) * sv.scaled
+        return self.synth.pair_traces_device(sv, spos, gpos, device=self.device,
+                                             seed=1000 + sid)
+
+    def line_y_model(self, L):
+        return L * self.sv.dyi
+
+    def setup(self, dev):
+        """Eikonal tables of the table lines, the surrogate and every brick
+        line's plain and surrogate tables (q_psdm_b200.surrogate.brick_tables)."""
+        from q_psdm_b200 import surrogate as S
+        sv = self.sv
+        self.device = dev
+        model = self.synth.config5_model(h=self.H)
+        bg = self.synth.config5_model(h=self.H, cloud=False)
+        self.model, self.bg = model, bg
+        self.tabs = S.brick_tables(
+            model, bg, q_bg=100.0, table_lines=list(self.TABLE_LINES),
+            brick_lines=list(range(self.LINE0, self.LINE0 + self.NLINES)),
+            line_y_of=self.line_y_model, fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi,
+            zmax=(sv.nzi - 1) * sv.dzi, dzii=self.dzii, nxi1=16, coarse_dx=self.COARSE,
+            coarse_dy=self.COARSE, fine_dx=self.FINE, fine_dy=self.FINE, half_x=self.HALF_X,
+            half_y=self.HALF_Y, h=self.H, steps=self.train_steps, device=dev, seed=0)
+
+    def form_lines(self, form):
+        if form == "batched":
+            return list(range(self.LINE0, self.LINE0 + self.NLINES))
+        return [self.LINE0 + self.NLINES // 2]   # plain / compat: the brick's middle line
+
+    def tables_for(self, form, L):
+        k = L - self.LINE0
+        return self.tabs["dense" if form == "batched" else "plain"][k]
+
     def config(self, form):
         sv = self.sv
-        ns, nl, dtype, _ = FORMS[form]
+        ns, nl, dtype, pf = FORMS[form]
+        st = self.tabs["stats"] if self.tabs else {}
+        return {"workload": f"config5 (image {sv.nxi}x{sv.nyi}x{sv.nzi} @10m, "
+                            f"{len(sv.shots)} shots x 100x100 receivers = 3.5M traces, "
+                            f"nt={sv.ntl}, dt=2ms, v(z) + gas-cloud ellipsoid Q=20 in Q=100, "
+                            f"40 dB gain limit), form {form}: {ns} shot gather(s) "
+                            f"({ns * self.ntr_shot} traces) x {nl} image line(s) of "
+                            f"{sv.nxi}x{sv.nzi} per step",
+                "form": form, "shots_per_step": ns, "lines_per_step": nl,
+                "traces_per_step": ns * self.ntr_shot,
+                "shots": f"{len(self.shot_ids)} shots whose sources lie within the tables' "
+                         f"reach of the brick (|y - brick| <= {self.HALF_Y:.0f} m), seeded "
+                         f"order; {self.nbatch} distinct batches of {ns} resident in HBM, "
+                         f"cycled by the steps",
+                "panels": DTYPE_NAME[dtype] if pf is not None else "none (stub kernel)",
+                "tables": ("surrogate: the MLP at surface nodes every 160 m for each brick "
+                           "line, gated at 2 ms against the eikonal tables"
+                           if form == "batched" else
+                           "eikonal tables of lines 504 and 520 (surface nodes every 320 m, "
+                           "depth 80 m), interpolated between the lines as get_ttt_all does"),
+                "eikonal": "config-5 model on a 50 m grid, background-corrected, t* in FP64",
+                "surrogate": st,
+                "aperture_cdps": self.HALF_CDPS, "aperture_lines": self.HALF_LINES,
+                "dtstar_s": self.DTSTAR,
+                "l2": "flushed (256 MiB write) before every timed step (inputs ~1 GB/batch)"}
+
+
+class Config2(Workload):
+    """Configuration 2's geometry with analytic v(z) tables (the previous
+    headline, kept for comparison)."""
+
+    LINE0 = 252
+    DTSTAR = 0.002
+    dzii = 80.0
+    nbatch = 2
+
+    def __init__(self, rank=0, tile=(0, 0), variant=0, train_steps=0):
+        super().__init__(rank, tile, variant)
+        self.sv = self.synth.config2(seed=11)
+        ly = self.sv.line_y(self.LINE0 + 4)
+        self.shot_ids = np.argsort(np.abs(self.sv.shots[:, 1] - ly), kind="stable")
+        self.ntr_shot = len(self.sv.receivers)
+        self._tab = None
+        self.tabs = None
+
+    def shot(self, k: int) -> int:
+        return int(self.shot_ids[(self.rank * 7 + k) % len(self.shot_ids)])
+
+    def traces(self, sid, sx, sy, gx, gy):
+        return self.synth.make_traces(self.sv, [sid])
+
+    def setup(self, dev):
+        from q_psdm_b200 import tables as T
+        sv = self.sv
+        self._tab = T.linear_gradient_tables(
+            sv, fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi, zmax=(sv.nzi - 1) * sv.dzi, sub=8,
+            nxi1=16, half_x=2500.0, half_y=1200.0)
+
+    def form_lines(self, form):
+        return list(range(self.LINE0, self.LINE0 + 16))
+
+    def tables_for(self, form, L):
+        return self._tab.as_engine_dict()
+
+    def config(self, form):
+        sv = self.sv
+        ns, nl, dtype, pf = FORMS[form]
         return {"workload": f"config2 ({len(sv.shots)} shots x 96x96 receivers, nt={sv.ntl}, "
                             f"dt=2ms, image {sv.nxi}x{sv.nyi}x{sv.nzi} @10m), form {form}: "
                             f"{ns} shot gather(s) x {nl} image line(s) of {sv.nxi}x{sv.nzi} "
                             f"per step",
                 "form": form, "shots_per_step": ns, "lines_per_step": nl,
                 "traces_per_step": ns * self.ntr_shot,
-                "panels": {0: "fp32", 1: "bf16", 2: "fp16"}[dtype] if FORMS[form][3] is not None
-                else "none (stub kernel)",
+                "panels": DTYPE_NAME[dtype] if pf is not None else "none (stub kernel)",
                 "tables": "analytic v(z)=1800+0.5z traveltime and t* (Q=80), surface and depth "
                           "subsampled 8x, reference ttt/qqq layout",
                 "aperture_cdps": self.HALF_CDPS, "aperture_lines": self.HALF_LINES,
                 "l2": "flushed (256 MiB write) before every timed step"}
+
+
+WORKLOADS = {"c5": Config5, "c2": Config2}
 
 
 # ---------------------------------------------------------------------------
@@ -318,16 +461,16 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     az = wl.aperture()
     o = E.offset_params(p, 0, p.nxi, aznx1=az[0], aznx2=az[1], azny1=az[2], azny2=az[3])
     eng.begin_offset(o)
-    nbatch = 2
-    recs = [wl.records(k, ns) for k in range(nbatch)]
+    nbatch = wl.nbatch if form == "batched" else 2
+    recs = [wl.batch(k, ns) for k in range(nbatch)]
     drecs = [torch.from_numpy(r).cuda() for r in recs]
     ntr = recs[0].shape[0]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    for k in range(warmup):
+    for k in range(max(warmup, nbatch + 1)):   # every batch eager once, then captured
         eng.submit_device(drecs[k % nbatch].data_ptr(), ntr)
     torch.cuda.synchronize()
-    _, npt0 = eng.counters()
+    nacc0, npt0 = eng.counters()
     eng.profile(True)
     if dist:
         dist.barrier()
@@ -346,7 +489,7 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     torch.cuda.synchronize()
     ck = clk.stop() if clocks else None
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    _, npt1 = eng.counters()
+    nacc1, npt1 = eng.counters()
     npt = npt1 - npt0
     kt = _kernel_times(eng, _lib)  # launch counts (graph replays included)
     eng.profile(False)
@@ -367,6 +510,7 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     out = {"value": npt_all / (ms_max * 1e-3) / 1e9, "ms_per_step": ms_max / steps,
            "point_traces_per_step": npt_all / steps, "clocks": ck,
            "kernel_ms_per_step": kms,
+           "gate_accepted_per_step": (nacc1 - nacc0) / steps,
            "launches": int(sum(v[1] for v in kt.values())),
            "image_ms_per_launch": img_launch,
            "image_launches": kt["image"][1], "npt": npt}
@@ -405,6 +549,7 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
                       "path": "qpsdm_submit_traces from pinned host SU records (DMA) + "
                               "qpsdm_get_image every step"}
     eng.close()
+    del drecs
     torch.cuda.set_stream(torch.cuda.default_stream())
     return out
 
@@ -417,16 +562,21 @@ def run_ours(args, rank, world, dist):
         ns, nl, dt, pf = FORMS[args.form]
         FORMS[args.form] = (args.shots or ns, args.lines or nl, dt, pf)
     tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else (0, 0)
-    wl = Workload(rank, tile, args.variant)
+    wl = WORKLOADS[args.config](rank, tile, args.variant, args.train_steps)
+    if args.batches:
+        wl.nbatch = args.batches
+    t0 = time.perf_counter()
+    wl.setup(dev)
+    setup_s = time.perf_counter() - t0
     head = run_form(args.form, wl, args, dev, dist, steps=args.steps, warmup=args.warmup,
                     e2e=not args.no_e2e)
-    forms = {args.form: {k: head[k] for k in ("value", "ms_per_step", "point_traces_per_step",
-                                              "kernel_ms_per_step")}}
+    keys = ("value", "ms_per_step", "point_traces_per_step", "kernel_ms_per_step",
+            "gate_accepted_per_step")
+    forms = {args.form: {k: head[k] for k in keys}}
     if args.form == "batched":
         pl = run_form("plain", wl, args, dev, dist, steps=max(3, args.steps // 2),
                       warmup=2, e2e=False, clocks=False)
-        forms["plain"] = {k: pl[k] for k in ("value", "ms_per_step", "point_traces_per_step",
-                                             "kernel_ms_per_step")}
+        forms["plain"] = {k: pl[k] for k in keys}
         forms["batched_over_plain"] = head["value"] / pl["value"]
     if rank != 0:
         return None, wl
@@ -458,7 +608,8 @@ def run_ours(args, rank, world, dist):
            "data": "synthetic", "config": wl.config(args.form), "roofline": roof,
            "e2e": head.get("e2e"), "gpu_launches": head["launches"], "clocks": head["clocks"],
            "point_traces_per_step": head["point_traces_per_step"],
-           "kernel_ms_per_step": head["kernel_ms_per_step"], "forms": forms}
+           "kernel_ms_per_step": head["kernel_ms_per_step"], "forms": forms,
+           "setup_s": setup_s}
     if "tuning" in head:
         res["config"]["autotuned"] = head["tuning"]
     if args.form == "batched":
@@ -555,7 +706,7 @@ def run_eikonal(dev, half_x=2000.0):
     h = 40.0
     model = synth.config2_model(h=h)
     bg = synth.config2_model(h=h, anomalies=False, layered_q=False)
-    line_y = (Workload.LINE0) * sv.dyi
+    line_y = Config2.LINE0 * sv.dyi
     kw = dict(fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi, zmax=(sv.nzi - 1) * sv.dzi, line_y=line_y,
               dzii=80.0, nxi1=16, surf_dx=160, surf_dy=160, half_x=half_x,
               half_y=half_x / 2, h=h, init_radius=200.0, background=bg, q_background=80.0)
@@ -579,7 +730,7 @@ def run_eikonal(dev, half_x=2000.0):
 
 
 # ---------------------------------------------------------------------------
-# CPU legs
+# CPU legs and accuracy
 # ---------------------------------------------------------------------------
 def _gate_params(O, wl, line):
     sv = wl.sv
@@ -603,21 +754,49 @@ def _hdr_traces(rec):
     return hdr, rec[:, 240:].copy().view(">f4").astype(np.float32)
 
 
-def cpu_compat_rate(wl, budget_s=10.0):
+def _host_tables(t):
+    """An engine table dict with host (numpy) data."""
+    d = dict(t)
+    for k in ("ttt", "qqq"):
+        if hasattr(d[k], "cpu"):
+            d[k] = d[k].cpu().numpy()
+    return d
+
+
+def _phys_params(O, wl, st, tab):
+    sv = wl.sv
+    return O.PhysParams(nzi=sv.nzi, nxb=sv.nxi, ixstart=0, nt=st["nffti"], nbins=16,
+                        dt1=float(st["dt1"]), dxi=sv.dxi, dzi=sv.dzi,
+                        taperzone=float(st["taperzone"]), dtstar=float(np.float32(wl.DTSTAR)),
+                        dzii=wl.dzii, tcdp1=tab["cdp1"] - sv.fci, tcdp2=tab["cdp2"] - sv.fci,
+                        nxg=tab["nxg"], nzg=tab["nzg"], nxi1=tab["nxi1"], nzi1=tab["nzi1"])
+
+
+def _cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_compat_rate(wl, budget_s=10.0, line=None):
     """The reference's CPU path of one image line: gate, its preprocessing
     (compiled reference code when oracle/_ref exists, else the oracle) and the
     C restatement of its imaging kernel, all host threads."""
     from oracle import oracle as O
     sv = wl.sv
-    line = wl.LINE0
-    st = O.derive_static(sv.ntl, np.float32(sv.dt), 600.0, 3.0, 8.0)
+    line = wl.form_lines("plain")[0] if line is None else line
+    st = O.derive_static(sv.ntl, np.float32(sv.dt), sv.threshold, 3.0, 8.0)
     w = O.window_split(sv.ntl, np.float32(sv.dt), 1.0, 140.0)
     gp = _gate_params(O, wl, line)
     ipar = O.ImageParams(nzi=sv.nzi, nxb=sv.nxi, ixstart=0, nt=st["nffti"], dt1=st["dt1"],
                          dxi=sv.dxi, dzi=sv.dzi, taperzone=st["taperzone"], tcdp1=0,
                          tcdp2=sv.nxi - 1)
     dips = [d.ravel() for d in wl.synth.dip_fields(sv.nxi, sv.nzi, float(st["contract"]))]
-    hdr, traces = _hdr_traces(wl.records(0, 1))
+    hdr, traces = _hdr_traces(wl.batch(0, 1))
     R = O.ref_cpu()
     nthr = os.cpu_count() or 1
     img = np.zeros(sv.nxi * sv.nzi, np.float32)
@@ -652,30 +831,30 @@ def cpu_compat_rate(wl, budget_s=10.0):
             n = min(hdr.shape[0], n * 2)
     kind = "reference" if R is not None else "port"
     return {"value": npt_tot / t_tot / 1e9, "unit": "Gpoint-traces/s", "cores": nthr,
-            "kind": kind,
-            "sample": f"{ntr_tot} traces of a config-2 shot gather into one 512x400 line "
-                      f"({npt_tot} point-traces, {t_tot:.1f} s): gate + the reference's "
-                      f"preprocessing ({'compiled from its sources' if R is not None else 'oracle'})"
-                      f" + C restatement of image_depth_gpu, {nthr} threads"}
+            "kind": kind, "cpu_model": _cpu_model(),
+            "sample": f"{ntr_tot} traces of a {wl.sv.name} shot gather into one "
+                      f"{sv.nxi}x{sv.nzi} line ({npt_tot} point-traces, {t_tot:.1f} s): gate + "
+                      f"the reference's preprocessing "
+                      f"({'compiled from its sources' if R is not None else 'oracle'}) + C "
+                      f"restatement of its image_depth_gpu (the stub body, ts = tg = 1: the "
+                      f"reference has no other imaging), {nthr} threads"}
 
 
 def cpu_physics_rate(wl, budget_s=10.0):
     """The physics method on the CPU (the FP64 restatement: numpy panels + C
-    imaging, all host threads) on a bounded sample of one shot and one line."""
+    imaging, all host threads) on a bounded sample of one shot and one line,
+    with the plain form's tables."""
     from oracle import oracle as O
     sv = wl.sv
-    line = wl.LINE0
-    st = O.derive_static(sv.ntl, np.float32(sv.dt), 600.0, 3.0, 8.0)
+    line = wl.form_lines("plain")[0]
+    st = O.derive_static(sv.ntl, np.float32(sv.dt), sv.threshold, 3.0, 8.0)
     gp = _gate_params(O, wl, line)
-    tab = wl.tables()
-    pp = O.PhysParams(nzi=sv.nzi, nxb=sv.nxi, ixstart=0, nt=st["nffti"], nbins=16,
-                      dt1=float(st["dt1"]), dxi=sv.dxi, dzi=sv.dzi,
-                      taperzone=float(st["taperzone"]), dtstar=float(np.float32(0.002)),
-                      dzii=tab.dzii, tcdp1=tab.cdp1 - sv.fci, tcdp2=tab.cdp2 - sv.fci,
-                      nxg=tab.nxg, nzg=tab.nzg, nxi1=tab.nxi1, nzi1=tab.nzi1)
-    filt = O.physics_filter(st["nfft"], np.float32(sv.dt), 130.0, 140.0, 30.0, 600.0, 16, 0.002)
+    tab = _host_tables(wl.tables_for("plain", line))
+    pp = _phys_params(O, wl, st, tab)
+    filt = O.physics_filter(st["nfft"], np.float32(sv.dt), 130.0, 140.0, sv.fpeak,
+                            sv.threshold, 16, wl.DTSTAR)
     dips = [d.ravel() for d in wl.synth.dip_fields(sv.nxi, sv.nzi, float(st["contract"]))]
-    hdr, traces = _hdr_traces(wl.records(0, 1))
+    hdr, traces = _hdr_traces(wl.batch(0, 1))
     nthr = os.cpu_count() or 1
     img = np.zeros(sv.nxi * sv.nzi)
     rng = np.random.default_rng(1)
@@ -689,8 +868,7 @@ def cpu_physics_rate(wl, budget_s=10.0):
         if ok.any():
             pan = O.physics_panels(traces[idx][ok], np.float32(sv.dt), st["nfft"], st["nffti"],
                                    filt)
-            _, npt = O.physics_image(pp, geom[ok], ints[ok][:, [4, 5, 7]], pan, dips,
-                                     tab.as_engine_dict(), img)
+            _, npt = O.physics_image(pp, geom[ok], ints[ok][:, [4, 5, 7]], pan, dips, tab, img)
         t_tot += time.perf_counter() - t0
         npt_tot += npt
         ntr_tot += n
@@ -699,56 +877,60 @@ def cpu_physics_rate(wl, budget_s=10.0):
         if t_tot < budget_s / 8:
             n = min(512, n * 2)
     return {"value": npt_tot / t_tot / 1e9, "unit": "Gpoint-traces/s", "cores": nthr,
-            "kind": "port",
-            "sample": f"{ntr_tot} random traces of a config-2 shot into one 512x400 line "
-                      f"({npt_tot} point-traces, {t_tot:.1f} s): the FP64 CPU restatement of "
-                      f"the physics method (numpy float64 panels + C imaging), {nthr} threads"}
+            "kind": "port", "cpu_model": _cpu_model(),
+            "sample": f"{ntr_tot} random traces of a {sv.name} shot into one {sv.nxi}x{sv.nzi} "
+                      f"line ({npt_tot} point-traces, {t_tot:.1f} s): the FP64 CPU "
+                      f"restatement of the physics method (numpy float64 panels + C imaging), "
+                      f"{nthr} threads"}
 
 
-def accuracy_vs_fp64(wl, dev, ntr=1536, seed=2):
+def accuracy_vs_fp64(wl, dev, ntr=1200, seed=2):
     """NRMSE of the batched-form image and of the plain FP32 image against the
-    FP64 oracle on the same input: a seeded sample of `ntr` traces of the
-    step's first two shot gathers, imaged into the brick's first line."""
+    FP64 oracle on the same input and the same tables each form uses: a
+    seeded sample of `ntr` traces of the step's first two shot gathers,
+    imaged into the plain form's line (the brick's middle line)."""
     from oracle import oracle as O
     from q_psdm_b200 import engine as E
     sv = wl.sv
-    line = wl.LINE0
-    rec = wl.records(0, 2)
+    line = wl.form_lines("plain")[0]
+    rec = wl.batch(0, 2)
     rng = np.random.default_rng(seed)
     rec = np.ascontiguousarray(rec[np.sort(rng.choice(rec.shape[0], ntr, replace=False))])
     hdr, traces = _hdr_traces(rec)
-    st = O.derive_static(sv.ntl, np.float32(sv.dt), 600.0, 3.0, 8.0)
-    tab = wl.tables()
-    pp = O.PhysParams(nzi=sv.nzi, nxb=sv.nxi, ixstart=0, nt=st["nffti"], nbins=16,
-                      dt1=float(st["dt1"]), dxi=sv.dxi, dzi=sv.dzi,
-                      taperzone=float(st["taperzone"]), dtstar=float(np.float32(0.002)),
-                      dzii=tab.dzii, tcdp1=tab.cdp1 - sv.fci, tcdp2=tab.cdp2 - sv.fci,
-                      nxg=tab.nxg, nzg=tab.nzg, nxi1=tab.nxi1, nzi1=tab.nzi1)
-    filt = O.physics_filter(st["nfft"], np.float32(sv.dt), 130.0, 140.0, 30.0, 600.0, 16, 0.002)
+    st = O.derive_static(sv.ntl, np.float32(sv.dt), sv.threshold, 3.0, 8.0)
+    filt = O.physics_filter(st["nfft"], np.float32(sv.dt), 130.0, 140.0, sv.fpeak,
+                            sv.threshold, 16, wl.DTSTAR)
     dips = [d.ravel() for d in wl.synth.dip_fields(sv.nxi, sv.nzi, float(st["contract"]))]
     ints, geom = O.gate_traces(_gate_params(O, wl, line), hdr)
     ok = ints[:, 0] == 3
     pan = O.physics_panels(traces[ok], np.float32(sv.dt), st["nfft"], st["nffti"], filt)
-    ref, npt = O.physics_image(pp, geom[ok], ints[ok][:, [4, 5, 7]], pan, dips,
-                               tab.as_engine_dict())
-    ref = np.asarray(ref, np.float64).reshape(sv.nxi, sv.nzi)
-    out = {"sample": f"{ntr} seeded traces of 2 config-2 shot gathers into line {line} "
-                     f"({npt} point-traces); FP64 oracle: numpy float64 panels + C imaging"}
+    out = {"sample": f"{ntr} seeded traces of 2 {sv.name} shot gathers into line {line}; "
+                     f"FP64 oracle: numpy float64 panels + C imaging with the form's own tables"}
     for form in ("batched", "plain"):
+        tab = wl.tables_for(form, line)
+        ref, npt = O.physics_image(_phys_params(O, wl, st, tab), geom[ok], ints[ok][:, [4, 5, 7]],
+                                   pan, dips, _host_tables(tab))
+        ref = np.asarray(ref, np.float64).reshape(sv.nxi, sv.nzi)
         p = wl.static(form, max_batch=ntr)
         eng = E.Engine(p, device=dev)
         try:
-            eng.set_lines(wl.lines(form, p.contract)[:1])
+            eng.set_lines([dict(fxi=sv.fxv, cyi=sv.line_y(line),
+                                dips=wl.synth.dip_fields(sv.nxi, sv.nzi, p.contract),
+                                tables=tab)])
             az = wl.aperture()
             eng.begin_offset(E.offset_params(p, 0, p.nxi, aznx1=az[0], aznx2=az[1],
                                              azny1=az[2], azny2=az[3]))
             eng.submit(rec)
             img = np.asarray(eng.get_image(False), np.float64).reshape(sv.nxi, sv.nzi)
+            _, n = eng.counters()
         finally:
             eng.close()
         e = float(np.sqrt(np.mean((img - ref) ** 2)) / np.sqrt(np.mean(ref ** 2)))
-        dt_name = {0: "fp32", 1: "bf16", 2: "fp16"}[FORMS[form][2]]
+        dt_name = DTYPE_NAME[FORMS[form][2]]
         out[f"nrmse_{form}_{dt_name}_panels_vs_fp64"] = e
+        out[f"point_traces_{form}"] = int(n)
+        if n != npt:
+            out[f"point_trace_mismatch_{form}"] = [int(n), int(npt)]
     return out
 
 
@@ -816,10 +998,23 @@ def accuracy_config(name, dev, ntr=1200):
     return out
 
 
+def surrogate_truth(wl, dev):
+    """Traveltime error of the surrogate's and of the plain tables against
+    the eikonal solver at the plain form's line (config 5)."""
+    from q_psdm_b200 import surrogate as S
+    sv = wl.sv
+    line = wl.form_lines("plain")[0]
+    return S.truth_error_sample(
+        wl.tabs["surrogate"], wl.model, wl.bg, q_bg=100.0, line_y=wl.line_y_model(line),
+        plain_tables=wl.tables_for("plain", line), fci=sv.fci, dxi=sv.dxi,
+        zmax=(sv.nzi - 1) * sv.dzi, dzii=wl.dzii, fine_dx=wl.FINE, fine_dy=wl.FINE,
+        half_x=wl.HALF_X, half_y=wl.HALF_Y, h=wl.H, ncells=32, seed=3, device=dev)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
-    wl = Workload(0)
+    wl = WORKLOADS[args.config](0)
     for _ in range(args.warmup):
         cpu_compat_rate(wl, budget_s=0.3)
     vals = []
@@ -831,15 +1026,22 @@ def run_reference(args, rank, world):
     el = time.perf_counter() - t0
     v = float(np.mean(vals))
     info = dict(info, value=v)
+    sv = wl.sv
+    cfg = {"workload": f"{sv.name} geometry (image {sv.nxi}x{sv.nyi}x{sv.nzi} @10m, "
+                       f"nt={sv.ntl}), the reference's own CPU path: one shot gather of the "
+                       f"benchmark's brick into one {sv.nxi}x{sv.nzi} image line per sample",
+           "form": "reference (per trace, per line)", "shots_per_step": 1, "lines_per_step": 1,
+           "computation": "gate + the reference's preprocessing compiled from its sources "
+                          "(oracle/_ref: t^2 gain, tapers, two PFA r2c windows, -i w) + the C "
+                          "restatement of image_depth_gpu, whose body is a stub (ts = tg = 1, "
+                          "src/q-psdm.cu:2350-2351): the reference has no physics imaging, "
+                          "on the CPU or elsewhere",
+           "aperture_cdps": wl.HALF_CDPS, "aperture_lines": wl.HALF_LINES}
     return {"metric": METRIC, "impl": "reference", "value": v, "unit": "Gpoint-traces/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(wl.config("batched"), reference_path=(
-                "the reference's own CPU path of the same workload: its preprocessing "
-                "compiled from its sources (oracle/_ref) and the C restatement of its "
-                "imaging kernel, per shot gather and line, all host threads")),
-            "cpu_baseline": info,
+            "config": cfg, "cpu_baseline": info,
             "e2e": {"value": v, "unit": "Gpoint-traces/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -849,7 +1051,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
-    if world > 1:
+    if world > 1 and args.impl != "reference":
         import datetime
         import torch
         import torch.distributed as tdist
@@ -876,6 +1078,8 @@ def main():
                                    else cpu_physics_rate(wl))
             if not args.no_accuracy:
                 res["accuracy"] = accuracy_vs_fp64(wl, dev)
+                if args.config == "c5":
+                    res["accuracy"]["surrogate_traveltime_vs_eikonal"] = surrogate_truth(wl, dev)
                 res["accuracy"]["configs"] = {n: accuracy_config(n, dev)
                                               for n in ("c1", "c3", "c5")}
     if res is not None:

@@ -417,6 +417,14 @@ typedef struct {
   float v0, kz, q_ref; /* the network's background */
 } qpsdm_sur_line;
 
+/* Table data of `line` between the lines line_lo <= line <= line_hi that
+ * have table files (d_lo, d_hi: n floats each, device): d_out = d_lo c1 +
+ * d_hi c2 with c2 = (line - line_lo) / (line_hi - line_lo), c1 = 1 - c2, in
+ * float without fused multiply-adds -- the interpolation of get_ttt_all
+ * (src/q-psdm.cu:2584-2596) on the device, bit for bit.  Asynchronous. */
+int qpsdm_tables_lerp(const float *d_lo, const float *d_hi, int64_t n, int line, int line_lo,
+                      int line_hi, float *d_out, void *stream);
+
 /* Background correction of a line's eikonal tables in place: with d_ttt_bg,
  * d_qqq_bg the same line's tables from solves of the linear-gradient
  * background (v0, kz of ln, constant Q = q_bg) on the same grids,

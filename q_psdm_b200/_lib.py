@@ -144,6 +144,7 @@ SYMBOLS = [
     ("qpsdm_mlp_status", _I, [_P]),
     ("qpsdm_eikonal_samples", _I, [_P, _P, _P, _P, C.POINTER(EikGrid), _P, _I,
                                    C.POINTER(SurBackground), C.c_uint64, _I, _P, _P, _P]),
+    ("qpsdm_tables_lerp", _I, [_P, _P, C.c_int64, _I, _I, _I, _P, _P]),
     ("qpsdm_eikonal_correct", _I, [C.POINTER(SurLine), _P, _P, _P, _P, _P, C.c_int64, _F, _P]),
     ("qpsdm_surrogate_gate", _I, [_P, C.POINTER(SurLine), _P, _P, C.c_int64, _P, _P]),
     ("qpsdm_surrogate_tables", _I, [_P, C.POINTER(SurLine), _P, _P, _P, C.c_int64, _P, _F, _P,

@@ -248,6 +248,16 @@ __global__ void k_tab_correct(TabView v, qpsdm_sur_line ln, float q_bg, float *_
   }
 }
 
+// Tables of a line between two lines that have table files, as get_ttt_all
+// interpolates them (src/q-psdm.cu:2584-2596): out = a c1 + b c2 in float,
+// no fused multiply-add, c2 = (line - lo) / (hi - lo), c1 = 1 - c2.
+__global__ void k_tab_lerp(const float *__restrict__ a, const float *__restrict__ b, int64_t n,
+                           float c1, float c2, float *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = __fadd_rn(__fmul_rn(a[i], c1), __fmul_rn(b[i], c2));
+}
+
 // Host: a table's descriptors and prefix sums on the device (one allocation).
 struct DevTab {
   void *mem = nullptr;
@@ -321,6 +331,19 @@ extern "C" int qpsdm_eikonal_samples(const float *d_T, const float *d_tstar, con
   k_eik_samples<<<148 * 4, 256, 0, (cudaStream_t)stream>>>(
       d_T, d_tstar, d_T_bg, d_tstar_bg, *grid, (const float4 *)d_src, ns, *bg, seed, nsamples,
       d_x, d_t);
+  return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
+}
+
+extern "C" int qpsdm_tables_lerp(const float *d_lo, const float *d_hi, int64_t n, int line,
+                                 int line_lo, int line_hi, float *d_out, void *stream) {
+  if (!d_lo || !d_hi || !d_out || n < 0 || line < line_lo || line > line_hi ||
+      (line_hi == line_lo && line != line_lo))
+    return QPSDM_EINVAL;
+  if (n == 0) return QPSDM_OK;
+  const float c2 = line_hi == line_lo ? 0.0f
+                                      : (float)(1.0 * (line - line_lo) / (line_hi - line_lo));
+  const float c1 = (float)(1.0 - c2);
+  k_tab_lerp<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(d_lo, d_hi, n, c1, c2, d_out);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
 

@@ -360,3 +360,295 @@ def coarse_to_fine(coarse: LineTables, *, fci: int, surf_dx: int, surf_dy: int,
                                        src[sc].reshape(shp_c).astype(np.float64))
             dst[sf] = v.astype(np.float32).ravel()
     return fine
+
+
+# ---------------------------------------------------------------------------
+# on the device: training samples from eikonal grids, gate and dense tables
+# ---------------------------------------------------------------------------
+class EikonalSamples:
+    """Training samples drawn from the eikonal solver's grids while they are
+    on the device: a sampler for `tables.eikonal_line_tables` (and any other
+    loop over solved source batches).  Every batch of `ns` sources yields
+    `per_source * ns` samples (qpsdm_eikonal_samples: uniform (source, node)
+    pairs, background-corrected targets); the set of all sources x grid
+    nodes is never formed."""
+
+    def __init__(self, bg: Background, q_bg: float, per_source: int = 256, device: int = 0,
+                 seed: int = 0):
+        import torch
+        self.torch = torch
+        self.bg = bg
+        self.q_bg = q_bg
+        self.per_source = per_source
+        self.dev = torch.device("cuda", device)
+        self.seed = seed
+        self.xs, self.ts = [], []
+        self.sources = 0
+
+    def __call__(self, d_T, d_S, d_Tb, d_Sb, grid, d_src, ns):
+        torch = self.torch
+        n = self.per_source * ns
+        x = torch.empty((n, 5), dtype=torch.float32, device=self.dev)
+        t = torch.empty((n, 2), dtype=torch.float32, device=self.dev)
+        b = _lib.SurBackground(self.bg.v0, self.bg.kz, self.bg.q_ref, self.q_bg)
+        ptr = lambda a: None if a is None else a.data_ptr()
+        rc = _lib.lib().qpsdm_eikonal_samples(
+            d_T.data_ptr(), d_S.data_ptr(), ptr(d_Tb), ptr(d_Sb), C.byref(grid),
+            d_src.data_ptr(), ns, C.byref(b), (self.seed * 1000003 + len(self.xs)) & (2**64 - 1),
+            n, x.data_ptr(), t.data_ptr(), None)
+        _lib.check(rc, what="eikonal_samples")
+        self.xs.append(x)
+        self.ts.append(t)
+        self.sources += ns
+
+    def tensors(self):
+        torch = self.torch
+        return torch.cat(self.xs), torch.cat(self.ts)
+
+
+def train_device(X, Y, bg: Background, *, steps: int = 4000, batch: int = 8192,
+                 lr: float = 2e-3, lr_end: float = 2e-5, seed: int = 0, device: int = 0,
+                 log_every: int = 500, w_out=(1.0, 25.0)) -> Surrogate:
+    """`train` on samples already on the device (X [n][5], Y [n][2] torch
+    float32, e.g. from EikonalSamples): Adam with cosine decay over uniformly
+    drawn mini-batches, every step the library's tcgen05 kernels."""
+    import torch
+    mlp = Mlp(device, seed)
+    lo = X.min(0).values.double().cpu().numpy()
+    hi = X.max(0).values.double().cpu().numpy()
+    span = hi - lo
+    scale = np.where(span > 1e-3, 2.0 / np.maximum(span, 1e-3), 1e-3).astype(np.float32)
+    mlp.set_scaling((0.5 * (lo + hi)).astype(np.float32), scale, w_out)
+    gen = torch.Generator(device=mlp.dev)
+    gen.manual_seed(seed)
+    n = X.shape[0]
+    bx = torch.empty((batch, 5), dtype=torch.float32, device=mlp.dev)
+    by = torch.empty((batch, 2), dtype=torch.float32, device=mlp.dev)
+    hist = []
+    for s in range(steps):
+        idx = torch.randint(0, n, (batch,), generator=gen, device=mlp.dev)
+        torch.index_select(X, 0, idx, out=bx)
+        torch.index_select(Y, 0, idx, out=by)
+        a = lr_end + 0.5 * (lr - lr_end) * (1.0 + np.cos(np.pi * s / steps))
+        want = log_every > 0 and (s % log_every == 0 or s == steps - 1)
+        loss = mlp.train_step(bx, by, a, want_loss=want)
+        if want:
+            hist.append((s, loss))
+    mlp.status()
+    return Surrogate(mlp, bg, hist)
+
+
+def layout(nxg: int, nzg: int, nxi1: int, nzi1: int, *, surf_dx: int, surf_dy: int,
+           half_x: float, half_y: float):
+    """Descriptors (DESC_DTYPE [nxg*nzg]) and total length of tables whose
+    cells all have the surface grid +-half_x, +-half_y at (surf_dx, surf_dy)."""
+    nxs = 2 * int(np.ceil(half_x / surf_dx)) + 1
+    nys = 2 * int(np.ceil(half_y / surf_dy)) + 1
+    block = nys * nxs * nxi1 * nzi1
+    desc = np.zeros(nxg * nzg, DESC_DTYPE)
+    for k in range(nxg * nzg):
+        desc[k] = (k * block, nys, nxs, surf_dy, surf_dx)
+    return desc, nxg * nzg * block
+
+
+def _sur_line(sur: Surrogate, tab: LineTables, fci: int, line_y: float):
+    return _lib.SurLine(tab.nxg, tab.nzg, tab.nxi1, tab.nzi1, tab.cdp1 - fci, tab.dx, tab.dzii,
+                        line_y, sur.bg.v0, sur.bg.kz, sur.bg.q_ref)
+
+
+def gate_errors(sur: Surrogate, tabs, line_ys, *, fci: int = 1):
+    """Node errors (ms, torch on the device) of the network against the
+    tables of the given lines (all with the same layout), the maximum over
+    the lines: qpsdm_surrogate_gate.  Table data from tab.dev when present."""
+    import torch
+    t0 = tabs[0]
+    nodes = int(sum(int(d["nys"]) * int(d["nxs"]) for d in t0.desc))
+    err = torch.zeros(nodes, dtype=torch.float32, device=sur.mlp.dev)
+    for tab, ly in zip(tabs, line_ys):
+        ttt = tab.dev["ttt"] if tab.dev is not None else torch.from_numpy(tab.ttt).to(sur.mlp.dev)
+        ln = _sur_line(sur, tab, fci, ly)
+        d = np.ascontiguousarray(tab.desc)
+        rc = _lib.lib().qpsdm_surrogate_gate(sur.mlp.h, C.byref(ln), d.ctypes.data,
+                                             ttt.data_ptr(), int(ttt.numel()), err.data_ptr(),
+                                             None)
+        _lib.check(rc, what="surrogate_gate")
+    return err
+
+
+def dense_tables_device(sur: Surrogate, coarse: LineTables, coarse_ttt, coarse_qqq, node_err,
+                        *, fci: int, line_y: float, surf_dx: int, surf_dy: int, half_x: float,
+                        half_y: float, gate_ms: float = 2.0):
+    """Tables of the line at model y `line_y` on the surface grid (surf_dx,
+    surf_dy, +-half_x, +-half_y) from the network, on the device
+    (qpsdm_surrogate_tables): returns (engine table dict with torch data,
+    gated fine nodes).  coarse_ttt / coarse_qqq (torch, device): the plain
+    method's tables of this line in coarse's layout -- the fallback in the
+    patches whose corner nodes the network missed by more than gate_ms."""
+    import torch
+    fdesc, flen = layout(coarse.nxg, coarse.nzg, coarse.nxi1, coarse.nzi1, surf_dx=surf_dx,
+                         surf_dy=surf_dy, half_x=half_x, half_y=half_y)
+    dev = sur.mlp.dev
+    ft = torch.empty(flen, dtype=torch.float32, device=dev)
+    fq = torch.empty(flen, dtype=torch.float32, device=dev)
+    ln = _sur_line(sur, coarse, fci, line_y)
+    cd = np.ascontiguousarray(coarse.desc)
+    gated = C.c_int64()
+    rc = _lib.lib().qpsdm_surrogate_tables(
+        sur.mlp.h, C.byref(ln), cd.ctypes.data, coarse_ttt.data_ptr(), coarse_qqq.data_ptr(),
+        int(coarse_ttt.numel()), node_err.data_ptr(), float(gate_ms), fdesc.ctypes.data,
+        ft.data_ptr(), fq.data_ptr(), int(flen), C.byref(gated), None)
+    _lib.check(rc, what="surrogate_tables")
+    d = fdesc.view(np.uint8).reshape(-1, 16).copy()
+    return (dict(nxg=coarse.nxg, nzg=coarse.nzg, nxi1=coarse.nxi1, nzi1=coarse.nzi1,
+                 cdp1=coarse.cdp1, cdp2=coarse.cdp2, ttt_desc=d, qqq_desc=d, ttt=ft, qqq=fq),
+            int(gated.value))
+
+
+def lerp_device(lo, hi, line: int, line_lo: int, line_hi: int):
+    """Device copy of the tables of `line` interpolated between two lines'
+    device tables, as get_ttt_all does (qpsdm_tables_lerp)."""
+    import torch
+    out = torch.empty_like(lo)
+    rc = _lib.lib().qpsdm_tables_lerp(lo.data_ptr(), hi.data_ptr(), int(lo.numel()), int(line),
+                                      int(line_lo), int(line_hi), out.data_ptr(), None)
+    _lib.check(rc, what="tables_lerp")
+    return out
+
+
+def brick_tables(model, background, *, q_bg: float, table_lines, brick_lines, line_y_of,
+                 fci: int, nxi: int, dxi: float, zmax: float, dzii: float, nxi1: int = 16,
+                 coarse_dx: int, coarse_dy: int, fine_dx: int, fine_dy: int, half_x: float,
+                 half_y: float, h: float, per_source: int = 512, steps: int = 4000,
+                 batch: int = 8192, gate_ms: float = 2.0, device: int = 0, seed: int = 0,
+                 batch_sources: int = 128):
+    """The learned part end to end for a brick of image lines, on one GPU.
+
+    1. Eikonal / t* tables (background-corrected) of the `table_lines` at the
+       coarse surface spacing -- the table files the reference would read --
+       while EikonalSamples draws training samples from every solved batch.
+    2. The network trained on those samples (tcgen05 kernels).
+    3. Its gate errors against the coarse tables of the table lines.
+    4. For every brick line: the plain method's tables (coarse, interpolated
+       between the bracketing table lines as get_ttt_all does, on the device)
+       and the surrogate's tables at the fine surface spacing, gated.
+
+    line_y_of(line) gives the model y of a line.  Returns a dict with the
+    coarse LineTables (with device copies), per brick line the engine table
+    dicts 'plain' and 'dense' (torch data), the trained Surrogate and timings."""
+    import time
+
+    import torch
+
+    from . import tables as T
+    dev = torch.device("cuda", device)
+    bg = Background(background.v0, background.kz, q_bg)
+    sampler = EikonalSamples(bg, q_bg, per_source=per_source, device=device, seed=seed)
+    kw = dict(fci=fci, nxi=nxi, dxi=dxi, zmax=zmax, dzii=dzii, nxi1=nxi1, surf_dx=coarse_dx,
+              surf_dy=coarse_dy, half_x=half_x, half_y=half_y, h=h, batch=batch_sources,
+              device=device, background=background, q_background=q_bg, sampler=sampler,
+              keep_device=True)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    coarse = [T.eikonal_line_tables(model, line_y=line_y_of(L), **kw) for L in table_lines]
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    X, Y = sampler.tensors()
+    sur = train_device(X, Y, bg, steps=steps, batch=batch, seed=seed, device=device)
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
+    err = gate_errors(sur, coarse, [line_y_of(L) for L in table_lines], fci=fci)
+    plain, dense, gated = [], [], 0
+    for L in brick_lines:
+        lo = max([t for t in table_lines if t <= L], default=None)
+        hi = min([t for t in table_lines if t >= L], default=None)
+        if lo is None or hi is None:
+            raise ValueError(f"no table line brackets line {L}")
+        a, b = coarse[table_lines.index(lo)], coarse[table_lines.index(hi)]
+        ct = lerp_device(a.dev["ttt"], b.dev["ttt"], L, lo, hi)
+        cq = lerp_device(a.dev["qqq"], b.dev["qqq"], L, lo, hi)
+        d = a.as_engine_dict()
+        d["ttt"], d["qqq"] = ct, cq
+        plain.append(d)
+        dd, g = dense_tables_device(sur, a, ct, cq, err, fci=fci, line_y=line_y_of(L),
+                                    surf_dx=fine_dx, surf_dy=fine_dy, half_x=half_x,
+                                    half_y=half_y, gate_ms=gate_ms)
+        dense.append(dd)
+        gated += g
+    torch.cuda.synchronize(dev)
+    t3 = time.perf_counter()
+    fd = np.frombuffer(dense[0]["ttt_desc"].tobytes(), DESC_DTYPE)
+    fine_nodes = int((fd["nys"].astype(np.int64) * fd["nxs"]).sum())
+    return dict(coarse=coarse, plain=plain, dense=dense, surrogate=sur,
+                stats=dict(eikonal_s=t1 - t0, train_s=t2 - t1, densify_s=t3 - t2,
+                           sources=sampler.sources, samples=int(X.shape[0]),
+                           train_steps=steps, train_batch=batch,
+                           loss_first_last=[sur.history[0][1], sur.history[-1][1]],
+                           gated_fine_nodes=gated,
+                           fine_nodes=fine_nodes * len(brick_lines),
+                           gated_fraction=gated / max(1, fine_nodes * len(brick_lines)),
+                           max_gate_err_ms=float(err.max().item())))
+
+
+def truth_error_sample(sur: Surrogate, model, background, *, q_bg: float, line_y: float,
+                       plain_tables, fci: int, dxi: float, zmax: float, dzii: float,
+                       fine_dx: int, fine_dy: int, half_x: float, half_y: float, h: float,
+                       ncells: int = 32, seed: int = 0, device: int = 0):
+    """Traveltime error (ms) of the surrogate and of the plain method's
+    tables against the eikonal solver itself: in `ncells` seeded table cells
+    of the line, one seeded node of the cell's fine surface grid is solved on
+    its own local grid (background-corrected as the tables are) and compared
+    at every table point of the cell with the network and with the plain
+    tables (plain_tables: the engine dict of this line's coarse tables,
+    bilinear in surface position as the kernels read them)."""
+    from . import tables as T
+    nxg, nzg = plain_tables["nxg"], plain_tables["nzg"]
+    nxi1, nzi1 = plain_tables["nxi1"], plain_tables["nzi1"]
+    cdesc = np.frombuffer(np.ascontiguousarray(plain_tables["ttt_desc"]).tobytes(), DESC_DTYPE)
+    fdesc, _ = layout(nxg, nzg, nxi1, nzi1, surf_dx=fine_dx, surf_dy=fine_dy, half_x=half_x,
+                      half_y=half_y)
+    geo = LineTables(plain_tables["cdp1"], plain_tables["cdp2"], dxi, 8.0, nxg, nzg, nxi1, nzi1,
+                     dzii, fdesc, np.zeros(0, np.float32), np.zeros(0, np.float32))
+    rng = np.random.default_rng(seed)
+    cells = np.sort(rng.choice(nxg * nzg, min(ncells, nxg * nzg), replace=False))
+    srcs = []
+    for c in cells:
+        xs, ys = cell_surface_nodes(geo, int(c) // nzg, int(c) % nzg, fci)
+        srcs.append((float(rng.choice(xs)), float(line_y + rng.choice(ys))))
+    truth = T.eikonal_cell_values(model, background, q_bg=q_bg, sources=srcs, cells=cells,
+                                  nxg=nxg, nzg=nzg, nxi1=nxi1, nzi1=nzi1,
+                                  x_cdp1=(plain_tables["cdp1"] - fci) * dxi, dxi=dxi,
+                                  dzii=dzii, zmax=zmax, line_y=line_y, h=h, half_x=half_x,
+                                  half_y=half_y, device=device)
+    ttt = plain_tables["ttt"]
+    ttt = ttt.cpu().numpy() if hasattr(ttt, "cpu") else np.asarray(ttt)
+    en, ep = [], []
+    for c, (sx, sy), tt in zip(cells, srcs, truth):
+        ixg, izg = divmod(int(c), nzg)
+        x = ((plain_tables["cdp1"] - fci) + ixg * nxi1 + np.arange(nxi1)) * dxi
+        z = (izg * nzi1 + np.arange(nzi1)) * dzii
+        X, Z = np.meshgrid(x, z, indexing="ij")
+        F = np.stack([np.full(X.size, sx), np.full(X.size, sy), X.ravel(),
+                      np.full(X.size, line_y), Z.ravel()], 1).astype(np.float32)
+        Tn, _ = sur.predict(F)
+        en.append(Tn.reshape(nxi1, nzi1) - tt)
+        # plain tables: bilinear between the cell's coarse surface nodes
+        d = cdesc[c]
+        xc = ((plain_tables["cdp1"] - fci) + ixg * nxi1 + 0.5 * (nxi1 - 1)) * dxi
+        fx = (sx - xc) / float(d["dxs"]) + 0.5 * (int(d["nxs"]) - 1)
+        fy = (sy - line_y) / float(d["dys"]) + 0.5 * (int(d["nys"]) - 1)
+        if not (0 <= fx <= int(d["nxs"]) - 1 and 0 <= fy <= int(d["nys"]) - 1):
+            continue
+        ix, iy = min(int(fx), int(d["nxs"]) - 2), min(int(fy), int(d["nys"]) - 2)
+        wx, wy = fx - ix, fy - iy
+        blk = ttt[int(d["idx"]):int(d["idx"]) + int(d["nys"]) * int(d["nxs"]) * nxi1 * nzi1]
+        blk = blk.reshape(int(d["nys"]), int(d["nxs"]), nxi1, nzi1).astype(np.float64)
+        v = ((1 - wy) * ((1 - wx) * blk[iy, ix] + wx * blk[iy, ix + 1])
+             + wy * ((1 - wx) * blk[iy + 1, ix] + wx * blk[iy + 1, ix + 1]))
+        ep.append(v - tt)
+    en = np.concatenate([e.ravel() for e in en]) * 1e3
+    ep = np.concatenate([e.ravel() for e in ep]) * 1e3
+    return dict(cells=len(cells), values=int(en.size),
+                surrogate_rms_ms=float(np.sqrt(np.mean(en ** 2))),
+                surrogate_max_ms=float(np.abs(en).max()),
+                tables_rms_ms=float(np.sqrt(np.mean(ep ** 2))),
+                tables_max_ms=float(np.abs(ep).max()))

@@ -45,8 +45,8 @@ class Survey:
     # records the whole spread
     gathers: list | None = None
     # Q model: None (constant q), ("layers", z_nodes, q_nodes) with Q linear
-    # between the nodes, or ("cloud", x, y, z, radius, q_cloud) inside a
-    # background of constant q
+    # between the nodes, or ("cloud", x, y, z, (ax, ay, az), q_cloud): an
+    # ellipsoid of semi-axes ax, ay, az (m) inside a background of constant q
     q_model: tuple | None = None
     threshold: float = 600.0   # gain limit of the inverse-Q filter
 
@@ -134,12 +134,16 @@ def config3(seed: int = 0) -> Survey:
                   gathers=gathers, q_model=("layers", zn, qn))
 
 
+CLOUD_AXES = (1200.0, 900.0, 450.0)  # semi-axes (m) of the config-5 gas cloud
+
+
 def config5(seed: int = 0) -> Survey:
     """Large, strongly attenuating case: image 1024x1024x600 at 10 m,
     v(z)=1800+0.5z, nt=3000, dt=2 ms, 25 Hz; 350 shots (14 x 25) x 100x100
-    receivers at 102.4 m = 3.5 M traces; Q = 100 with a gas cloud of Q = 20
-    (radius 800 m, centre 1500 m deep under the middle of the image); 40 dB
-    gain limit of the inverse-Q filter (threshold 100)."""
+    receivers at 102.4 m = 3.5 M traces; Q = 100 with a gas-cloud ellipsoid
+    of Q = 20 (semi-axes 1200 x 900 x 450 m, centre 1500 m deep under the
+    middle of the image; its low velocity is in `config5_model`); 40 dB gain
+    limit of the inverse-Q filter (threshold 100)."""
     sxg = X0 + 366.0 + 731.0 * np.arange(14)
     syg = Y0 + 205.0 + 410.0 * np.arange(25)
     shots = np.array([(x, y) for y in syg for x in sxg])
@@ -150,7 +154,7 @@ def config5(seed: int = 0) -> Survey:
                      [X0 + 7000.0, Y0 + 4500.0, 4500.0]])
     return Survey("c5", 1024, 1024, 600, 10.0, 10.0, 10.0, 3000, 0.002, 1800.0, 0.5,
                   100.0, 25.0, shots, receivers, 3000.0, diff, 20.0, seed=seed,
-                  q_model=("cloud", X0 + 5120.0, Y0 + 5120.0, 1500.0, 800.0, 20.0),
+                  q_model=("cloud", X0 + 5120.0, Y0 + 5120.0, 1500.0, CLOUD_AXES, 20.0),
                   threshold=100.0)
 
 
@@ -193,7 +197,7 @@ def tstar(sv: Survey, px, py, x, y, z, t):
     Constant Q: t / q.  Layers: t times the vertical-time average of 1/Q over
     [0, z] (Q linear between the model's nodes; the integral by 64-point
     midpoint rule).  Cloud: t / q plus (1/q_cloud - 1/q) times the time spent
-    inside the sphere, the chord length over v at the sphere's centre."""
+    inside the ellipsoid, the chord length over v at the cloud's centre."""
     t = np.asarray(t, np.float64)
     if sv.q_model is None:
         return t / sv.q
@@ -209,19 +213,23 @@ def tstar(sv: Survey, px, py, x, y, z, t):
         den = w.sum(-1)
         ratio = np.where(zu > 0, num / np.maximum(den, 1e-30), 1.0 / np.interp(0.0, zn, qn))
         return t * ratio[inv].reshape(z.shape)
-    _, cx, cy, cz, rad, qc = sv.q_model
+    _, cx, cy, cz, axes, qc = sv.q_model
+    ax = np.broadcast_to(np.asarray(axes, float), (3,))
     a = np.stack(np.broadcast_arrays(np.asarray(px, float), np.asarray(py, float),
                                      np.zeros_like(np.asarray(px, float))), -1)
     b = np.stack(np.broadcast_arrays(np.asarray(x, float), np.asarray(y, float),
                                      np.asarray(z, float)), -1)
-    d = b - a
-    L = np.linalg.norm(d, axis=-1)
+    L = np.linalg.norm(b - a, axis=-1)
     c = np.array([cx, cy, cz])
-    # chord of the segment a + s d (s in [0, 1]) inside the sphere
+    # chord of the segment a + s (b - a), s in [0, 1], inside the ellipsoid:
+    # in coordinates scaled by the semi-axes it is a unit sphere, and the
+    # parameter interval is the same in both
+    a, b, c = a / ax, b / ax, c / ax
+    d = b - a
     dd = np.maximum((d * d).sum(-1), 1e-30)
     s0 = ((c - a) * d).sum(-1) / dd
     m = a + s0[..., None] * d
-    h2 = rad * rad - ((m - c) ** 2).sum(-1)
+    h2 = 1.0 - ((m - c) ** 2).sum(-1)
     half = np.sqrt(np.maximum(h2, 0.0) / dd)
     s1, s2 = np.clip(s0 - half, 0.0, 1.0), np.clip(s0 + half, 0.0, 1.0)
     chord = np.where(h2 > 0, (s2 - s1) * L, 0.0)
@@ -291,6 +299,54 @@ def pair_traces(sv: Survey, spos: np.ndarray, gpos: np.ndarray,
     return out
 
 
+def pair_traces_device(sv: Survey, spos: np.ndarray, gpos: np.ndarray, *, device: int = 0,
+                       seed: int = 0, chunk: int = 8192) -> np.ndarray:
+    """pair_traces computed with torch on a GPU (float64 spectra): the same
+    events, amplitudes, t* and dispersion, noise from a seeded torch
+    generator.  For benchmark batches of many traces; returns float32
+    [ntr, ntl] on the host."""
+    import torch
+    dev = torch.device("cuda", device)
+    ntr, n = spos.shape[0], sv.ntl
+    nf = n // 2 + 1
+    f = torch.fft.rfftfreq(n, sv.dt, device=dev, dtype=torch.float64)
+    fpos = torch.clamp(f, min=1e-6)
+    W = torch.from_numpy(ricker_spectrum(np.fft.rfftfreq(n, sv.dt), sv.fpeak)).to(dev)
+    lnf = torch.log(fpos / sv.fpeak)
+    sx, sy = spos[:, 0].astype(np.float64), spos[:, 1].astype(np.float64)
+    gx, gy = gpos[:, 0].astype(np.float64), gpos[:, 1].astype(np.float64)
+    mx, my = 0.5 * (sx + gx), 0.5 * (sy + gy)
+    h = 0.5 * np.hypot(gx - sx, gy - sy)
+    tr1 = traveltime(sv, h, sv.reflector_z)
+    events = [(2.0 * tr1, np.full(ntr, 1.0),
+               tstar(sv, sx, sy, mx, my, sv.reflector_z, tr1)
+               + tstar(sv, gx, gy, mx, my, sv.reflector_z, tr1))]
+    for (dx, dy, dz) in sv.diffractors:
+        ts = traveltime(sv, np.hypot(sx - dx, sy - dy), dz)
+        tg = traveltime(sv, np.hypot(gx - dx, gy - dy), dz)
+        events.append((ts + tg, np.full(ntr, 0.5),
+                       tstar(sv, sx, sy, dx, dy, dz, ts) + tstar(sv, gx, gy, dx, dy, dz, tg)))
+    out = np.empty((ntr, n), np.float32)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(seed))
+    for c0 in range(0, ntr, chunk):
+        c1 = min(ntr, c0 + chunk)
+        spec = torch.zeros((c1 - c0, nf), dtype=torch.complex128, device=dev)
+        for t, a, q in events:
+            tt = torch.from_numpy(t[c0:c1]).to(dev)[:, None]
+            qq = torch.from_numpy(q[c0:c1]).to(dev)[:, None]
+            aa = torch.from_numpy(a[c0:c1]).to(dev)[:, None]
+            amp = aa * W[None, :] * torch.exp(-np.pi * f * qq)
+            phase = 2.0 * fpos * qq * lnf - 2.0 * np.pi * f * tt
+            spec += amp * torch.polar(torch.ones_like(phase), phase)
+        trc = torch.fft.irfft(spec, n=n, dim=1) / sv.dt
+        rms = torch.sqrt(torch.mean(trc * trc, dim=1, keepdim=True)) + 1e-30
+        trc = trc + torch.randn(trc.shape, generator=gen, device=dev, dtype=torch.float64) \
+            * rms * 10 ** (-sv.snr_db / 20.0)
+        out[c0:c1] = trc.float().cpu().numpy()
+    return out
+
+
 def aperture_tables(half_cdps: int, half_lines: int, *, vary: bool = True):
     """aznx1, aznx2, azny1, azny2 (18 azimuth sectors) in image cells.
 
@@ -347,6 +403,35 @@ def config2_model(h: float = 40.0, seed: int = 0, anomalies: bool = True,
     if layered_q:
         for ztop, qv in Q_LAYERS:
             iq[Z >= ztop] = 1.0 / qv
+    return GridModel(v.astype(np.float32), iq.astype(np.float32), h, float(xs[0]),
+                     float(ys[0]), v0, kz)
+
+
+def config5_model(h: float = 50.0, cloud: bool = True, xr=(-2800.0, 13100.0),
+                  yr=(-1400.0, 11700.0), zmax: float = 6200.0, v0: float = 1800.0,
+                  kz: float = 0.5, q: float = 100.0, q_cloud: float = 20.0,
+                  dv: float = -0.2):
+    """Config-5 model on a grid (coordinates relative to the first image cdp
+    and line): v(z) = v0 + kz z, and a gas cloud -- the ellipsoid of
+    `config5`'s Q model (centre under the middle of the image, 1500 m deep,
+    semi-axes CLOUD_AXES) -- with velocity lowered by 20 % and Q = 20 inside,
+    Q = 100 outside; both blend over a shell of 0.8 to 1.2 ellipsoidal radii
+    so that the eikonal grid sees a smooth model."""
+    from .tables import GridModel
+    xs = np.arange(xr[0], xr[1] + h, h, dtype=np.float32)
+    ys = np.arange(yr[0], yr[1] + h, h, dtype=np.float32)
+    zs = np.arange(0.0, zmax + h, h, dtype=np.float32)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    v = v0 + kz * Z
+    iq = np.full(v.shape, 1.0 / q, np.float32)
+    if cloud:
+        ax, ay, az = CLOUD_AXES
+        rho = np.sqrt(((X - 5120.0) / ax) ** 2 + ((Y - 5120.0) / ay) ** 2
+                      + ((Z - 1500.0) / az) ** 2)
+        w = np.clip((1.2 - rho) / 0.4, 0.0, 1.0)
+        w = w * w * (3.0 - 2.0 * w)          # smoothstep: 1 inside, 0 outside
+        v = v * (1.0 + dv * w)
+        iq = (1.0 - w) / q + w / q_cloud
     return GridModel(v.astype(np.float32), iq.astype(np.float32), h, float(xs[0]),
                      float(ys[0]), v0, kz)
 

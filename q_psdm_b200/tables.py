@@ -49,6 +49,7 @@ class LineTables:
     desc: np.ndarray   # DESC_DTYPE [nxg*nzg]
     ttt: np.ndarray    # float32
     qqq: np.ndarray    # float32 (t*, s), same layout and descriptors
+    dev: dict | None = None  # device copies (torch tensors ttt, qqq), when kept
 
     def as_engine_dict(self):
         d = self.desc.view(np.uint8).reshape(-1, 16).copy()
@@ -220,7 +221,8 @@ def eikonal_line_tables(model: GridModel, *, fci: int, nxi: int, dxi: float, zma
                         surf_dy: int, half_x: float, half_y: float, h: float | None = None,
                         batch: int = 128, init_radius: float | None = None,
                         device: int = 0, background: GridModel | None = None,
-                        q_background: float | None = None) -> LineTables:
+                        q_background: float | None = None, sampler=None,
+                        keep_device: bool = False) -> LineTables:
     """Tables of the image line at model y = line_y, computed by the GPU
     eikonal / t* generator (qpsdm_eikonal_solve + qpsdm_eikonal_fill) in the
     reference layout; every distinct surface node of the cells' grids is one
@@ -230,29 +232,14 @@ def eikonal_line_tables(model: GridModel, *, fci: int, nxi: int, dxi: float, zma
     constant Q = q_background) the first-order scheme's systematic error is
     cancelled: T = T_exact(bg) + T(model) - T(bg) and
     t* = t*(model) * t*_exact(bg) / t*(bg), the background solved on the same
-    grids and its exact values from the linear-gradient formula."""
-    if background is not None:
-        kw = dict(fci=fci, nxi=nxi, dxi=dxi, zmax=zmax, line_y=line_y, dzii=dzii, nxi1=nxi1,
-                  surf_dx=surf_dx, surf_dy=surf_dy, half_x=half_x, half_y=half_y, h=h,
-                  batch=batch, init_radius=init_radius, device=device)
-        full = eikonal_line_tables(model, **kw)
-        bg = eikonal_line_tables(background, **kw)
-        v0, kz = background.v0, background.kz
+    grids (batch by batch, next to the model's solve) and the correction
+    applied on the device (qpsdm_eikonal_correct).
 
-        def tfn(px, py, x, z):
-            r = np.hypot(px - x, py)
-            if kz < 1e-9:
-                return np.hypot(r, z) / v0
-            v = v0 + kz * z
-            return np.arccosh(np.maximum(1.0 + kz * kz * (r * r + z * z) / (2 * v0 * v), 1.0)) / kz
-
-        ana = build_line_tables(tfn, lambda *a: tfn(*a) / q_background, fci=fci, nxi=nxi,
-                                dxi=dxi, zmax=zmax, dzii=dzii, nxi1=nxi1, nzi1=full.nzi1,
-                                surf_dx=surf_dx, surf_dy=surf_dy, half_x=half_x, half_y=half_y)
-        full.ttt[:] = (ana.ttt.astype(np.float64) + full.ttt - bg.ttt).astype(np.float32)
-        ratio = np.where(bg.qqq > 0, ana.qqq / np.maximum(bg.qqq, 1e-12), 1.0)
-        full.qqq[:] = (full.qqq * ratio).astype(np.float32)
-        return full
+    sampler(d_T, d_S, d_Tb, d_Sb, grid, d_src, ns): called for every batch
+    of sources while its solved grids are on the device (training samples of
+    the surrogate; d_Tb, d_Sb are None without a background).  keep_device:
+    the returned tables also carry the device copies (tab.dev = dict(ttt=,
+    qqq=) as torch tensors)."""
     import ctypes as C
 
     import torch
@@ -288,22 +275,26 @@ def eikonal_line_tables(model: GridModel, *, fci: int, nxi: int, dxi: float, zma
     gz = int(np.ceil(zmax / h)) + 3
     grid = _lib.EikGrid(gx, gy, gz, h)
     oy = line_y - half_y - 2 * h
-    mdl = _lib.EikModel(model.vel.shape[2], model.vel.shape[1], model.vel.shape[0], model.h,
-                        model.ox, model.oy, model.v0, model.kz)
     fg = _lib.EikFillGeom(nxi1, nnodes, nzg, dxi, dzii, 0.0, line_y)
     dev = torch.device("cuda", device)
-    d_vel = torch.from_numpy(np.ascontiguousarray(model.vel, np.float32)).to(dev)
-    d_iq = torch.from_numpy(np.ascontiguousarray(model.invq, np.float32)).to(dev)
+    models = [model] + ([background] if background is not None else [])
+    d_models = []
+    for m in models:
+        d_models.append((torch.from_numpy(np.ascontiguousarray(m.vel, np.float32)).to(dev),
+                         torch.from_numpy(np.ascontiguousarray(m.invq, np.float32)).to(dev),
+                         _lib.EikModel(m.vel.shape[2], m.vel.shape[1], m.vel.shape[0], m.h,
+                                       m.ox, m.oy, m.v0, m.kz)))
     d_desc = torch.from_numpy(desc.view(np.uint8).copy()).to(dev)
     d_cb = torch.from_numpy(cell_base).to(dev)
     d_nb = torch.from_numpy(node_base).to(dev)
     d_ns = torch.from_numpy(np.array(node_src, np.int32)).to(dev)
-    d_ttt = torch.zeros(tab.ttt.size, dtype=torch.float32, device=dev)
-    d_qqq = torch.zeros(tab.qqq.size, dtype=torch.float32, device=dev)
     n = gx * gy * gz
     nb = min(batch, nsrc)
-    d_T = torch.empty(nb * n, dtype=torch.float32, device=dev)
-    d_S = torch.empty(nb * n, dtype=torch.float32, device=dev)
+    # per model: solved grids and the line's tables
+    d_T = [torch.empty(nb * n, dtype=torch.float32, device=dev) for _ in models]
+    d_S = [torch.empty(nb * n, dtype=torch.float32, device=dev) for _ in models]
+    d_tab = [(torch.zeros(tab.ttt.size, dtype=torch.float32, device=dev),
+              torch.zeros(tab.qqq.size, dtype=torch.float32, device=dev)) for _ in models]
     d_w = torch.empty(4 * nb * n + 4, dtype=torch.float32, device=dev)  # QPSDM_EIK_WORK_FLOATS
     for s0 in range(0, nsrc, nb):
         ns = min(nb, nsrc - s0)
@@ -312,16 +303,110 @@ def eikonal_line_tables(model: GridModel, *, fci: int, nxi: int, dxi: float, zma
         sp[:, 2] = sp[:, 0] - 0.5 * (gx - 1) * h
         sp[:, 3] = oy
         d_sp = torch.from_numpy(sp).to(dev)
-        rc = L.qpsdm_eikonal_solve(d_vel.data_ptr(), d_iq.data_ptr(), C.byref(mdl),
-                                   d_sp.data_ptr(), ns, C.byref(grid), r0, 4 * (gx + gy + gz),
-                                   d_w.data_ptr(), d_T.data_ptr(), d_S.data_ptr(), None)
-        _lib.check(rc, what="eikonal_solve")
-        rc = L.qpsdm_eikonal_fill(d_T.data_ptr(), d_S.data_ptr(), C.byref(grid), d_sp.data_ptr(),
-                                  s0, ns, d_desc.data_ptr(), d_cb.data_ptr(), d_nb.data_ptr(),
-                                  d_ns.data_ptr(), nxg * nzg, C.byref(fg), d_ttt.data_ptr(),
-                                  d_qqq.data_ptr(), None)
-        _lib.check(rc, what="eikonal_fill")
+        for k, (dv, dq, mdl) in enumerate(d_models):
+            rc = L.qpsdm_eikonal_solve(dv.data_ptr(), dq.data_ptr(), C.byref(mdl),
+                                       d_sp.data_ptr(), ns, C.byref(grid), r0,
+                                       4 * (gx + gy + gz), d_w.data_ptr(), d_T[k].data_ptr(),
+                                       d_S[k].data_ptr(), None)
+            _lib.check(rc, what="eikonal_solve")
+            rc = L.qpsdm_eikonal_fill(d_T[k].data_ptr(), d_S[k].data_ptr(), C.byref(grid),
+                                      d_sp.data_ptr(), s0, ns, d_desc.data_ptr(),
+                                      d_cb.data_ptr(), d_nb.data_ptr(), d_ns.data_ptr(),
+                                      nxg * nzg, C.byref(fg), d_tab[k][0].data_ptr(),
+                                      d_tab[k][1].data_ptr(), None)
+            _lib.check(rc, what="eikonal_fill")
+        if sampler is not None:
+            bgT = d_T[1] if background is not None else None
+            bgS = d_S[1] if background is not None else None
+            sampler(d_T[0], d_S[0], bgT, bgS, grid, d_sp, ns)
+    d_ttt, d_qqq = d_tab[0]
+    if background is not None:
+        ln = _lib.SurLine(nxg, nzg, nxi1, nnodes, 0, dxi, dzii, line_y, background.v0,
+                          background.kz, q_background)
+        dsc = np.ascontiguousarray(desc)
+        rc = L.qpsdm_eikonal_correct(C.byref(ln), dsc.ctypes.data, d_ttt.data_ptr(),
+                                     d_qqq.data_ptr(), d_tab[1][0].data_ptr(),
+                                     d_tab[1][1].data_ptr(), int(tab.ttt.size),
+                                     float(q_background), None)
+        _lib.check(rc, what="eikonal_correct")
     torch.cuda.synchronize(dev)
     tab.ttt[:] = d_ttt.cpu().numpy()
     tab.qqq[:] = d_qqq.cpu().numpy()
+    if keep_device:
+        tab.dev = dict(ttt=d_ttt, qqq=d_qqq)
     return tab
+
+
+def eikonal_cell_values(model: GridModel, background: GridModel, *, q_bg: float, sources,
+                        cells, nxg: int, nzg: int, nxi1: int, nzi1: int, x_cdp1: float,
+                        dxi: float, dzii: float, zmax: float, line_y: float, h: float,
+                        half_x: float, half_y: float, device: int = 0):
+    """Traveltime (s) from surface point sources[k] (model x, y) to every
+    table point of cell cells[k] (distinct cells of a line's tables, nxg x nzg
+    cells of nxi1 cdps x nzi1 depth nodes), background-corrected as the
+    tables are: T = T_exact(bg) + T(model) - T(bg).  Returns [k][nxi1][nzi1]
+    float64.  The solves run on local grids as in eikonal_line_tables (one
+    batch), read back through qpsdm_eikonal_fill with one surface node per
+    cell."""
+    import ctypes as C
+
+    import torch
+
+    from . import _lib
+    L = _lib.lib()
+    dev = torch.device("cuda", device)
+    ns = len(sources)
+    ncell = nxg * nzg
+    gx = int(np.ceil((2 * (half_x + nxi1 * dxi) + 4 * h) / h)) + 1
+    gy = int(np.ceil((2 * half_y + 4 * h) / h)) + 1
+    gz = int(np.ceil(zmax / h)) + 3
+    grid = _lib.EikGrid(gx, gy, gz, h)
+    n = gx * gy * gz
+    sp = np.zeros((ns, 4), np.float32)
+    sp[:, 0:2] = np.asarray(sources, np.float32)
+    sp[:, 2] = sp[:, 0] - 0.5 * (gx - 1) * h   # local grids as eikonal_line_tables'
+    sp[:, 3] = line_y - half_y - 2 * h
+    block = nxi1 * nzi1
+    desc = np.zeros(ncell, DESC_DTYPE)
+    for c in range(ncell):
+        desc[c] = (c * block, 1, 1, 1, 1)
+    node_src = np.full(ncell, -(1 << 30), np.int32)
+    node_src[np.asarray(cells, int)] = np.arange(ns, dtype=np.int32)
+    d_sp = torch.from_numpy(sp).to(dev)
+    d_desc = torch.from_numpy(desc.view(np.uint8).copy()).to(dev)
+    d_cb = torch.from_numpy(np.arange(ncell + 1, dtype=np.int64) * block).to(dev)
+    d_nb = torch.from_numpy(np.arange(ncell + 1, dtype=np.int32)).to(dev)
+    d_ns = torch.from_numpy(node_src).to(dev)
+    fg = _lib.EikFillGeom(nxi1, nzi1, nzg, dxi, dzii, x_cdp1, line_y)
+    d_w = torch.empty(4 * ns * n + 4, dtype=torch.float32, device=dev)  # QPSDM_EIK_WORK_FLOATS
+    out = []
+    for m in (model, background):
+        dv = torch.from_numpy(np.ascontiguousarray(m.vel, np.float32)).to(dev)
+        dq = torch.from_numpy(np.ascontiguousarray(m.invq, np.float32)).to(dev)
+        mdl = _lib.EikModel(m.vel.shape[2], m.vel.shape[1], m.vel.shape[0], m.h, m.ox, m.oy,
+                            m.v0, m.kz)
+        d_T = torch.empty(ns * n, dtype=torch.float32, device=dev)
+        d_S = torch.empty(ns * n, dtype=torch.float32, device=dev)
+        _lib.check(L.qpsdm_eikonal_solve(dv.data_ptr(), dq.data_ptr(), C.byref(mdl),
+                                         d_sp.data_ptr(), ns, C.byref(grid), 3.0 * h,
+                                         4 * (gx + gy + gz), d_w.data_ptr(), d_T.data_ptr(),
+                                         d_S.data_ptr(), None), what="eikonal_solve")
+        tt = torch.zeros(ncell * block, dtype=torch.float32, device=dev)
+        qq = torch.zeros(ncell * block, dtype=torch.float32, device=dev)
+        _lib.check(L.qpsdm_eikonal_fill(d_T.data_ptr(), d_S.data_ptr(), C.byref(grid),
+                                        d_sp.data_ptr(), 0, ns, d_desc.data_ptr(),
+                                        d_cb.data_ptr(), d_nb.data_ptr(), d_ns.data_ptr(), ncell,
+                                        C.byref(fg), tt.data_ptr(), qq.data_ptr(), None),
+                   what="eikonal_fill")
+        out.append(tt.cpu().numpy().reshape(ncell, nxi1, nzi1).astype(np.float64))
+    from .surrogate import background_time
+    res = []
+    for k, c in enumerate(cells):
+        ixg, izg = divmod(int(c), nzg)
+        x = x_cdp1 + (ixg * nxi1 + np.arange(nxi1)) * dxi
+        z = (izg * nzi1 + np.arange(nzi1)) * dzii
+        X, Z = np.meshgrid(x, z, indexing="ij")
+        r = np.hypot(X - sources[k][0], line_y - sources[k][1])
+        ana = background_time(r, Z, background.v0, background.kz)
+        res.append(ana + out[0][int(c)] - out[1][int(c)])
+    return res

@@ -26,11 +26,31 @@ def test_config5_gas_cloud():
     sv = synth.config5(0)
     assert sv.ntraces == 3_500_000 and sv.threshold == 100.0
     cx, cy = synth.X0 + 5120.0, synth.Y0 + 5120.0
-    # vertical path through the whole cloud (1600 m) against one beside it
+    # vertical path through the whole ellipsoid (2 x 450 m) against one beside it
     through = synth.tstar(sv, cx, cy, cx, cy, 3000.0, 1.0)
     beside = synth.tstar(sv, cx + 3000.0, cy, cx + 3000.0, cy, 3000.0, 1.0)
     assert abs(beside - 0.01) < 1e-12
-    assert abs(through - (0.01 + 1600.0 / 2550.0 * (1 / 20 - 1 / 100))) < 1e-9
+    assert abs(through - (0.01 + 900.0 / 2550.0 * (1 / 20 - 1 / 100))) < 1e-9
+    ax = synth.CLOUD_AXES[0]
+    # a straight path from (cx - L, 0) down to (cx + L, 3000): the chord through
+    # the cloud follows from the ellipsoid's equation, here checked numerically
+    L = 1500.0
+    a, b = np.array([cx - L, cy, 0.0]), np.array([cx + L, cy, 3000.0])
+    s = np.linspace(0, 1, 400001)
+    p = a + s[:, None] * (b - a)
+    inside = (((p[:, 0] - cx) / ax) ** 2 + ((p[:, 2] - 1500.0) / synth.CLOUD_AXES[2]) ** 2) <= 1
+    chord = inside.mean() * np.linalg.norm(b - a)
+    got = synth.tstar(sv, a[0], a[1], b[0], b[1], b[2], 1.0)
+    assert abs(got - (0.01 + chord / 2550.0 * (1 / 20 - 1 / 100))) < 2e-6
+
+
+def test_config5_model_cloud():
+    m = synth.config5_model(h=100.0)
+    iz, iy, ix = int(1500 / 100), int((5120 - m.oy) / 100), int((5120 - m.ox) / 100)
+    v_in, q_in = m.vel[iz, iy, ix], 1.0 / m.invq[iz, iy, ix]
+    assert abs(v_in - 0.8 * (1800 + 0.5 * 1500)) < 1.0 and abs(q_in - 20.0) < 1e-3
+    far = m.vel[iz, iy, 0], 1.0 / m.invq[iz, iy, 0]
+    assert abs(far[0] - (1800 + 0.5 * 1500)) < 1e-3 and abs(far[1] - 100.0) < 1e-3
 
 
 def test_accuracy_samples_build():

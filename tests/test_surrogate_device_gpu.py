@@ -1,0 +1,136 @@
+"""The surrogate's device pipeline: training samples drawn from the eikonal
+solver's grids, the gate and the surrogate's tables, all on the GPU.
+
+* With the background as the model every training target is zero: the
+  sampler applies the same background correction as the tables.
+* Trained on samples of the solves of two table lines, the network's tables
+  of a line between them (at a four times finer surface spacing) are closer
+  to the eikonal solver itself than the plain method's tables of that line
+  (interpolated between the table lines as get_ttt_all does, bilinear in
+  surface position).
+* With an untrained network every patch fails the 2 ms gate and the
+  surrogate's tables are the bilinear interpolation of the plain tables.
+* The device interpolation between lines equals the reference's float
+  arithmetic (a c1 + b c2, no fused multiply-add) bit for bit.
+"""
+import numpy as np
+import pytest
+
+from q_psdm_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+BOX = dict(xr=(-1300, 2600), yr=(-1300, 2600), zmax=1100, v0=2000.0, kz=0.6, q=60.0)
+GEOM = dict(fci=1, nxi=128, dxi=10.0, zmax=990.0, dzii=40.0, nxi1=16, half_x=800.0,
+            half_y=480.0, h=40.0)
+ANOMALIES = ((500.0, 700.0, 450.0, 200.0, 0.15), (900.0, 560.0, 700.0, 250.0, -0.12))
+
+
+def _model(h):
+    m = synth.config2_model(h=h, anomalies=False, layered_q=True, **BOX)
+    nz, ny, nx = m.vel.shape
+    Z, Y, X = np.meshgrid(np.arange(nz) * h, m.oy + np.arange(ny) * h, m.ox + np.arange(nx) * h,
+                          indexing="ij")
+    for ax, ay, az, rad, amp in ANOMALIES:
+        m.vel *= (1 + amp * np.exp(-((X - ax) ** 2 + (Y - ay) ** 2 + (Z - az) ** 2)
+                                   / rad ** 2)).astype(np.float32)
+    return m
+
+
+def _bg(h):
+    return synth.config2_model(h=h, anomalies=False, layered_q=False, **BOX)
+
+
+def test_samples_of_the_background_are_zero(cuda):
+    from q_psdm_b200 import surrogate as S
+    from q_psdm_b200 import tables as T
+    bg = _bg(40.0)
+    back = S.Background(BOX["v0"], BOX["kz"], BOX["q"])
+    smp = S.EikonalSamples(back, BOX["q"], per_source=512)
+    T.eikonal_line_tables(bg, line_y=640.0, surf_dx=320, surf_dy=320, background=bg,
+                          q_background=BOX["q"], sampler=smp, **GEOM)
+    X, Y = smp.tensors()
+    assert X.shape[0] == 512 * smp.sources and smp.sources > 0
+    y = Y.cpu().numpy()
+    assert np.isfinite(y).all()
+    # T - T_bgsolve = 0 and t* (T_bg/q) / t* = T_bg/q up to the solver's
+    # stopping tolerance (1e-7 relative; two solves of one model relax in
+    # different orders)
+    assert np.abs(y[:, 0]).max() < 1e-3 and np.abs(y[:, 1]).max() < 1e-3
+    x = X.cpu().numpy()
+    assert x[:, 4].min() >= 0.0 and x[:, 4].max() > 900.0      # depths over the grid
+
+
+@pytest.fixture(scope="module")
+def brick():
+    from q_psdm_b200 import surrogate as S
+    model, bg = _model(40.0), _bg(40.0)
+    out = S.brick_tables(model, bg, q_bg=BOX["q"], table_lines=[48, 80], brick_lines=[64],
+                         line_y_of=lambda L: 10.0 * L, coarse_dx=160, coarse_dy=160,
+                         fine_dx=40, fine_dy=40, steps=3000, **GEOM)
+    out["model"], out["bg"] = model, bg
+    return out
+
+
+def test_training_converged(cuda, brick):
+    st = brick["stats"]
+    print(st)
+    a, b = st["loss_first_last"]
+    assert b < 1e-2 * a
+    assert st["samples"] == 512 * st["sources"]
+
+
+def test_surrogate_tables_beat_the_plain_tables(cuda, brick):
+    from q_psdm_b200 import surrogate as S
+    g = {k: GEOM[k] for k in ("fci", "dxi", "zmax", "dzii", "half_x", "half_y", "h")}
+    e = S.truth_error_sample(brick["surrogate"], brick["model"], brick["bg"], q_bg=BOX["q"],
+                             line_y=640.0, plain_tables=brick["plain"][0], fine_dx=40,
+                             fine_dy=40, ncells=8, seed=1, **g)
+    print(f"traveltime vs eikonal at line 64 (ms rms/max): surrogate "
+          f"{e['surrogate_rms_ms']:.3f}/{e['surrogate_max_ms']:.2f}, plain tables "
+          f"{e['tables_rms_ms']:.3f}/{e['tables_max_ms']:.2f} ({e['values']} values)")
+    assert e["surrogate_rms_ms"] < 0.5 * e["tables_rms_ms"]
+    assert e["surrogate_max_ms"] < e["tables_max_ms"]
+
+
+def test_untrained_network_keeps_the_tables(cuda, brick):
+    from q_psdm_b200 import surrogate as S
+    sur = brick["surrogate"]
+    raw = S.Surrogate(S.Mlp(0, params=S.init_params(9, out_scale=1e3)), sur.bg, [])
+    raw.mlp.set_scaling(sur.mlp.shift, sur.mlp.scale)
+    coarse = brick["coarse"][0]
+    err = S.gate_errors(raw, brick["coarse"], [480.0, 800.0])
+    assert float(err.min().item()) > 2.0
+    plain = brick["plain"][0]
+    dense, gated = S.dense_tables_device(raw, coarse, plain["ttt"], plain["qqq"], err, fci=1,
+                                         line_y=640.0, surf_dx=40, surf_dy=40,
+                                         half_x=GEOM["half_x"], half_y=GEOM["half_y"])
+    fd = np.frombuffer(dense["ttt_desc"].tobytes(), S.DESC_DTYPE)
+    assert gated == int((fd["nys"].astype(np.int64) * fd["nxs"]).sum())
+    # bilinear resampling of the plain tables on the host
+    host = coarse.__class__(coarse.cdp1, coarse.cdp2, coarse.dx, coarse.dz, coarse.nxg,
+                            coarse.nzg, coarse.nxi1, coarse.nzi1, coarse.dzii, coarse.desc,
+                            plain["ttt"].cpu().numpy(), plain["qqq"].cpu().numpy())
+    want = S.coarse_to_fine(host, fci=1, surf_dx=40, surf_dy=40, half_x=GEOM["half_x"],
+                            half_y=GEOM["half_y"])
+    got_t = dense["ttt"].cpu().numpy()
+    assert np.abs(got_t - want.ttt).max() <= 2e-6 * np.abs(want.ttt).max()
+    got_q = dense["qqq"].cpu().numpy()
+    assert np.abs(got_q - want.qqq).max() <= 2e-6 * np.abs(want.qqq).max()
+    raw.mlp.close()
+
+
+def test_device_lerp_matches_the_reference_arithmetic(cuda):
+    import torch
+
+    from q_psdm_b200 import surrogate as S
+    rng = np.random.default_rng(4)
+    a = rng.uniform(0.1, 3.0, 100003).astype(np.float32)
+    b = rng.uniform(0.1, 3.0, 100003).astype(np.float32)
+    for line, lo, hi in ((505, 500, 510), (503, 500, 507), (500, 500, 510), (507, 507, 507)):
+        got = S.lerp_device(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), line, lo,
+                            hi).cpu().numpy()
+        c2 = np.float32(0.0 if hi == lo else 1.0 * (line - lo) / (hi - lo))
+        c1 = np.float32(1.0 - np.float64(c2))
+        want = a * c1 + b * c2          # float32 products and sum, as the reference
+        assert np.array_equal(got, want), (line, lo, hi)
