@@ -470,7 +470,8 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     for k in range(max(warmup, nbatch + 1)):   # every batch eager once, then captured
         eng.submit_device(drecs[k % nbatch].data_ptr(), ntr)
     torch.cuda.synchronize()
-    nacc0, npt0 = eng.counters()
+    st0 = eng.stats()
+    nacc0, npt0 = st0["accepted"], st0["point_traces"]
     eng.profile(True)
     if dist:
         dist.barrier()
@@ -489,8 +490,10 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     torch.cuda.synchronize()
     ck = clk.stop() if clocks else None
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    nacc1, npt1 = eng.counters()
+    st1 = eng.stats()
+    nacc1, npt1 = st1["accepted"], st1["point_traces"]
     npt = npt1 - npt0
+    pairs = {k: (st1[k] - st0[k]) / steps for k in ("tile_decided", "imaged")}
     kt = _kernel_times(eng, _lib)  # launch counts (graph replays included)
     eng.profile(False)
     kms = {k: v[0] / steps for k, v in kt.items()}
@@ -511,6 +514,9 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
            "point_traces_per_step": npt_all / steps, "clocks": ck,
            "kernel_ms_per_step": kms,
            "gate_accepted_per_step": (nacc1 - nacc0) / steps,
+           "pairs_per_step": dict(pairs, point_traces=npt / steps,
+                                  kept_fraction=1.0 - pairs["tile_decided"] / max(npt / steps, 1),
+                                  imaged_fraction=pairs["imaged"] / max(npt / steps, 1)),
            "launches": int(sum(v[1] for v in kt.values())),
            "image_ms_per_launch": img_launch,
            "image_launches": kt["image"][1], "npt": npt}
@@ -565,13 +571,17 @@ def run_ours(args, rank, world, dist):
     wl = WORKLOADS[args.config](rank, tile, args.variant, args.train_steps)
     if args.batches:
         wl.nbatch = args.batches
+    if args.lines and hasattr(wl, "NLINES"):
+        wl.NLINES = args.lines
     t0 = time.perf_counter()
     wl.setup(dev)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()   # the table generator's scratch
     setup_s = time.perf_counter() - t0
     head = run_form(args.form, wl, args, dev, dist, steps=args.steps, warmup=args.warmup,
                     e2e=not args.no_e2e)
     keys = ("value", "ms_per_step", "point_traces_per_step", "kernel_ms_per_step",
-            "gate_accepted_per_step")
+            "gate_accepted_per_step", "pairs_per_step")
     forms = {args.form: {k: head[k] for k in keys}}
     if args.form == "batched":
         pl = run_form("plain", wl, args, dev, dist, steps=max(3, args.steps // 2),
@@ -595,6 +605,11 @@ def run_ours(args, rank, world, dist):
                             "of a smaller capture (profiles/) x this launch's point-traces",
             "flop_per_point_trace": F_PT[args.form],
             "point_traces_per_launch": npt_launch,
+            "kept_fraction": head["pairs_per_step"]["kept_fraction"],
+            "imaged_fraction": head["pairs_per_step"]["imaged_fraction"],
+            "flop_note": "64 flop credited per point-trace; pairs decided for a whole tile "
+                         "(1 - kept_fraction) execute none of them, pairs that fail the dip "
+                         "test or the time window (kept - imaged) about half",
             "kernel_ms_per_launch": head["image_ms_per_launch"],
             "peak_source": "measured in this run: cuBLAS SGEMM 8192^3, TF32 off (of measured)",
             "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),

@@ -252,6 +252,14 @@ int qpsdm_tuning_info(qpsdm_engine *e, int *variant, int *tile_z, int *tile_x,
 int qpsdm_get_counters(qpsdm_engine *e, int64_t *traces_accepted,
                        int64_t *point_traces);
 
+/* Counters since begin_offset, up to n of: [0] traces accepted by the gate,
+ * [1] point-traces, [2] point-traces decided for a whole image tile by the
+ * batched kernel (members whose dip test fails at every point of the tile;
+ * 0 in the plain form), [3] point-traces imaged (past the dip test and the
+ * time window; 0 in compat mode).  Returns the number of counters (4).  No
+ * counterpart in the reference, which counts nothing. */
+int qpsdm_get_stats(qpsdm_engine *e, int64_t *out, int n);
+
 /* Per-trace spectra of the last submit (re, im: [ntr][2*nww], rejected
  * traces untouched), as psdm_kernel leaves them in red/imd
  * (src/q-psdm.cu:2186-2219).  Device pointers, valid until the next submit. */

@@ -47,7 +47,7 @@ struct qpsdm_engine {
   int *d_ints = nullptr;
   float *d_geom = nullptr;
   unsigned *d_err = nullptr;
-  unsigned long long *d_npt = nullptr;
+  unsigned long long *d_npt = nullptr;  // point-traces, decided per tile, imaged
   unsigned long long *d_nacc = nullptr;  // (trace, line) pairs the gate accepted
   // lines of the image brick
   bool line_set = false;
@@ -187,8 +187,8 @@ extern "C" int qpsdm_engine_create(const qpsdm_static_params *p,
   CKC(cudaMalloc(&e->d_geom, sizeof(float) * kGateF * e->p.max_batch));
   CKC(cudaMalloc(&e->d_err, sizeof(unsigned)));
   CKC(cudaMemset(e->d_err, 0, sizeof(unsigned)));
-  CKC(cudaMalloc(&e->d_npt, sizeof(unsigned long long)));
-  CKC(cudaMemset(e->d_npt, 0, sizeof(unsigned long long)));
+  CKC(cudaMalloc(&e->d_npt, 3 * sizeof(unsigned long long)));
+  CKC(cudaMemset(e->d_npt, 0, 3 * sizeof(unsigned long long)));
   CKC(cudaMalloc(&e->d_nacc, sizeof(unsigned long long)));
   CKC(cudaMemset(e->d_nacc, 0, sizeof(unsigned long long)));
   if (e->p.mode == QPSDM_MODE_PHYSICS) {
@@ -303,7 +303,7 @@ extern "C" int qpsdm_begin_offset(qpsdm_engine *e, const qpsdm_offset_params *o)
   if ((rc = grow(e, &e->d_img, &e->img_cap, nimg))) return rc;
   if (o->zero_image || realloc_img || !e->offset_set)
     CK(cudaMemsetAsync(e->d_img, 0, sizeof(float) * nimg, e->s_comp));
-  CK(cudaMemsetAsync(e->d_npt, 0, sizeof(unsigned long long), e->s_comp));
+  CK(cudaMemsetAsync(e->d_npt, 0, 3 * sizeof(unsigned long long), e->s_comp));
   CK(cudaMemsetAsync(e->d_nacc, 0, sizeof(unsigned long long), e->s_comp));
   if (e->p.mode == QPSDM_MODE_PHYSICS) {
     rc = physics_begin_offset(e->phys, e->p, *o, (int)e->lines.size(), e->s_comp, &e->err);
@@ -607,6 +607,17 @@ extern "C" int qpsdm_get_counters(qpsdm_engine *e, int64_t *acc, int64_t *npt) {
   if (npt) *npt = (int64_t)v;
   if (acc) *acc = (int64_t)na;
   return QPSDM_OK;
+}
+
+extern "C" int qpsdm_get_stats(qpsdm_engine *e, int64_t *out, int n) {
+  if (!e || (!out && n > 0) || n < 0) return QPSDM_EINVAL;
+  DeviceGuard g(e->device);
+  CK(cudaStreamSynchronize(e->s_comp));
+  unsigned long long v[4] = {0, 0, 0, 0};
+  CK(cudaMemcpy(&v[0], e->d_nacc, sizeof(v[0]), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&v[1], e->d_npt, 3 * sizeof(v[0]), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n && i < 4; ++i) out[i] = (int64_t)v[i];
+  return 4;
 }
 
 extern "C" int qpsdm_spectra_device_ptr(qpsdm_engine *e, float **d_re, float **d_im) {

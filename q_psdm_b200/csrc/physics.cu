@@ -746,6 +746,31 @@ __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
 
 constexpr int kPhysBz = 32, kPhysBx = 8, kPhysChunk = 256;
 
+// Per-launch counters cnt[0..2] += the block's per-thread counts: point-traces
+// (pairs in the aperture with table values at both ends), of which decided
+// for a whole tile (members dropped before any point saw them), and imaged
+// (past the dip test and the time window).  One atomic per counter and block.
+__device__ __forceinline__ void add_counts(unsigned long long *cnt, unsigned long long *s,
+                                           unsigned c0, unsigned c1, unsigned c2) {
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int nthr = blockDim.x * blockDim.y;
+  if (tid < 3) s[tid] = 0;
+  __syncthreads();
+  for (int off = 16; off > 0; off >>= 1) {
+    c0 += __shfl_down_sync(0xffffffffu, c0, off);
+    c1 += __shfl_down_sync(0xffffffffu, c1, off);
+    c2 += __shfl_down_sync(0xffffffffu, c2, off);
+  }
+  if ((tid & 31) == 0) {
+    if (c0) atomicAdd(&s[0], (unsigned long long)c0);
+    if (c1) atomicAdd(&s[1], (unsigned long long)c1);
+    if (c2) atomicAdd(&s[2], (unsigned long long)c2);
+  }
+  __syncthreads();
+  if (tid < 3 && s[tid]) atomicAdd(cnt + tid, s[tid]);
+  (void)nthr;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kPhysBz *kPhysBx)
     k_image_plain(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
@@ -757,13 +782,12 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
                   unsigned long long *npt) {
   __shared__ float4 s_geom[kPhysChunk];
   __shared__ int4 s_rng[kPhysChunk];
-  __shared__ unsigned long long s_cnt;
+  __shared__ unsigned long long s_cnt[3];
   const int tid = threadIdx.y * kPhysBz + threadIdx.x;
   const int izi = blockIdx.x * kPhysBz + threadIdx.x;
   const int ixb = blockIdx.y * kPhysBx + threadIdx.y;
   const bool live = izi < a.nzi && ixb < a.nxb;
   const int ixi = ixb + a.ixstart;
-  if (tid == 0) s_cnt = 0;
 
   // per-point constants: cells, depth weights, dip limits
   PointCells pc;
@@ -792,7 +816,7 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
   // source terms are reused while consecutive traces share a source
   float last_sx = NAN, last_sy = NAN, ts = 0.f, qs = 0.f;
   bool s_ok = false;
-  unsigned cnt = 0;
+  unsigned cnt = 0, cimg = 0;
 
   for (int c0 = 0; c0 < ntr; c0 += kPhysChunk) {
     const int nc = min(kPhysChunk, ntr - c0);
@@ -836,6 +860,7 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
       const float ft = t * inv_dt1;
       const int it1 = (int)ft;
       if (!(it1 > 0 && it1 + 1 < a.nt)) continue;
+      ++cimg;
       const float wt = ft - (float)it1;
       float fb = fminf(fmaxf((qs + qg) * inv_dts, 0.0f), (float)(a.nbins - 1));
       const int b0 = min((int)fb, a.nbins - 2);
@@ -864,12 +889,7 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
     img[(size_t)ixb * a.nzi + izi] = acc;
     if (comp) comp[(size_t)ixb * a.nzi + izi] = cmp;
   }
-  if (npt) {
-    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
-    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&s_cnt, (unsigned long long)cnt);
-    __syncthreads();
-    if (tid == 0 && s_cnt) atomicAdd(npt, s_cnt);
-  }
+  if (npt) add_counts(npt, s_cnt, cnt, 0u, cimg);
 }
 
 // ---------------------------------------------------------------------------
@@ -1076,14 +1096,13 @@ __global__ void __launch_bounds__(TZ *TX, MB)
   __shared__ TileGrid s_tg;         // the tile's shared surface grid (uniform tiles)
   __shared__ int s_tgw;             // the thread that writes it
   __shared__ int s_tile;
-  __shared__ unsigned long long s_cnt;
+  __shared__ unsigned long long s_cnt[3];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int lz = tid % TZ, lx = tid / TZ;
   const int nsrc = *nsrc_ptr;
   const float inv_dt1 = 1.0f / a.dt1, inv_dts = 1.0f / a.dtstar;
   const size_t pstride = (size_t)a.nbins * a.nt;
-  if (tid == 0) s_cnt = 0;
-  unsigned cnt = 0;
+  unsigned cnt = 0, cdrop = 0, cimg = 0;
   for (;;) {
     __syncthreads();
     if (tid == 0) {
@@ -1218,7 +1237,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
                 const bool cov = tile_covers(s_tg, sp) && tile_covers(s_tg, gp);
                 keep = cov && tile_keep(sp, gp, box);
                 // dropped by the dip bound: its in-aperture points still count
-                if (cov && !keep) cnt += s_col[hi - ixi_lo + 1] - s_col[lo - ixi_lo];
+                if (cov && !keep) cdrop += s_col[hi - ixi_lo + 1] - s_col[lo - ixi_lo];
               } else {
                 keep = true;  // several cells in the tile: every point decides alone
               }
@@ -1342,6 +1361,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
               if (std::is_same<T, __half>::value)  // 2^e from the record's exponent bits
                 fac[u] *= __int_as_float((int)((((unsigned)mi[u].y >> 24) - 1u) << 23));
               on[u] = true;
+              ++cimg;
             }
             float smp[U];
 #pragma unroll
@@ -1378,12 +1398,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
       if (comp) comp[(size_t)ixb * a.nzi + izi] = cmp;
     }
   }
-  if (npt) {
-    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
-    if ((tid & 31) == 0 && cnt) atomicAdd(&s_cnt, (unsigned long long)cnt);
-    __syncthreads();
-    if (tid == 0 && s_cnt) atomicAdd(npt, s_cnt);
-  }
+  if (npt) add_counts(npt, s_cnt, cnt + cdrop, cdrop, cimg);
 }
 
 static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p) {

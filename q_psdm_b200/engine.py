@@ -268,6 +268,15 @@ class Engine:
         self._ck(lib().qpsdm_get_counters(self.h, C.byref(a), C.byref(n)), "get_counters")
         return a.value, n.value
 
+    def stats(self):
+        """dict(accepted, point_traces, tile_decided, imaged) since begin_offset."""
+        a = np.zeros(4, np.int64)
+        rc = lib().qpsdm_get_stats(self.h, a.ctypes.data, 4)
+        if rc < 0 or rc != 4:
+            self._ck(rc if rc else 1, "get_stats")
+        return dict(accepted=int(a[0]), point_traces=int(a[1]), tile_decided=int(a[2]),
+                    imaged=int(a[3]))
+
     def spectra_device_ptrs(self):
         r, i = C.c_void_p(), C.c_void_p()
         self._ck(lib().qpsdm_spectra_device_ptr(self.h, C.byref(r), C.byref(i)), "spectra")
