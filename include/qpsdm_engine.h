@@ -265,6 +265,15 @@ int qpsdm_get_stats(qpsdm_engine *e, int64_t *out, int n);
  * (src/q-psdm.cu:2186-2219).  Device pointers, valid until the next submit. */
 int qpsdm_spectra_device_ptr(qpsdm_engine *e, float **d_re, float **d_im);
 
+/* Physics mode: the t*-binned compensated panels of the last submit,
+ * [ntr][nbins][nffti] in the engine's panel type (the plain form holds the
+ * last image line's accepted traces, the batched form every trace some line
+ * of the brick accepted), and for FP16 panels the per-trace sample
+ * multipliers [ntr] (powers of two).  Device pointers, valid until the next
+ * submit.  The panels stand where psdm_kernel leaves its spectra (red/imd,
+ * src/q-psdm.cu:2186-2219). */
+int qpsdm_panels_device_ptr(qpsdm_engine *e, void **d_panels, float **d_pscale);
+
 /* Per-trace gate results of the last submit: [ntr][8] ints
  * (status, cdpx, cdpy, iaz, ixi1, ixi2, ntibeg, izimin) and [ntr][4] floats
  * (sx, sy, gx, gy relative to fxi, cyi).  Device pointers. */

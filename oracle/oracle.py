@@ -313,3 +313,43 @@ def physics_image(pp: PhysParams, geom, ints3, panels, dips, tables, img=None):
                         np.ascontiguousarray(tables["ttt"], np.float32), qtab.ctypes.data,
                         np.ascontiguousarray(tables["qqq"], np.float32), img, C.byref(npt))
     return img, int(npt.value)
+
+
+class P32(C.Structure):
+    """Parameters of orc_image_plain_fp32 (oracle/physics_fp32.c)."""
+    _fields_ = [
+        ("nzi", C.c_int), ("nxb", C.c_int), ("ixstart", C.c_int), ("nt", C.c_int),
+        ("nbins", C.c_int),
+        ("dt1", C.c_float), ("dxi", C.c_float), ("dzi", C.c_float),
+        ("taperzone", C.c_float), ("dtstar", C.c_float), ("dzii", C.c_float),
+        ("tcdp1", C.c_int), ("tcdp2", C.c_int),
+        ("nxg", C.c_int), ("nzg", C.c_int), ("nxi1", C.c_int), ("nzi1", C.c_int),
+    ]
+
+
+def image_plain_fp32(p: P32, ints, geom, panels, dips, tables, img=None):
+    """The FP32 restatement of the engine's plain physics kernel
+    (physics_fp32.c): image [nxb*nzi] float32 accumulated in place, and the
+    (point-traces, imaged) counts.  ints [ntr][8] and geom [ntr][4] are the
+    gate's results of every trace; panels [ntr][nbins][nt] float32."""
+    L = lib()
+    if not hasattr(L, "_p32_bound"):
+        L.orc_image_plain_fp32.argtypes = [C.POINTER(P32), C.c_int, _i32p, _f32p, _f32p,
+                                           _f32p, C.c_size_t, C.c_void_p, _f32p, C.c_void_p,
+                                           _f32p, _f32p, C.POINTER(C.c_longlong)]
+        L.orc_image_plain_fp32.restype = None
+        L._p32_bound = True
+    if img is None:
+        img = np.zeros(p.nxb * p.nzi, np.float32)
+    dtab = np.ascontiguousarray(tables["ttt_desc"]).view(np.uint8)
+    qtab = np.ascontiguousarray(tables["qqq_desc"]).view(np.uint8)
+    dips = np.ascontiguousarray(np.stack([np.asarray(d, np.float32).ravel() for d in dips]))
+    counts = (C.c_longlong * 2)(0, 0)
+    L.orc_image_plain_fp32(C.byref(p), int(np.asarray(geom).shape[0]),
+                           np.ascontiguousarray(ints, np.int32).ravel(),
+                           np.ascontiguousarray(geom, np.float32).ravel(),
+                           np.ascontiguousarray(panels, np.float32).ravel(), dips.ravel(),
+                           dips.shape[1], dtab.ctypes.data,
+                           np.ascontiguousarray(tables["ttt"], np.float32), qtab.ctypes.data,
+                           np.ascontiguousarray(tables["qqq"], np.float32), img, counts)
+    return img, int(counts[0]), int(counts[1])

@@ -124,6 +124,7 @@ SYMBOLS = [
     ("qpsdm_profile_get", _I, [_P, _I, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("qpsdm_get_counters", _I, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("qpsdm_get_stats", _I, [_P, _P, _I]),
+    ("qpsdm_panels_device_ptr", _I, [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     ("qpsdm_spectra_device_ptr", _I, [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     ("qpsdm_gate_device_ptr", _I, [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     ("qpsdm_fft_r2c", _I, [_P, _I, _I, _P, _P]),

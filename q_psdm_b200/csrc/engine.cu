@@ -620,6 +620,13 @@ extern "C" int qpsdm_get_stats(qpsdm_engine *e, int64_t *out, int n) {
   return 4;
 }
 
+extern "C" int qpsdm_panels_device_ptr(qpsdm_engine *e, void **d_panels, float **d_pscale) {
+  if (!e || !d_panels || !d_pscale) return QPSDM_EINVAL;
+  if (!e->phys) return fail(e, QPSDM_ESTATE, "panels exist in physics mode only");
+  physics_panels(e->phys, d_panels, d_pscale);
+  return QPSDM_OK;
+}
+
 extern "C" int qpsdm_spectra_device_ptr(qpsdm_engine *e, float **d_re, float **d_im) {
   if (!e || !d_re || !d_im) return QPSDM_EINVAL;
   *d_re = e->d_re;

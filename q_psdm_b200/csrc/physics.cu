@@ -584,6 +584,20 @@ __device__ __forceinline__ bool grid_pos(float px, float py, float xc, float rdx
   return fx >= 0.0f && fx <= (float)(nxs - 1) && fy >= 0.0f && fy <= (float)(nys - 1);
 }
 
+// a + w (b - a) as one fused multiply-add (the form every table and sample
+// interpolation of the image kernels takes; the FP32 oracle repeats it).
+__device__ __forceinline__ float lerp(float a, float b, float w) {
+  return __fmaf_rn(w, __fsub_rn(b, a), a);
+}
+
+// Bilinear value of a 2 x 2 node block starting at tab + base.
+__device__ __forceinline__ float bilin(const float *__restrict__ tab, int64_t base, int64_t sx,
+                                       int64_t sy, float wx, float wy) {
+  const float v00 = __ldg(tab + base), v01 = __ldg(tab + base + sx);
+  const float v10 = __ldg(tab + base + sy), v11 = __ldg(tab + base + sy + sx);
+  return lerp(lerp(v00, v01, wx), lerp(v10, v11, wx), wy);
+}
+
 // Table value at one depth node of a cell for surface point (px, py).
 // Returns false outside the cell's surface grid.
 __device__ __forceinline__ bool table_node(const qpsdm_ttt_desc &d, const float *__restrict__ tab,
@@ -596,14 +610,12 @@ __device__ __forceinline__ bool table_node(const qpsdm_ttt_desc &d, const float 
     return false;
   int ix = min((int)fx, max(nxs - 2, 0));
   int iy = min((int)fy, max(nys - 2, 0));
-  const float wx = nxs > 1 ? fx - ix : 0.0f, wy = nys > 1 ? fy - iy : 0.0f;
+  const float wx = nxs > 1 ? __fsub_rn(fx, (float)ix) : 0.0f;
+  const float wy = nys > 1 ? __fsub_rn(fy, (float)iy) : 0.0f;
   const int64_t sx = nxs > 1 ? (int64_t)nxi1 * nzi1 : 0;
   const int64_t sy = nys > 1 ? (int64_t)nxs * nxi1 * nzi1 : 0;
   const int64_t base = d.idx + (int64_t)(iy * nxs + ix) * nxi1 * nzi1 + poff;
-  const float v00 = __ldg(tab + base), v01 = __ldg(tab + base + sx);
-  const float v10 = __ldg(tab + base + sy), v11 = __ldg(tab + base + sy + sx);
-  const float a = v00 + wx * (v01 - v00), b = v10 + wx * (v11 - v10);
-  v = a + wy * (b - a);
+  v = bilin(tab, base, sx, sy, wx, wy);
   return true;
 }
 
@@ -633,9 +645,9 @@ __device__ __forceinline__ void setup_cells(PointCells &pc, int ixi, float z,
   const int lx = ixi - a.tcdp1;
   const int ixg = lx / a.nxi1;
   const int ixl = lx - ixg * a.nxi1;
-  const float fz = z / a.dzii;
+  const float fz = __fdiv_rn(z, a.dzii);
   const int izn = (int)fz;
-  pc.c2 = fz - (float)izn;
+  pc.c2 = __fsub_rn(fz, (float)izn);
   int izgA = izn / a.nzi1, izgB = (izn + 1) / a.nzi1;
   int izlA = izn - izgA * a.nzi1;
   int izlB = izn + 1 - izgB * a.nzi1;
@@ -656,7 +668,7 @@ __device__ __forceinline__ void setup_cells(PointCells &pc, int ixi, float z,
   pc.tB = tB.idx;
   pc.qA = qA.idx;
   pc.qB = qB.idx;
-  pc.xc = (a.tcdp1 + ixg * a.nxi1 + 0.5f * (a.nxi1 - 1)) * a.dxi;
+  pc.xc = __fmul_rn(__fadd_rn((float)(a.tcdp1 + ixg * a.nxi1), 0.5f * (a.nxi1 - 1)), a.dxi);
   pc.same = same_grid(tA, tB) && same_grid(tA, qA) && same_grid(tA, qB);
   pc.nxs = tA.nxs;
   pc.nys = tA.nys;
@@ -666,14 +678,6 @@ __device__ __forceinline__ void setup_cells(PointCells &pc, int ixi, float z,
   pc.hy = 0.5f * (tA.nys - 1);
 }
 
-// Bilinear value of a 2 x 2 node block starting at tab + base.
-__device__ __forceinline__ float bilin(const float *__restrict__ tab, int64_t base, int64_t sx,
-                                       int64_t sy, float wx, float wy) {
-  const float v00 = __ldg(tab + base), v01 = __ldg(tab + base + sx);
-  const float v10 = __ldg(tab + base + sy), v11 = __ldg(tab + base + sy + sx);
-  const float a = v00 + wx * (v01 - v00), b = v10 + wx * (v11 - v10);
-  return a + wy * (b - a);
-}
 
 __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
                                           const qpsdm_ttt_desc *__restrict__ dt,
@@ -687,7 +691,8 @@ __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
     if (!grid_pos(px, py, pc.xc, pc.rdx, pc.rdy, pc.hx, pc.hy, nxs, nys, fx, fy)) return false;
     const int ix = min((int)fx, max(nxs - 2, 0));
     const int iy = min((int)fy, max(nys - 2, 0));
-    const float wx = nxs > 1 ? fx - ix : 0.0f, wy = nys > 1 ? fy - iy : 0.0f;
+    const float wx = nxs > 1 ? __fsub_rn(fx, (float)ix) : 0.0f;
+    const float wy = nys > 1 ? __fsub_rn(fy, (float)iy) : 0.0f;
     const int64_t plane = (int64_t)nxi1 * nzi1;
     const int64_t sx = nxs > 1 ? plane : 0, sy = nys > 1 ? (int64_t)nxs * plane : 0;
     const int64_t off = (int64_t)(iy * nxs + ix) * plane;
@@ -695,8 +700,8 @@ __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
     const float tb = bilin(ttt, pc.tB + off + pc.offB, sx, sy, wx, wy);
     const float qa = bilin(qqq, pc.qA + off + pc.offA, sx, sy, wx, wy);
     const float qb = bilin(qqq, pc.qB + off + pc.offB, sx, sy, wx, wy);
-    t = ta + pc.c2 * (tb - ta);
-    q = qa + pc.c2 * (qb - qa);
+    t = lerp(ta, tb, pc.c2);
+    q = lerp(qa, qb, pc.c2);
     return true;
   }
   // cells with different surface grids: one lookup per descriptor
@@ -705,8 +710,8 @@ __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
   if (!table_node(dt[pc.cB], ttt, px, py, pc.xc, pc.offB, nxi1, nzi1, tb)) return false;
   if (!table_node(dq[pc.cA], qqq, px, py, pc.xc, pc.offA, nxi1, nzi1, qa)) return false;
   if (!table_node(dq[pc.cB], qqq, px, py, pc.xc, pc.offB, nxi1, nzi1, qb)) return false;
-  t = ta + pc.c2 * (tb - ta);
-  q = qa + pc.c2 * (qb - qa);
+  t = lerp(ta, tb, pc.c2);
+  q = lerp(qa, qb, pc.c2);
   return true;
 }
 
@@ -716,9 +721,8 @@ __device__ __forceinline__ float2 bilin2(const float2 *__restrict__ tab, int64_t
                                          int64_t sy, float wx, float wy) {
   const float2 v00 = __ldg(tab + base), v01 = __ldg(tab + base + sx);
   const float2 v10 = __ldg(tab + base + sy), v11 = __ldg(tab + base + sy + sx);
-  const float at = v00.x + wx * (v01.x - v00.x), bt = v10.x + wx * (v11.x - v10.x);
-  const float aq = v00.y + wx * (v01.y - v00.y), bq = v10.y + wx * (v11.y - v10.y);
-  return make_float2(at + wy * (bt - at), aq + wy * (bq - aq));
+  return make_float2(lerp(lerp(v00.x, v01.x, wx), lerp(v10.x, v11.x, wx), wy),
+                     lerp(lerp(v00.y, v01.y, wx), lerp(v10.y, v11.y, wx), wy));
 }
 __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
                                           const qpsdm_ttt_desc *__restrict__ dt,
@@ -733,14 +737,15 @@ __device__ __forceinline__ bool lookup_tq(const PointCells &pc,
   if (!grid_pos(px, py, pc.xc, pc.rdx, pc.rdy, pc.hx, pc.hy, nxs, nys, fx, fy)) return false;
   const int ix = min((int)fx, max(nxs - 2, 0));
   const int iy = min((int)fy, max(nys - 2, 0));
-  const float wx = nxs > 1 ? fx - ix : 0.0f, wy = nys > 1 ? fy - iy : 0.0f;
+  const float wx = nxs > 1 ? __fsub_rn(fx, (float)ix) : 0.0f;
+  const float wy = nys > 1 ? __fsub_rn(fy, (float)iy) : 0.0f;
   const int64_t plane = (int64_t)nxi1 * nzi1;
   const int64_t sx = nxs > 1 ? plane : 0, sy = nys > 1 ? (int64_t)nxs * plane : 0;
   const int64_t off = (int64_t)(iy * nxs + ix) * plane;
   const float2 a = bilin2(tq, pc.tA + off + pc.offA, sx, sy, wx, wy);
   const float2 b = bilin2(tq, pc.tB + off + pc.offB, sx, sy, wx, wy);
-  t = a.x + pc.c2 * (b.x - a.x);
-  q = a.y + pc.c2 * (b.y - a.y);
+  t = lerp(a.x, b.x, pc.c2);
+  q = lerp(a.y, b.y, pc.c2);
   return true;
 }
 
@@ -793,7 +798,11 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
   PointCells pc;
   pc.ok = false;
   float tanx1 = 0.f, tanx2 = 0.f, tany1 = 0.f, tany2 = 0.f, acc = 0.f, cmp = 0.f;
-  const float z = izi * a.dzi;
+  // Every operation below that feeds an index, a mask or the image is an
+  // explicit IEEE operation (fused multiply-adds written out), so that the
+  // FP32 C restatement in the oracle computes the same bits from the same
+  // panels.
+  const float z = __fmul_rn((float)izi, a.dzi);
   if (live) {
     const size_t k = (size_t)ixi * a.nzi + izi;
     tanx1 = dips[k];
@@ -805,13 +814,14 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
     setup_cells(pc, ixi, z, a, dt, dq);
   }
   const float tz = a.taperzone;
-  const float tanx1c = tanx1 - tz * (1.0f + tanx1 * tanx1);
-  const float tanx2c = tanx2 + tz * (1.0f + tanx2 * tanx2);
-  const float tany1c = tany1 - tz * (1.0f + tany1 * tany1);
-  const float tany2c = tany2 + tz * (1.0f + tany2 * tany2);
-  const float z2 = z * z;
-  const float x = ixi * a.dxi;
-  const float inv_dt1 = 1.0f / a.dt1, inv_dts = 1.0f / a.dtstar;
+  // tan -/+ tz (1 + tan^2): the limits widened by the taper zone
+  const float tanx1c = __fsub_rn(tanx1, __fmul_rn(tz, __fmaf_rn(tanx1, tanx1, 1.0f)));
+  const float tanx2c = __fadd_rn(tanx2, __fmul_rn(tz, __fmaf_rn(tanx2, tanx2, 1.0f)));
+  const float tany1c = __fsub_rn(tany1, __fmul_rn(tz, __fmaf_rn(tany1, tany1, 1.0f)));
+  const float tany2c = __fadd_rn(tany2, __fmul_rn(tz, __fmaf_rn(tany2, tany2, 1.0f)));
+  const float z2 = __fmul_rn(z, z);
+  const float x = __fmul_rn((float)ixi, a.dxi);
+  const float inv_dt1 = __fdiv_rn(1.0f, a.dt1), inv_dts = __fdiv_rn(1.0f, a.dtstar);
   const size_t pstride = (size_t)a.nbins * a.nt;
   // source terms are reused while consecutive traces share a source
   float last_sx = NAN, last_sy = NAN, ts = 0.f, qs = 0.f;
@@ -843,45 +853,54 @@ __global__ void __launch_bounds__(kPhysBz *kPhysBx)
       if (!lookup_tq(pc, dt, ttt, dq, qqq, a.nxi1, a.nzi1, gm.z, gm.w, tg, qg)) continue;
       ++cnt;  // a point-trace: in the aperture, table values at both ends
       // ray directions and dip taper (src/q-psdm.cu:2303-2340)
-      const float dsx = gm.x - x, dgx = gm.z - x;
-      const float ds = sqrtf(dsx * dsx + gm.y * gm.y + z2);
-      const float dg = sqrtf(dgx * dgx + gm.w * gm.w + z2);
-      const float rs = 1.0f / ds, rg2 = 1.0f / dg;
-      const float ux = dsx * rs + dgx * rg2, uy = gm.y * rs + gm.w * rg2, uz = z * (rs + rg2);
-      const float tanx = ux / uz, tany = uy / uz;
+      const float dsx = __fsub_rn(gm.x, x), dgx = __fsub_rn(gm.z, x);
+      const float ds = __fsqrt_rn(__fmaf_rn(dsx, dsx, __fmaf_rn(gm.y, gm.y, z2)));
+      const float dg = __fsqrt_rn(__fmaf_rn(dgx, dgx, __fmaf_rn(gm.w, gm.w, z2)));
+      const float rs = __fdiv_rn(1.0f, ds), rg2 = __fdiv_rn(1.0f, dg);
+      const float ux = __fmaf_rn(dsx, rs, __fmul_rn(dgx, rg2));
+      const float uy = __fmaf_rn(gm.y, rs, __fmul_rn(gm.w, rg2));
+      const float uz = __fmul_rn(z, __fadd_rn(rs, rg2));
+      const float tanx = __fdiv_rn(ux, uz), tany = __fdiv_rn(uy, uz);
       if (!(tanx > tanx1c && tanx < tanx2c && tany > tany1c && tany < tany2c)) continue;
       float w = 1.0f;
-      if (tanx < tanx1) w *= (tanx - tanx1c) / (tanx1 - tanx1c);
-      if (tanx > tanx2) w *= (tanx2c - tanx) / (tanx2c - tanx2);
-      if (tany < tany1) w *= (tany - tany1c) / (tany1 - tany1c);
-      if (tany > tany2) w *= (tany2c - tany) / (tany2c - tany2);
-      // time and t* picks
-      const float t = ts + tg;
-      const float ft = t * inv_dt1;
+      if (tanx < tanx1)
+        w = __fmul_rn(w, __fdiv_rn(__fsub_rn(tanx, tanx1c), __fsub_rn(tanx1, tanx1c)));
+      if (tanx > tanx2)
+        w = __fmul_rn(w, __fdiv_rn(__fsub_rn(tanx2c, tanx), __fsub_rn(tanx2c, tanx2)));
+      if (tany < tany1)
+        w = __fmul_rn(w, __fdiv_rn(__fsub_rn(tany, tany1c), __fsub_rn(tany1, tany1c)));
+      if (tany > tany2)
+        w = __fmul_rn(w, __fdiv_rn(__fsub_rn(tany2c, tany), __fsub_rn(tany2c, tany2)));
+      // time and t* picks (src/q-psdm.cu:2354-2357)
+      const float t = __fadd_rn(ts, tg);
+      const float ft = __fmul_rn(t, inv_dt1);
       const int it1 = (int)ft;
       if (!(it1 > 0 && it1 + 1 < a.nt)) continue;
       ++cimg;
-      const float wt = ft - (float)it1;
-      float fb = fminf(fmaxf((qs + qg) * inv_dts, 0.0f), (float)(a.nbins - 1));
+      const float wt = __fsub_rn(ft, (float)it1);
+      const float fb = fminf(fmaxf(__fmul_rn(__fadd_rn(qs, qg), inv_dts), 0.0f),
+                             (float)(a.nbins - 1));
       const int b0 = min((int)fb, a.nbins - 2);
-      const float wb = fb - (float)b0;
+      const float wb = __fsub_rn(fb, (float)b0);
       const T *pp = panels + (size_t)(c0 + i) * pstride + (size_t)b0 * a.nt + it1;
       const float p00 = ld_sample<T>(pp), p01 = ld_sample<T>(pp + 1);
       const float p10 = ld_sample<T>(pp + a.nt), p11 = ld_sample<T>(pp + a.nt + 1);
-      const float s0 = p00 + wt * (p01 - p00), s1 = p10 + wt * (p11 - p10);
-      float smp = s0 + wb * (s1 - s0);
-      if (std::is_same<T, __half>::value) smp *= __ldg(pscale + c0 + i);
-      // amplitude weight (src/q-psdm.cu:2366-2374)
-      const float v = t > 0.1f ? 100.0f / (t * t) : 10000.0f;
-      const float r = (ds * rg2) * (ds * rg2) * (ds * rg2) * (tg / ts);
-      const float val = w * (r + 1.0f / r) * v * smp;
+      float smp = lerp(lerp(p00, p01, wt), lerp(p10, p11, wt), wb);
+      if (std::is_same<T, __half>::value) smp = __fmul_rn(smp, __ldg(pscale + c0 + i));
+      // amplitude weight (src/q-psdm.cu:2366-2374): w v (r + 1/r),
+      // r = (ds/dg)^3 tg/ts, v = 100 / t^2 (10^4 below 0.1 s)
+      const float v = t > 0.1f ? __fdiv_rn(100.0f, __fmul_rn(t, t)) : 10000.0f;
+      const float dr = __fmul_rn(ds, rg2);
+      const float r = __fmul_rn(__fmul_rn(__fmul_rn(dr, dr), dr), __fdiv_rn(tg, ts));
+      const float val =
+          __fmul_rn(__fmul_rn(__fmul_rn(w, __fadd_rn(r, __fdiv_rn(1.0f, r))), v), smp);
       if (comp) {  // Kahan-compensated sum
-        const float y = val - cmp;
-        const float tt = acc + y;
-        cmp = (tt - acc) - y;
+        const float y = __fsub_rn(val, cmp);
+        const float tt = __fadd_rn(acc, y);
+        cmp = __fsub_rn(__fsub_rn(tt, acc), y);
         acc = tt;
       } else {
-        acc += val;
+        acc = __fadd_rn(acc, val);
       }
     }
   }
@@ -1797,6 +1816,11 @@ int physics_tuning(const PhysicsState *s, int *variant, int *tz, int *tx, int *m
   if (mb) *mb = v >= 0 ? kVariants[v].mb : 0;
   for (int i = 0; times && i < ntimes && i < kNumVariants; ++i) times[i] = s->tune_ms[i];
   return kNumVariants;
+}
+
+void physics_panels(const PhysicsState *s, void **d_panels, float **d_pscale) {
+  *d_panels = s->d_panels;
+  *d_pscale = s->d_pscale;
 }
 
 int physics_finalize_image(PhysicsState *s, float *d_img, size_t n, cudaStream_t st,

@@ -51,6 +51,9 @@ int physics_process(PhysicsState *s, const qpsdm_static_params &p,
                     const PhysicsBatch &b, cudaStream_t st, std::string *err);
 int physics_tuning(const PhysicsState *s, int *variant, int *tz, int *tx, int *mb,
                    float *times, int ntimes);
+// Panels of the last batch ([max_batch][nbins][nffti], the panel type) and,
+// for FP16 panels, the per-trace sample multipliers.
+void physics_panels(const PhysicsState *s, void **d_panels, float **d_pscale);
 int physics_finalize_image(PhysicsState *s, float *d_img, size_t n, cudaStream_t st,
                            std::string *err);
 

@@ -277,6 +277,12 @@ class Engine:
         return dict(accepted=int(a[0]), point_traces=int(a[1]), tile_decided=int(a[2]),
                     imaged=int(a[3]))
 
+    def panels_device_ptrs(self):
+        """(d_panels, d_pscale) device pointers of the last submit's panels."""
+        a, b = C.c_void_p(), C.c_void_p()
+        self._ck(lib().qpsdm_panels_device_ptr(self.h, C.byref(a), C.byref(b)), "panels")
+        return a.value, b.value
+
     def spectra_device_ptrs(self):
         r, i = C.c_void_p(), C.c_void_p()
         self._ck(lib().qpsdm_spectra_device_ptr(self.h, C.byref(r), C.byref(i)), "spectra")
