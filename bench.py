@@ -855,35 +855,42 @@ def cpu_compat_rate(wl, budget_s=10.0, line=None):
                       f"reference has no other imaging), {nthr} threads"}
 
 
-def cpu_physics_rate(wl, budget_s=10.0):
-    """The physics method on the CPU (the FP64 restatement: numpy panels + C
-    imaging, all host threads) on a bounded sample of one shot and one line,
-    with the plain form's tables."""
+def cpu_physics_rate(wl, budget_s=12.0):
+    """The physics method on the CPU in FP32: the oracle's FP32 restatement of
+    the engine's plain kernel (oracle/physics_fp32.c, OpenMP over image
+    points, all host threads) on panels computed in single precision by
+    numpy, with the plain form's tables, on a bounded sample of one shot
+    gather into one line.  Gate, panels and imaging are timed together."""
     from oracle import oracle as O
     sv = wl.sv
     line = wl.form_lines("plain")[0]
     st = O.derive_static(sv.ntl, np.float32(sv.dt), sv.threshold, 3.0, 8.0)
     gp = _gate_params(O, wl, line)
     tab = _host_tables(wl.tables_for("plain", line))
-    pp = _phys_params(O, wl, st, tab)
+    a = O.P32(nzi=sv.nzi, nxb=sv.nxi, ixstart=0, nt=st["nffti"], nbins=16, dt1=st["dt1"],
+              dxi=sv.dxi, dzi=sv.dzi, taperzone=st["taperzone"], dtstar=wl.DTSTAR,
+              dzii=wl.dzii, tcdp1=tab["cdp1"] - sv.fci, tcdp2=tab["cdp2"] - sv.fci,
+              nxg=tab["nxg"], nzg=tab["nzg"], nxi1=tab["nxi1"], nzi1=tab["nzi1"])
     filt = O.physics_filter(st["nfft"], np.float32(sv.dt), 130.0, 140.0, sv.fpeak,
                             sv.threshold, 16, wl.DTSTAR)
-    dips = [d.ravel() for d in wl.synth.dip_fields(sv.nxi, sv.nzi, float(st["contract"]))]
+    dips = np.stack([d.ravel() for d in wl.synth.dip_fields(sv.nxi, sv.nzi,
+                                                            float(st["contract"]))])
     hdr, traces = _hdr_traces(wl.batch(0, 1))
     nthr = os.cpu_count() or 1
-    img = np.zeros(sv.nxi * sv.nzi)
+    img = np.zeros(sv.nxi * sv.nzi, np.float32)
     rng = np.random.default_rng(1)
-    n, t_tot, npt_tot, ntr_tot = 8, 0.0, 0, 0
+    n, t_tot, npt_tot, ntr_tot = 16, 0.0, 0, 0
     while True:
-        idx = rng.choice(hdr.shape[0], n, replace=False)
+        idx = np.sort(rng.choice(hdr.shape[0], n, replace=False))
         t0 = time.perf_counter()
         ints, geom = O.gate_traces(gp, hdr[idx])
         ok = ints[:, 0] == 3
         npt = 0
         if ok.any():
-            pan = O.physics_panels(traces[idx][ok], np.float32(sv.dt), st["nfft"], st["nffti"],
-                                   filt)
-            _, npt = O.physics_image(pp, geom[ok], ints[ok][:, [4, 5, 7]], pan, dips, tab, img)
+            pan = np.zeros((n, 16, st["nffti"]), np.float32)
+            pan[ok] = O.physics_panels(traces[idx][ok], np.float32(sv.dt), st["nfft"],
+                                       st["nffti"], filt, fp32=True)
+            _, npt, _ = O.image_plain_fp32(a, ints, geom, pan, dips, tab, img)
         t_tot += time.perf_counter() - t0
         npt_tot += npt
         ntr_tot += n
@@ -894,9 +901,10 @@ def cpu_physics_rate(wl, budget_s=10.0):
     return {"value": npt_tot / t_tot / 1e9, "unit": "Gpoint-traces/s", "cores": nthr,
             "kind": "port", "cpu_model": _cpu_model(),
             "sample": f"{ntr_tot} random traces of a {sv.name} shot into one {sv.nxi}x{sv.nzi} "
-                      f"line ({npt_tot} point-traces, {t_tot:.1f} s): the FP64 CPU "
-                      f"restatement of the physics method (numpy float64 panels + C imaging), "
-                      f"{nthr} threads"}
+                      f"line ({npt_tot} point-traces, {t_tot:.1f} s): the physics method in "
+                      f"FP32 on the CPU -- the FP32 C restatement of the engine's plain kernel "
+                      f"(OpenMP over image points, {nthr} threads) on numpy FP32 panels, gate "
+                      f"included"}
 
 
 def accuracy_vs_fp64(wl, dev, ntr=1200, seed=2):
@@ -949,15 +957,15 @@ def accuracy_vs_fp64(wl, dev, ntr=1200, seed=2):
     return out
 
 
-def accuracy_config(name, dev, ntr=1200):
+def accuracy_config(name, dev, ntr=1200, eikonal=True):
     """Image NRMSE of the batched (FP16 panels) and plain (FP32 panels) forms
     against the FP64 oracle on a seeded sample of configuration `name`
     (`synth.accuracy_sample`: its own geometry, trace length, Q model, gain
-    limit and image size), one line."""
+    limit and image size; eikonal tables of its own model), one line."""
     from oracle import oracle as O
     from q_psdm_b200 import engine as E
     from q_psdm_b200 import synth
-    smp = synth.accuracy_sample(name, ntr=ntr)
+    smp = synth.accuracy_sample(name, ntr=ntr, eikonal=eikonal, device=dev)
     sv, tab = smp["sv"], smp["tab"]
     st = O.derive_static(sv.ntl, np.float32(sv.dt), sv.threshold, 3.0, 8.0)
     az = np.stack(smp["az"]).astype(np.int32)
@@ -1096,7 +1104,7 @@ def main():
                 if args.config == "c5":
                     res["accuracy"]["surrogate_traveltime_vs_eikonal"] = surrogate_truth(wl, dev)
                 res["accuracy"]["configs"] = {n: accuracy_config(n, dev)
-                                              for n in ("c1", "c3", "c5")}
+                                              for n in ("c1", "c2", "c3", "c5")}
     if res is not None:
         print(json.dumps(res), flush=True)
     if dist:

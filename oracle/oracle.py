@@ -271,8 +271,10 @@ def physics_filter(nfft, dt, f3, f4, fc, threshold, nbins, dtstar):
     return out
 
 
-def physics_panels(traces, dt, nfft, nffti, filt):
-    """[ntr, nbins, nffti] float64 compensated panels of float32 traces."""
+def physics_panels(traces, dt, nfft, nffti, filt, fp32: bool = False):
+    """[ntr, nbins, nffti] compensated panels of float32 traces: float64, or
+    with fp32 the same computation in single precision (float32 FFTs and a
+    complex64 filter; the CPU baseline's panels)."""
     traces = np.ascontiguousarray(traces, np.float32)
     ntr, ntl = traces.shape
     x = np.empty_like(traces)
@@ -282,6 +284,13 @@ def physics_panels(traces, dt, nfft, nffti, filt):
         g[:] = traces[i]
         L.orc_gain(g, ntl, dt)
         L.orc_fetch_and_taper(g, ntl, 0, ntl - 1, x[i])
+    if fp32:
+        X = np.fft.rfft(x, n=nfft, axis=1)
+        f32 = filt.astype(np.complex64) * np.float32(nffti)
+        out = np.empty((ntr, filt.shape[0], nffti), np.float32)
+        for b in range(filt.shape[0]):
+            out[:, b, :] = np.fft.irfft(X * f32[b][None, :], n=nffti, axis=1)
+        return out
     X = np.fft.rfft(x.astype(np.float64), n=nfft, axis=1)
     out = np.empty((ntr, filt.shape[0], nffti))
     for b in range(filt.shape[0]):

@@ -443,18 +443,44 @@ SAMPLES = {
     # name: (survey, line, shots near the line, dtstar (s), aperture half-width
     # (m) or None for a seeded value in [1, 4] km, table half-widths (m))
     "c1": (config1, 64, 4, 0.0015, 400.0, (900.0, 900.0)),
+    "c2": (config2, 256, 2, 0.002, 2000.0, (2500.0, 1500.0)),
     "c3": (config3, 384, 3, 0.0025, None, (2500.0, 1500.0)),
     "c5": (config5, 512, 2, 0.005, 2000.0, (2500.0, 1500.0)),
 }
 
 
-def accuracy_sample(name: str, ntr: int = 1200, seed: int = 7) -> dict:
+def config_models(name: str, h: float = 50.0):
+    """(model, background, Q of the background) of a configuration on a grid
+    for the eikonal table generator: c2 the anomalies and the 5 Q layers,
+    c3 v(z) with its smooth random Q layers, c5 the gas cloud."""
+    if name == "c2":
+        return (config2_model(h=h), config2_model(h=h, anomalies=False, layered_q=False),
+                80.0)
+    if name == "c5":
+        return config5_model(h=h), config5_model(h=h, cloud=False), 100.0
+    if name == "c3":
+        sv = config3()
+        m = config2_model(h=h, anomalies=False, layered_q=False, xr=(-2800.0, 10500.0),
+                          yr=(-1400.0, 9100.0), zmax=5200.0, v0=sv.v0, kz=sv.k, q=80.0)
+        zn, qn = np.asarray(sv.q_model[1], float), np.asarray(sv.q_model[2], float)
+        z = np.arange(m.vel.shape[0]) * h
+        m.invq[:] = (1.0 / np.interp(z, zn, qn)).astype(np.float32)[:, None, None]
+        bg = config2_model(h=h, anomalies=False, layered_q=False, xr=(-2800.0, 10500.0),
+                           yr=(-1400.0, 9100.0), zmax=5200.0, v0=sv.v0, kz=sv.k, q=80.0)
+        return m, bg, 80.0
+    raise ValueError(f"no gridded model for {name}")
+
+
+def accuracy_sample(name: str, ntr: int = 1200, seed: int = 7, eikonal: bool = False,
+                    device: int = 0) -> dict:
     """A seeded sample of a configuration for image accuracy against the FP64
     oracle: `ntr` traces drawn from the shots nearest to one image line (their
-    gathers as the configuration records them), the line's analytic tables
-    (depth and surface nodes every 160 m; t* from the configuration's Q model)
-    and the aperture tables.  Configuration 2's sample is the benchmark's own
-    (two of its step's gathers)."""
+    gathers as the configuration records them), the line's tables and the
+    aperture tables.  Tables: with eikonal=True (configurations 2, 3, 5) the
+    project's eikonal / t* generator on the configuration's gridded model
+    (`config_models`: anomalies and Q layers, smooth random Q, the gas
+    cloud), else analytic v(z) tables with t* of the configuration's Q model
+    along straight rays; surface nodes every 160 m in both."""
     from . import tables as T
     from .engine import encode_su
     make, line, nsh, dtstar, ap, (hx, hy) = SAMPLES[name]
@@ -475,12 +501,24 @@ def accuracy_sample(name: str, ntr: int = 1200, seed: int = 7) -> dict:
     rec = encode_su(hdr[:, 0], hdr[:, 1], hdr[:, 2], hdr[:, 3], traces,
                     dt_us=int(round(sv.dt * 1e6)), scalco=sv.scalco)
     sub_n = 16  # 160 m nodes
-    tab = T.linear_gradient_tables(sv, fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi,
-                                   zmax=(sv.nzi - 1) * sv.dzi, sub=sub_n, nxi1=16,
-                                   half_x=hx, half_y=hy, line_y=ly)
+    if eikonal and name != "c1":
+        # the configuration's own model through the eikonal / t* generator
+        # (surface nodes every 160 m, depth nodes every 80 m, 50 m grid)
+        model, bg, qb = config_models(name, h=50.0)
+        tab = T.eikonal_line_tables(model, fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi,
+                                    zmax=(sv.nzi - 1) * sv.dzi, line_y=line * sv.dyi,
+                                    dzii=80.0, nxi1=16, surf_dx=160, surf_dy=160, half_x=hx,
+                                    half_y=hy, h=50.0, background=bg, q_background=qb,
+                                    device=device)
+    else:
+        tab = T.linear_gradient_tables(sv, fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi,
+                                       zmax=(sv.nzi - 1) * sv.dzi, sub=sub_n, nxi1=16,
+                                       half_x=hx, half_y=hy, line_y=ly)
     half_cdps, half_lines = int(round(ap / sv.dxi)), int(round(0.5 * ap / sv.dyi))
     return dict(name=name, sv=sv, line=line, cyi=ly, hdr=hdr, traces=traces, records=rec,
                 tab=tab, az=aperture_tables(half_cdps, half_lines), dtstar=dtstar,
                 aperture_m=ap,
                 describe=f"{len(pick)} seeded traces of the {nsh} shot gathers nearest to "
-                         f"line {line} of configuration {name[1:]}, aperture +-{ap:.0f} m")
+                         f"line {line} of configuration {name[1:]}, aperture +-{ap:.0f} m, "
+                         + ("eikonal tables of the configuration's model"
+                            if eikonal and name != "c1" else "analytic v(z) tables"))
