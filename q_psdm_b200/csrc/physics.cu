@@ -75,6 +75,7 @@ struct PhysicsState {
   float2 *d_grppos = nullptr;                  // [max_batch] receiver positions
   int *d_memgrp = nullptr;                     // [max_batch] group of each sorted member
   int *d_tile_ctr = nullptr;
+  int *d_nmem = nullptr;                       // accepted members of the current line's batch
   void *d_cub = nullptr;
   size_t cub_bytes = 0;
   int num_sms = 0;
@@ -201,6 +202,7 @@ void physics_destroy(PhysicsState *s) {
   cudaFree(s->d_grppos);
   cudaFree(s->d_memgrp);
   cudaFree(s->d_tile_ctr);
+  cudaFree(s->d_nmem);
   cudaFree(s->d_cub);
   cudaFree(s->d_filter);
   cudaFree(s->d_spec);
@@ -921,8 +923,12 @@ constexpr unsigned long long kNoKey = ~0ull;
 __global__ void k_batch_keys(const uint8_t *__restrict__ rec, int rec_bytes, int be, int ntr,
                              const int *__restrict__ ints, const float *__restrict__ geom,
                              unsigned long long *__restrict__ key, int *__restrict__ val,
-                             int *__restrict__ srcflag) {
+                             int *__restrict__ srcflag, int *__restrict__ naccepted) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // accepted members of the batch (they sort first: rejected keys are the largest)
+  const bool acc = i < ntr && ints[(size_t)i * kGateInts] == kAccepted;
+  const unsigned ballot = __ballot_sync(0xffffffffu, acc);
+  if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(naccepted, __popc(ballot));
   if (i >= ntr) return;
   const uint8_t *r = rec + (size_t)i * rec_bytes;
   int flag = 1;
@@ -932,7 +938,7 @@ __global__ void k_batch_keys(const uint8_t *__restrict__ rec, int rec_bytes, int
            su_i32(r, kOffSy, be) != su_i32(q, kOffSy, be);
   }
   srcflag[i] = flag;
-  const bool ok = ints[(size_t)i * kGateInts] == kAccepted;
+  const bool ok = acc;
   const float gx = geom[(size_t)i * kGateF + 2], gy = geom[(size_t)i * kGateF + 3];
   key[i] = ok ? ((unsigned long long)__float_as_uint(gy) << 32) | __float_as_uint(gx) : kNoKey;
   val[i] = i;
@@ -1099,7 +1105,8 @@ template <int TZ, int TX, int MB, int U, typename T>
 __global__ void __launch_bounds__(TZ *TX, MB)
     k_image_batched(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
                     const float *__restrict__ dips, const int *__restrict__ memgrp,
-                    const float2 *__restrict__ grppos, const int4 *__restrict__ mem, int nmem,
+                    const float2 *__restrict__ grppos, const int4 *__restrict__ mem,
+                    const int *__restrict__ nmem_ptr,
                     const float2 *__restrict__ srcpos, const int *__restrict__ nsrc_ptr,
                     const qpsdm_ttt_desc *__restrict__ dt, const float *__restrict__ ttt,
                     const qpsdm_ttt_desc *__restrict__ dq, const float *__restrict__ qqq,
@@ -1108,6 +1115,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
                     unsigned long long *npt) {
   constexpr int NT = TZ * TX, NW = NT / 32, MC = 32 * NT;
   static_assert(NT % 32 == 0, "whole warps");
+  const int nmem = *nmem_ptr;  // the accepted members (sorted first)
   extern __shared__ float2 smap[];  // [kMapN][sc][NT]
   __shared__ unsigned s_mask[NT];   // kept members of the chunk, one bit each
   __shared__ int s_col[TX + 1];     // active points of the tile's columns (prefix sums)
@@ -1438,6 +1446,7 @@ static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p) {
   ok &= cudaMalloc(&s->d_grppos, sizeof(float2) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_memgrp, sizeof(int) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_tile_ctr, sizeof(int)) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_nmem, sizeof(int)) == cudaSuccess;
   if (!ok) return QPSDM_ENOMEM;
   size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b1, s->d_key[0], s->d_key[1], s->d_val[0],
@@ -1503,7 +1512,7 @@ static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const Ph
   const int grid = std::max(1, std::min(ntz * ntx, std::max(per_sm, 1) * s->num_sms));
   cudaMemsetAsync(s->d_tile_ctr, 0, sizeof(int), st);
   kern<<<grid, TZ * TX, smem, st>>>(img, comp, a, v.dips, s->d_memgrp, s->d_grppos, s->d_mem,
-                                    b.ntr, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
+                                    s->d_nmem, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
                                     v.tab->ttt, v.tab->dq, v.tab->qqq,
                                     v.tab->paired ? v.tab->tq : nullptr, (const T *)s->d_panels,
                                     s->d_tile_ctr, ntz, ntx, sc, npt);
@@ -1600,8 +1609,9 @@ static int batched_group(PhysicsState *s, const qpsdm_static_params &p, const Li
                          const PhysicsBatch &b, cudaStream_t st) {
   const qpsdm_line_params &l = *v.l;
   const int n = b.ntr, blk = 256, grd = (n + blk - 1) / blk;
+  cudaMemsetAsync(s->d_nmem, 0, sizeof(int), st);
   k_batch_keys<<<grd, blk, 0, st>>>(b.d_rec, b.rec_bytes, b.big_endian, n, v.ints, v.geom,
-                                    s->d_key[0], s->d_val[0], s->d_srcflag);
+                                    s->d_key[0], s->d_val[0], s->d_srcflag, s->d_nmem);
   size_t tb = s->cub_bytes;
   if (cub::DeviceScan::InclusiveSum(s->d_cub, tb, s->d_srcflag, s->d_sid, n, st) != cudaSuccess)
     return QPSDM_ECUDA;
