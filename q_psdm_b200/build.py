@@ -2,7 +2,9 @@
 
 ``python -m q_psdm_b200.build`` compiles every ``csrc/*.cu`` / ``csrc/*.cpp``
 with nvcc (``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``) into
-``q_psdm_b200/libqpsdm_b200.so``, then the ``q-psdm`` command-line driver
+``q_psdm_b200/libqpsdm_b200.so``, the driver's utility library
+(``pkg/*.cpp``: psdmpkg and the SU trace I/O, host C++ with g++) into
+``q_psdm_b200/libqpsdm_pkg.so``, then the ``q-psdm`` command-line driver
 (``driver/q_psdm.cpp``) into ``q_psdm_b200/bin/q-psdm``.  Objects go to ``q_psdm_b200/_build/``;
 a source is recompiled only when it, or a header, is newer than its object.
 """
@@ -19,6 +21,9 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libqpsdm_b200.so")
+PKGSRC = os.path.join(PKG, "pkg")
+PKGLIB = os.path.join(PKG, "libqpsdm_pkg.so")
+CXX = os.environ.get("CXX", "g++")
 DRIVER = os.path.join(PKG, "driver")
 DRIVER_BIN = os.path.join(PKG, "bin", "q-psdm")
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -52,17 +57,36 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
+def build_pkg() -> str:
+    """libqpsdm_pkg.so: psdmpkg (parameters, lists, mute, taper, paths) and
+    the SU trace readers/writers.  No contraction: float arithmetic exactly as
+    written (-ffp-contract=off), so results match the reference's bit for bit."""
+    srcs = sorted(glob.glob(os.path.join(PKGSRC, "*.cpp")))
+    if (os.path.exists(PKGLIB)
+            and all(os.path.getmtime(PKGLIB) >= os.path.getmtime(s) for s in srcs)
+            and os.path.getmtime(PKGLIB) >= _headers_mtime()):
+        return PKGLIB
+    cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off",
+           "-fno-fast-math", "-Wall", "-I" + os.path.join(ROOT, "include"),
+           "-o", PKGLIB] + srcs
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"libqpsdm_pkg build failed:\n{r.stdout}\n{r.stderr}")
+    return PKGLIB
+
+
 def build_driver() -> str:
     """The q-psdm command-line driver (host C++ over the C ABI), linked
-    against the in-tree library (rpath $ORIGIN/..)."""
+    against the in-tree libraries (rpath $ORIGIN/..)."""
     src = os.path.join(DRIVER, "q_psdm.cpp")
     os.makedirs(os.path.dirname(DRIVER_BIN), exist_ok=True)
     if (os.path.exists(DRIVER_BIN) and os.path.getmtime(DRIVER_BIN) >= os.path.getmtime(src)
             and os.path.getmtime(DRIVER_BIN) >= os.path.getmtime(LIB)
+            and os.path.getmtime(DRIVER_BIN) >= os.path.getmtime(PKGLIB)
             and os.path.getmtime(DRIVER_BIN) >= _headers_mtime()):
         return DRIVER_BIN
     cmd = [NVCC, "-O2", "-std=c++17", "-x", "c++", src, "-o", DRIVER_BIN,
-           "-I" + os.path.join(ROOT, "include"), "-L" + PKG, "-lqpsdm_b200", "-lpthread",
+           "-I" + os.path.join(ROOT, "include"), "-L" + PKG, "-lqpsdm_b200", "-lqpsdm_pkg", "-lpthread",
            "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/.."]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -81,6 +105,7 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_pkg()
     build_driver()
     return LIB
 

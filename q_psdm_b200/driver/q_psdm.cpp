@@ -60,6 +60,7 @@
 #include <vector>
 
 #include "qpsdm_engine.h"
+#include "qpsdm_psdmpkg.h"
 
 namespace {
 
@@ -83,76 +84,30 @@ void logf(const char *fmt, ...) {
 bool exists(const std::string &p) { return access(p.c_str(), F_OK) == 0; }
 
 // ---------------------------------------------------------------------------
-// command line and par.dat
+// command line and par.dat, through libqpsdm_pkg (include/qpsdm_psdmpkg.h)
 // ---------------------------------------------------------------------------
-// Command line: "key=value" words; the first word with that key wins
-// (getparstr, src/psdmpkg.cc:233-334).
-struct CmdLine {
-  std::vector<std::string> words;
-  bool get(const std::string &key, std::string &out) const {
-    for (const auto &w : words)
-      if (w.size() > key.size() && w.compare(0, key.size(), key) == 0 && w[key.size()] == '=') {
-        out = w.substr(key.size() + 1);
-        return true;
-      }
-    return false;
-  }
-};
-
-// par.dat: "key=value" records, '#' comments (whole line or trailing), a
-// trailing backslash continues a record, blanks around a record ignored.  A
-// key counts only when exactly one record has it (readparfile,
-// src/psdmpkg.cc:338-574); the value is the record's first word.
-struct ParFile {
-  std::vector<std::string> recs;
-  void load(const std::string &path) {
-    FILE *fp = std::fopen(path.c_str(), "r");
-    if (!fp) die("Parameter File [%s] Open Error", path.c_str());
-    std::string cur;
-    char buf[4096];
-    while (std::fgets(buf, sizeof buf, fp)) {
-      cur += buf;
-      if (cur.empty() || cur.back() != '\n') continue;  // long line: keep reading
-      cur.pop_back();
-      if (!cur.empty() && cur.back() == '\\') {  // continuation
-        cur.pop_back();
-        continue;
-      }
-      add(cur);
-      cur.clear();
-    }
-    if (!cur.empty()) add(cur);
-    std::fclose(fp);
-  }
-  void add(std::string s) {
-    size_t b = 0;
-    while (b < s.size() && std::isspace((unsigned char)s[b])) ++b;
-    s = s.substr(b);
-    if (s.empty() || s[0] == '#') return;
-    const size_t h = s.find('#');
-    if (h != std::string::npos) s = s.substr(0, h);
-    while (!s.empty() && std::isspace((unsigned char)s.back())) s.pop_back();
-    if (!s.empty()) recs.push_back(s);
-  }
-  bool get(const std::string &key, std::string &out) const {
-    int n = 0;
-    std::string v;
-    for (const auto &r : recs)
-      if (r.size() > key.size() && r.compare(0, key.size(), key) == 0 && r[key.size()] == '=') {
-        ++n;
-        v = r.substr(key.size() + 1);
-      }
-    if (n != 1) return false;
-    const size_t e = v.find_first_of(" \t");
-    out = e == std::string::npos ? v : v.substr(0, e);
-    return !out.empty();
-  }
-};
-
+// A key is taken from the command line first (getpar*), else from par.dat,
+// where exactly one record must match the typed pattern "key=%d" / "key=%f"
+// / "key=%s" (src/q-psdm.cu:425-871: getparX(k) || readparfile(...) == 1).
 struct Keys {
-  CmdLine cmd;
-  ParFile par;
-  bool str(const char *k, std::string &out) const { return cmd.get(k, out) || par.get(k, out); }
+  std::string parfile;
+  bool str(const char *k, std::string &out) const {
+    char *v = nullptr;
+    if (getparstring(k, &v)) {
+      out = v;
+      return true;
+    }
+    char buf[1024];
+    if (readparfile(parfile.c_str(), (std::string(k) + "=%s").c_str(), buf) != 1) return false;
+    out = buf;
+    return true;
+  }
+  bool num(const char *k, int &out) const {
+    return getparint(k, &out) || readparfile(parfile.c_str(), (std::string(k) + "=%d").c_str(), &out) == 1;
+  }
+  bool num(const char *k, float &out) const {
+    return getparfloat(k, &out) || readparfile(parfile.c_str(), (std::string(k) + "=%f").c_str(), &out) == 1;
+  }
   std::string str_or(const char *k, const std::string &def) const {
     std::string v;
     return str(k, v) ? v : def;
@@ -163,103 +118,67 @@ struct Keys {
     return v;
   }
   int int_or(const char *k, int def) const {
-    std::string v;
-    return str(k, v) ? (int)std::strtol(v.c_str(), nullptr, 10) : def;
+    int v = def;
+    return num(k, v) ? v : def;
   }
-  int int_req(const char *k) const { return (int)std::strtol(str_req(k).c_str(), nullptr, 10); }
+  int int_req(const char *k) const {
+    int v = 0;
+    if (!num(k, v)) die("%s must be specified", k);
+    return v;
+  }
   float flt_or(const char *k, float def) const {
-    std::string v;
-    return str(k, v) ? (float)std::strtod(v.c_str(), nullptr) : def;
+    float v = def;
+    return num(k, v) ? v : def;
   }
-  float flt_req(const char *k) const { return (float)std::strtod(str_req(k).c_str(), nullptr); }
+  float flt_req(const char *k) const {
+    float v = 0.0f;
+    if (!num(k, v)) die("%s must be specified", k);
+    return v;
+  }
 };
 
-// "1,5-8,10:2:16" -> 1 5 6 7 8 10 12 14 16 (parseline, src/psdmpkg.cc:108-206)
+// "1,5-8,10:2:16" -> 1 5 6 7 8 10 12 14 16 (parseline)
 std::vector<int> parse_list(const std::string &s) {
-  std::vector<int> out;
-  size_t i = 0;
-  while (i < s.size()) {
-    size_t j = s.find(',', i);
-    if (j == std::string::npos) j = s.size();
-    const std::string item = s.substr(i, j - i);
-    int a, b, c;
-    if (std::sscanf(item.c_str(), "%d:%d:%d", &a, &b, &c) == 3) {
-      if (b > 0)
-        for (int v = a; v <= c; v += b) out.push_back(v);
-      else if (b < 0)
-        for (int v = a; v >= c; v += b) out.push_back(v);
-    } else if (std::sscanf(item.c_str(), "%d-%d", &a, &b) == 2) {
-      for (int v = a; v <= b; ++v) out.push_back(v);
-    } else if (std::sscanf(item.c_str(), "%d", &a) == 1) {
-      out.push_back(a);
-    }
-    i = j + 1;
-  }
+  int n = 0;
+  int *p = parseline(s.c_str(), &n);
+  std::vector<int> out(p, p + std::max(n, 0));
+  std::free(p);
   return out;
 }
 
-// "(d1,o1),(d2,o2)..." -> pairs (parsetuple, src/psdmpkg.cc:686-880)
-std::vector<std::pair<float, float>> parse_pairs(const std::string &s) {
-  std::vector<std::pair<float, float>> out;
-  size_t i = 0;
-  while ((i = s.find('(', i)) != std::string::npos) {
-    const size_t j = s.find(')', i);
-    if (j == std::string::npos) break;
-    float a, b;
-    if (std::sscanf(s.c_str() + i + 1, "%f%*[ ,;\t]%f", &a, &b) == 2) out.push_back({a, b});
-    i = j + 1;
-  }
-  return out;
+// "(d1,o1),(d2,o2)..." -> the (depth, offset) pairs made increasing
+// (parsetuple + time_offset_mute_santity, src/q-psdm.cu:1014-1025)
+std::vector<float> mute_pairs(const std::string &s) {
+  int nt = 0, ne = 0;
+  float *p = parsetuple(s.c_str(), &nt, &ne);
+  if (!p || ne != 2 || nt < 1) die("mute [%s] is not a list of (depth,offset) pairs", s.c_str());
+  std::vector<float> m(p, p + 2 * nt);
+  std::free(p);
+  time_offset_mute_santity(m.data(), nt);
+  return m;
+}
+float mute_depth(std::vector<float> &m, float o) {
+  return time_offset_mute(m.data(), (int)m.size() / 2, o);
 }
 
-// Monotone (depth, offset) pairs, then the depth of a given offset:
-// linear inside, the end segments extended outside
-// (time_offset_mute_santity / time_offset_mute, src/psdmpkg.cc:576-600, :1030-1075).
-void mute_sanity(std::vector<std::pair<float, float>> &m) {
-  for (size_t i = 0; i + 1 < m.size(); ++i) {
-    if (m[i].first > m[i + 1].first) m[i + 1].first = 2.0f * m[i].first - m[i + 1].first;
-    if (m[i].second > m[i + 1].second) m[i + 1].second = 2.0f * m[i].second - m[i + 1].second;
-  }
-  for (size_t i = 0; i + 1 < m.size(); ++i) {
-    if (m[i].first >= m[i + 1].first) m[i + 1].first = m[i].first + 0.01f;
-    if (m[i].second >= m[i + 1].second) m[i + 1].second = m[i].second + 10.0f;
-  }
-}
-float mute_depth(const std::vector<std::pair<float, float>> &m, float o) {
-  const size_t n = m.size();
-  if (n == 0) return 0.0f;
-  if (n == 1) return m[0].first;
-  size_t a = 0;
-  if (o < m[0].second)
-    a = 0;
-  else if (o >= m[n - 1].second)
-    a = n - 2;
-  else
-    for (size_t i = 0; i + 1 < n; ++i)
-      if (m[i].second <= o && o < m[i + 1].second) {
-        a = i;
-        break;
-      }
-  const float o1 = m[a].second, o2 = m[a + 1].second, t1 = m[a].first, t2 = m[a + 1].first;
-  return t1 + (t2 - t1) / (o2 - o1) * (o - o1);
-}
-
-// <projpath>/<projname>/<iproc>/<task> split as parsepath (src/psdmpkg.cc:633-684)
+// <projpath>/<iproc>/<task>, trailing '/' removed first (strrtrim +
+// parsepath, src/q-psdm.cu:396-420)
 struct ProjPath {
   std::string projpath, projname, task;
   int iproc = 0;
 };
-ProjPath parse_path(std::string path) {
-  while (!path.empty() && path.back() == '/') path.pop_back();
+ProjPath parse_path(std::string &path) {
+  std::vector<char> buf(path.begin(), path.end());
+  buf.push_back(0);
+  strrtrim(buf.data(), '/');
+  path = buf.data();
+  const size_t n = buf.size() + 1;
+  std::vector<char> pp(n, 0), pn(n, 0), task(n, 0);
   ProjPath r;
-  size_t s = path.rfind('/');
-  r.task = s == std::string::npos ? path : path.substr(s + 1);
-  const std::string rest = s == std::string::npos ? "" : path.substr(0, s);
-  s = rest.rfind('/');
-  r.iproc = std::atoi((s == std::string::npos ? rest : rest.substr(s + 1)).c_str());
-  r.projpath = s == std::string::npos ? "" : rest.substr(0, s);
-  s = r.projpath.rfind('/');
-  r.projname = s == std::string::npos ? r.projpath : r.projpath.substr(s + 1);
+  parsepath(buf.data(), pp.data(), pn.data(), &r.iproc, task.data());
+  r.projpath = pp.data();
+  r.projname = pn.data();
+  r.task = task.data();
   return r;
 }
 
@@ -295,13 +214,6 @@ bool read_header(FILE *fp, long k, int ns, TraceHdr &t) {
   if (std::fseek(fp, k * (kHdr + 4L * ns), SEEK_SET) != 0) return false;
   return std::fread(t.h, 1, kHdr, fp) == (size_t)kHdr;
 }
-// getscale (src/psdmpkg.cc:1013-1027): single precision, as the reference
-// derives its geometry from it in float
-float su_scale(int16_t scalco) {
-  if (scalco == 0) return 1.0f;
-  return scalco > 0 ? (float)scalco : -1.0f / scalco;
-}
-
 // ---------------------------------------------------------------------------
 // tables: Lxxx.{tidx,qidx} + L<line>.{ttt,qqq}, inter-line lerp
 // (get_ttt_all, src/q-psdm.cu:2382-2622)
@@ -492,15 +404,19 @@ void check_engine(int rc, qpsdm_engine *e, const char *what) {
 }  // namespace
 
 int main(int argc, char **argv) {
-  Keys K;
-  for (int i = 1; i < argc; ++i) K.cmd.words.push_back(argv[i]);
-  std::string path, parfilepath, nodename, ttpath;
-  if (!K.cmd.get("path", path)) die("path must be specified");
-  if (!K.cmd.get("parfilepath", parfilepath)) die("parfilepath must be specified");
-  if (!K.cmd.get("nodename", nodename)) die("nodename must be specified");
-  if (!K.cmd.get("ttpath", ttpath)) die("ttpath must be specified");
-  while (!path.empty() && path.back() == '/') path.pop_back();
-  K.par.load(parfilepath);
+  initargs_inner(argc, argv, nullptr);
+  auto cmd = [](const char *k) {
+    char *v = nullptr;
+    if (!getparstring(k, &v)) die("%s must be specified", k);
+    return std::string(v);
+  };
+  std::string path = cmd("path");
+  const std::string parfilepath = cmd("parfilepath"), nodename = cmd("nodename"),
+                    ttpath = cmd("ttpath");
+  FILE *pf = std::fopen(parfilepath.c_str(), "r");
+  if (!pf) die("Parameter File [%s] Open Error", parfilepath.c_str());
+  std::fclose(pf);
+  Keys K{parfilepath};
   const ProjPath pp = parse_path(path);
 
   // ---- keys (src/q-psdm.cu:433-714) ----
@@ -565,7 +481,7 @@ int main(int argc, char **argv) {
   std::fseek(vf, -(long)(kHdr + 4L * ntv), SEEK_END);
   if (std::fread(v1.h, 1, kHdr, vf) != (size_t)kHdr) die("velocity file last header");
   // float arithmetic as src/q-psdm.cu:846-858 (int x float -> float)
-  const float scalev = su_scale(be_i16(v0.h + oScalco));
+  const float scalev = getscale(be_i16(v0.h + oScalco));
   const double fxv = (float)be_i32(v0.h + oGx) * scalev;
   const double fyv = (float)be_i32(v0.h + oGy) * scalev;
   const int fcv = be_i32(v0.h + oCdp), flv = be_i32(v0.h + oFldr);
@@ -574,11 +490,9 @@ int main(int argc, char **argv) {
   const float dxv = (float)(be_i32(v1.h + oGx) - be_i32(v0.h + oGx)) * scalev / (float)(nxv - 1);
   float dyv;
   if (nyv == 1) {
-    std::string s;
-    if (!K.str("dyv", s))
+    if (!K.num("dyv", dyv))
       die("since first fldr and last fldr in the velocity file is the same:%d please specify dyv!",
           flv);
-    dyv = (float)std::strtod(s.c_str(), nullptr);
   } else {
     dyv = (float)(be_i32(v1.h + oGy) - be_i32(v0.h + oGy)) * scalev / (float)(nyv - 1);
     dyv = K.flt_or("dyv", dyv);
@@ -595,7 +509,7 @@ int main(int argc, char **argv) {
     FILE *fp = std::fopen(f.c_str(), "rb");
     TraceHdr t;
     if (fp && std::fread(t.h, 1, kHdr, fp) == (size_t)kHdr) {
-      scaled = su_scale(be_i16(t.h + oScalco));
+      scaled = getscale(be_i16(t.h + oScalco));
       if ((uint16_t)be_i16(t.h + oNs) != ntl)
         die("In Data Space (tr.ns=%d)!=(ntl=%d)", (uint16_t)be_i16(t.h + oNs), ntl);
       if ((uint16_t)be_i16(t.h + oDt) != (int)(dt * 1.0E6f))
@@ -625,8 +539,7 @@ int main(int argc, char **argv) {
       offmax[id].push_back(b);
     }
   }
-  auto mute = parse_pairs(zmute);
-  mute_sanity(mute);
+  auto mute = mute_pairs(zmute);
 
   logf("q-psdm: node %s gpu %d  image %d cdps x %d lines x %d depths  dx %g dy %g dz %g\n",
        nodename.c_str(), igpu, nxi, nyi, nzi, dxi, dyi, dzi);

@@ -19,6 +19,14 @@ The GPU vectors come from the reference's own psdm_kernel + image_depth_gpu
 traces: per-trace acceptance, spectra and the accumulated stub image.  They
 are written to OUTDIR (default tests/golden/) and copied here by hand when
 they were made on another machine.
+
+    make -C oracle ref
+    python tests/golden/make_golden.py pkg
+
+The driver-utility transcript (pkg_cases.txt, pkg_cases.err): tests/pkg_cases.cpp
+compiled with -DPKG_REF against the reference's psdmpkg.h / segy.h and its
+psdmpkg.cc / segy.cc objects in oracle/_ref, run in an empty directory;
+stdout and stderr as printed.
 """
 from __future__ import annotations
 
@@ -135,9 +143,33 @@ def gpu(outdir: str | None = None) -> None:
         print(name, "accepted", int(acc.sum()), "of", ntr, "img max", float(np.abs(img).max()))
 
 
+def pkg() -> None:
+    import subprocess
+    import tempfile
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    objs = [os.path.join(ref, o) for o in ("psdmpkg.o", "segy.o", "fft.o")]
+    if not all(os.path.exists(o) for o in objs):
+        raise SystemExit("oracle/_ref objects missing: make -C oracle ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = os.path.join(tmp, "pkg_cases_ref")
+        subprocess.run(["g++", "-O2", "-std=c++17", "-DPKG_REF", "-w", "-I" + O.ref_src(),
+                        os.path.join(ROOT, "tests", "pkg_cases.cpp")] + objs
+                       + ["-fopenmp", "-o", exe], check=True)
+        run = os.path.join(tmp, "run")
+        os.mkdir(run)
+        r = subprocess.run([exe], cwd=run, capture_output=True, text=True, check=True)
+    with open(os.path.join(HERE, "pkg_cases.txt"), "w") as f:
+        f.write(r.stdout)
+    with open(os.path.join(HERE, "pkg_cases.err"), "w") as f:
+        f.write(r.stderr)
+    print(f"pkg_cases: {len(r.stdout.splitlines())} lines")
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "cpu"
-    if what == "gpu":
+    if what == "pkg":
+        pkg()
+    elif what == "gpu":
         gpu(sys.argv[2] if len(sys.argv) > 2 else None)
     else:
         cpu()
