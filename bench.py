@@ -90,12 +90,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c5", choices=["c5", "c2"])
+    ap.add_argument("--config", default="c5", choices=["c5", "c3", "c2"])
     ap.add_argument("--form", default="batched", choices=list(FORMS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-c3", action="store_true",
+                    help="skip configuration 3 (uneven gathers) beside the headline")
     ap.add_argument("--only-surrogate", action="store_true",
                     help="time only the surrogate network's kernels (for profiling)")
     ap.add_argument("--only-eikonal", action="store_true",
@@ -163,6 +165,12 @@ class Workload:
 
     def aperture(self):
         return self.synth.aperture_tables(self.HALF_CDPS, self.HALF_LINES)
+
+    def form_batches(self, form: str, nbatch: int):
+        """The distinct batches a form's steps cycle through: (SU records,
+        per-trace apertures or None)."""
+        ns = FORMS[form][0]
+        return [(self.batch(k, ns), None) for k in range(nbatch)]
 
     def batch(self, k: int, nshots: int) -> np.ndarray:
         """SU records (big-endian) of shots k*nshots .. k*nshots+nshots-1."""
@@ -275,6 +283,145 @@ class Config5(Workload):
                 "l2": "flushed (256 MiB write) before every timed step (inputs ~1 GB/batch)"}
 
 
+class Config3(Workload):
+    """Configuration 3: shot gathers of uneven size and aperture through one
+    persistent imaging launch per batch."""
+
+    LINE0 = 376
+    NLINES = 16
+    TABLE_LINES = (376, 392)
+    DTSTAR = 0.0025
+    SURF = 320               # surface-node spacing (m) of the eikonal tables
+    HALF_X, HALF_Y = 2500.0, 1500.0
+    H = 50.0
+    dzii = 80.0
+    nbatch = 4
+    BATCH_TRACES = 81920     # a batched step: whole gathers up to this many traces
+    HALF_CDPS, HALF_LINES = 400, 200  # the offset group's tables: the largest aperture
+
+    def __init__(self, rank=0, tile=(0, 0), variant=0, train_steps=0):
+        super().__init__(rank, tile, variant)
+        sv = self.sv = self.synth.config3(seed=11)
+        y0, y1 = sv.line_y(self.LINE0), sv.line_y(self.LINE0 + self.NLINES - 1)
+        near = np.nonzero((sv.shots[:, 1] >= y0 - self.HALF_Y)
+                          & (sv.shots[:, 1] <= y1 + self.HALF_Y))[0]
+        rng = np.random.default_rng([11, 3])
+        self.shot_ids = near[rng.permutation(near.size)]
+        # each gather's aperture, seeded uniform in [1, 4] km: half-widths
+        # in cdps (x) and lines (y, half of x) as the accuracy samples use
+        ap = np.random.default_rng([11, 33]).uniform(1000.0, 4000.0, size=len(sv.shots))
+        self.ap_m = ap
+        self.ap_half = np.stack([np.rint(ap / sv.dxi), np.rint(0.5 * ap / sv.dyi)],
+                                1).astype(np.int32)
+        self.ntr_shot = int(np.mean([len(sv.gathers[i]) for i in self.shot_ids]))
+        self.tabs = None
+        self.device = 0
+        self._packed = None
+
+    def shot(self, k: int) -> int:
+        return int(self.shot_ids[(self.rank * 7 + k) % len(self.shot_ids)])
+
+    def traces(self, sid, sx, sy, gx, gy):
+        sv = self.sv
+        spos = np.stack([sx, sy], 1).astype(np.float64) * sv.scaled
+        gpos = np.stack([gx, gy], 1).astype(np.float64) * sv.scaled
+        return self.synth.pair_traces_device(sv, spos, gpos, device=self.device,
+                                             seed=3000 + sid)
+
+    def line_y_model(self, L):
+        return L * self.sv.dyi
+
+    def setup(self, dev):
+        """Eikonal / t* tables of the two table lines (config 3's v(z) with its
+        smooth random Q layers) and, per brick line, their interpolation
+        between the lines on the device."""
+        from q_psdm_b200 import surrogate as S
+        from q_psdm_b200 import tables as T
+        import torch
+        sv = self.sv
+        self.device = dev
+        model, bg, qb = self.synth.config_models("c3", h=self.H)
+        t0 = time.perf_counter()
+        coarse = [T.eikonal_line_tables(
+            model, fci=sv.fci, nxi=sv.nxi, dxi=sv.dxi, zmax=(sv.nzi - 1) * sv.dzi,
+            line_y=self.line_y_model(L), dzii=self.dzii, nxi1=16, surf_dx=self.SURF,
+            surf_dy=self.SURF, half_x=self.HALF_X, half_y=self.HALF_Y, h=self.H, background=bg,
+            q_background=qb, device=dev, keep_device=True) for L in self.TABLE_LINES]
+        lo, hi = self.TABLE_LINES
+        plain = []
+        for L in range(self.LINE0, self.LINE0 + self.NLINES):
+            d = coarse[0].as_engine_dict()
+            d["ttt"] = S.lerp_device(coarse[0].dev["ttt"], coarse[1].dev["ttt"], L, lo, hi)
+            d["qqq"] = S.lerp_device(coarse[0].dev["qqq"], coarse[1].dev["qqq"], L, lo, hi)
+            plain.append(d)
+        torch.cuda.synchronize()
+        self.tabs = {"plain": plain, "coarse": coarse, "eikonal_s": time.perf_counter() - t0}
+
+    def form_lines(self, form):
+        if form == "batched":
+            return list(range(self.LINE0, self.LINE0 + self.NLINES))
+        return [self.LINE0 + self.NLINES // 2]
+
+    def tables_for(self, form, L):
+        return self.tabs["plain"][L - self.LINE0]
+
+    def gather(self, k: int):
+        """SU records and per-trace apertures of the k-th gather (seeded order)."""
+        recs = self.batch(k, 1)
+        sid = self.shot(k)
+        return recs, np.repeat(self.ap_half[sid][None], recs.shape[0], axis=0)
+
+    def form_batches(self, form: str, nbatch: int):
+        """batched: whole gathers packed in order up to BATCH_TRACES traces a
+        batch; plain: one gather a step (launch per shot)."""
+        if form != "batched":
+            return [self.gather(k) for k in range(nbatch)]
+        out, k, self._packed = [], 0, []
+        for _ in range(nbatch):
+            rs, aps, n = [], [], 0
+            while True:
+                r, a = self.gather(k)
+                if rs and n + r.shape[0] > self.BATCH_TRACES:
+                    break
+                rs.append(r)
+                aps.append(a)
+                n += r.shape[0]
+                k += 1
+            out.append((np.concatenate(rs), np.concatenate(aps)))
+            self._packed.append((len(rs), n))   # (gathers, traces) of each batch
+        return out
+
+    def sample_batch(self):
+        """The first two gathers (records, apertures) for the accuracy sample."""
+        (r0, a0), (r1, a1) = self.gather(0), self.gather(1)
+        return np.concatenate([r0, r1]), np.concatenate([a0, a1])
+
+    def config(self, form):
+        sv = self.sv
+        _, nl, dtype, pf = FORMS[form]
+        sizes = [len(sv.gathers[i]) for i in self.shot_ids]
+        return {"workload": f"config3 (image {sv.nxi}x{sv.nyi}x{sv.nzi} @10m, "
+                            f"{len(sv.shots)} shot gathers of U[500,12000] traces with "
+                            f"apertures U[1,4] km, nt={sv.ntl}, dt=2ms, v(z) with smooth random "
+                            f"Q layers 25-150), form {form}: "
+                            + (f"whole gathers packed up to {self.BATCH_TRACES} traces "
+                               f"x {nl} image lines per step (one persistent launch per "
+                               f"batch, replayed from a CUDA graph)" if form == "batched" else
+                               "1 gather x 1 image line per step (launch per shot)"),
+                "form": form, "lines_per_step": nl,
+                "gathers": f"{len(self.shot_ids)} gathers whose shots lie within "
+                           f"{self.HALF_Y:.0f} m of the brick, seeded order; sizes "
+                           f"{min(sizes)}..{max(sizes)} (mean {np.mean(sizes):.0f}); each "
+                           f"trace carries its gather's aperture (qpsdm_submit_gathers)",
+                "panels": DTYPE_NAME[dtype],
+                "tables": f"eikonal / t* tables of config 3's model (50 m grid) for lines "
+                          f"{self.TABLE_LINES[0]} and {self.TABLE_LINES[1]} (surface nodes "
+                          f"every {self.SURF} m, depth 80 m), interpolated between the lines on "
+                          f"the device for every brick line",
+                "dtstar_s": self.DTSTAR,
+                "l2": "flushed (256 MiB write) before every timed step"}
+
+
 class Config2(Workload):
     """Configuration 2's geometry with analytic v(z) tables (the previous
     headline, kept for comparison)."""
@@ -328,7 +475,7 @@ class Config2(Workload):
                 "l2": "flushed (256 MiB write) before every timed step"}
 
 
-WORKLOADS = {"c5": Config5, "c2": Config2}
+WORKLOADS = {"c5": Config5, "c3": Config3, "c2": Config2}
 
 
 # ---------------------------------------------------------------------------
@@ -413,7 +560,16 @@ def _kernel_times(eng, _lib):
              ("grouping", _lib.K_OTHER))}
 
 
-def _eager_kernel_times(form, wl, dev, stream, drecs, ntr, flush, nsteps=2):
+def _submit(eng, batch):
+    """One batch of resident records (and per-trace apertures, if any)."""
+    d, a, n = batch
+    if a is None:
+        eng.submit_device(d.data_ptr(), n)
+    else:
+        eng.submit_gathers_device(d.data_ptr(), a.data_ptr(), n)
+
+
+def _eager_kernel_times(form, wl, dev, stream, dbat, max_batch, flush, nsteps=2):
     """Per-kernel CUDA-event times of `nsteps` steps of a second engine that
     runs the batches eagerly (an engine replaying CUDA graphs records no
     events inside them): the per-kernel breakdown and the image kernel's time
@@ -421,8 +577,7 @@ def _eager_kernel_times(form, wl, dev, stream, drecs, ntr, flush, nsteps=2):
     from q_psdm_b200 import _lib
     from q_psdm_b200 import engine as E
     import torch
-    ns = FORMS[form][0]
-    p = wl.static(form, max_batch=ns * wl.ntr_shot)
+    p = wl.static(form, max_batch=max_batch)
     eng = E.Engine(p, device=dev)
     try:
         eng.set_stream(stream.cuda_stream)
@@ -430,12 +585,12 @@ def _eager_kernel_times(form, wl, dev, stream, drecs, ntr, flush, nsteps=2):
         az = wl.aperture()
         eng.begin_offset(E.offset_params(p, 0, p.nxi, aznx1=az[0], aznx2=az[1], azny1=az[2],
                                          azny2=az[3]))
-        eng.submit_device(drecs[0].data_ptr(), ntr)
+        _submit(eng, dbat[0])
         torch.cuda.synchronize()
         eng.profile(True)
         for k in range(nsteps):
             flush.zero_()
-            eng.submit_device(drecs[k % len(drecs)].data_ptr(), ntr)
+            _submit(eng, dbat[k % len(dbat)])
         torch.cuda.synchronize()
         kt = _kernel_times(eng, _lib)
         eng.profile(False)
@@ -449,10 +604,12 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     from q_psdm_b200 import _lib
     from q_psdm_b200 import engine as E
 
-    ns, nl, _, _ = FORMS[form]
     # the batched form replays each batch from a captured CUDA graph
     graph = form == "batched"
-    p = wl.static(form, max_batch=ns * wl.ntr_shot, use_graph=int(graph))
+    nbatch = wl.nbatch if form == "batched" else 2
+    bats = wl.form_batches(form, nbatch)   # [(records, apertures or None)]
+    max_batch = max(r.shape[0] for r, _ in bats)
+    p = wl.static(form, max_batch=max_batch, use_graph=int(graph))
     eng = E.Engine(p, device=dev)
     stream = torch.cuda.Stream()  # non-default: its handle is never 0
     torch.cuda.set_stream(stream)
@@ -461,14 +618,12 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     az = wl.aperture()
     o = E.offset_params(p, 0, p.nxi, aznx1=az[0], aznx2=az[1], azny1=az[2], azny2=az[3])
     eng.begin_offset(o)
-    nbatch = wl.nbatch if form == "batched" else 2
-    recs = [wl.batch(k, ns) for k in range(nbatch)]
-    drecs = [torch.from_numpy(r).cuda() for r in recs]
-    ntr = recs[0].shape[0]
+    dbat = [(torch.from_numpy(r).cuda(), None if a is None else torch.from_numpy(a).cuda(),
+             r.shape[0]) for r, a in bats]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     for k in range(max(warmup, nbatch + 1)):   # every batch eager once, then captured
-        eng.submit_device(drecs[k % nbatch].data_ptr(), ntr)
+        _submit(eng, dbat[k % nbatch])
     torch.cuda.synchronize()
     st0 = eng.stats()
     nacc0, npt0 = st0["accepted"], st0["point_traces"]
@@ -484,7 +639,7 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        eng.submit_device(drecs[k % nbatch].data_ptr(), ntr)
+        _submit(eng, dbat[k % nbatch])
         e1.record(stream)
         ev.append((e0, e1))
     torch.cuda.synchronize()
@@ -499,7 +654,7 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     kms = {k: v[0] / steps for k, v in kt.items()}
     img_launch = kt["image"][0] / max(kt["image"][1], 1)
     if graph:  # kernel times from eager steps of the same batches
-        kte, nst = _eager_kernel_times(form, wl, dev, stream, drecs, ntr, flush)
+        kte, nst = _eager_kernel_times(form, wl, dev, stream, dbat, max_batch, flush)
         kms = {k: v[0] / nst for k, v in kte.items()}
         img_launch = kte["image"][0] / max(kte["image"][1], 1)
     t = torch.tensor([ms, float(npt)], dtype=torch.float64, device="cuda")
@@ -518,6 +673,7 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
                                   kept_fraction=1.0 - pairs["tile_decided"] / max(npt / steps, 1),
                                   imaged_fraction=pairs["imaged"] / max(npt / steps, 1)),
            "launches": int(sum(v[1] for v in kt.values())),
+           "traces_per_step": sum(dbat[k % nbatch][2] for k in range(steps)) / steps,
            "image_ms_per_launch": img_launch,
            "image_launches": kt["image"][1], "npt": npt}
     if form == "batched":
@@ -529,19 +685,28 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     if e2e:
         eng.set_stream(None)
         eng.begin_offset(o)
-        pinned = [torch.empty(r.shape, dtype=torch.uint8).pin_memory() for r in recs]
-        for pr, r in zip(pinned, recs):
+        pinned = [torch.empty(r.shape, dtype=torch.uint8).pin_memory() for r, _ in bats]
+        for pr, (r, _) in zip(pinned, bats):
             pr.numpy()[:] = r
-        hosts = [pr.numpy() for pr in pinned]
-        eng.submit(hosts[0])
+        hosts = [(pr.numpy(), a) for pr, (_, a) in zip(pinned, bats)]
+
+        def host_submit(h):
+            if h[1] is None:
+                eng.submit(h[0])
+            else:
+                eng.submit_gathers(h[0], h[1])
+        host_submit(hosts[0])
         img = eng.get_image(True)
         _, n0 = eng.counters()
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
+        h2d = 0
         for k in range(steps):
-            eng.submit(hosts[k % nbatch])
+            h = hosts[k % nbatch]
+            host_submit(h)
             img = eng.get_image(True)
+            h2d += h[0].nbytes + (0 if h[1] is None else h[1].nbytes)
         t1 = time.perf_counter()
         _, n1 = eng.counters()
         te = torch.tensor([t1 - t0], dtype=torch.float64, device="cuda")
@@ -550,12 +715,12 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
             dist.all_reduce(nn, op=dist.ReduceOp.SUM)
         out["e2e"] = {"value": float(nn.item()) / float(te.item()) / 1e9,
-                      "unit": "Gpoint-traces/s", "h2d_bytes_per_step": int(recs[0].nbytes),
+                      "unit": "Gpoint-traces/s", "h2d_bytes_per_step": int(h2d // steps),
                       "d2h_bytes_per_step": int(img.nbytes),
                       "path": "qpsdm_submit_traces from pinned host SU records (DMA) + "
                               "qpsdm_get_image every step"}
     eng.close()
-    del drecs
+    del dbat
     torch.cuda.set_stream(torch.cuda.default_stream())
     return out
 
@@ -631,6 +796,34 @@ def run_ours(args, rank, world, dist):
         res["config"]["cuda_graph"] = ("each batch replayed from a captured CUDA graph (captured "
                                        "in the warm-up steps); per-kernel times from eager steps")
     return res, wl
+
+
+def run_config3(args, rank, dev, dist):
+    """Configuration 3 beside the headline: uneven gathers with their own
+    apertures, batched (one persistent launch per packed batch, graph
+    replay) against plain (launch per shot), with e2e and an accuracy sample."""
+    import torch
+    wl = Config3(rank)
+    t0 = time.perf_counter()
+    wl.setup(dev)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    steps = max(4, args.steps // 2)
+    b = run_form("batched", wl, args, dev, dist, steps=steps, warmup=args.warmup,
+                 e2e=not args.no_e2e, clocks=False)
+    pl = run_form("plain", wl, args, dev, dist, steps=max(4, steps), warmup=2, e2e=False,
+                  clocks=False)
+    keys = ("value", "ms_per_step", "traces_per_step", "point_traces_per_step",
+            "kernel_ms_per_step", "gate_accepted_per_step", "pairs_per_step")
+    out = {"config": wl.config("batched"),
+           "forms": {"batched": {k: b[k] for k in keys}, "plain": {k: pl[k] for k in keys},
+                     "batched_over_plain": b["value"] / pl["value"]},
+           "e2e": b.get("e2e"), "tuning": b.get("tuning"), "image_launches": b["image_launches"],
+           "batches": [{"gathers": g, "traces": n} for g, n in wl._packed],
+           "steps": steps, "setup_s": setup_s, "eikonal_s": wl.tabs["eikonal_s"]}
+    if rank == 0 and not (args.no_cpu or args.no_accuracy):
+        out["accuracy"] = accuracy_vs_fp64(wl, dev)
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -916,19 +1109,23 @@ def accuracy_vs_fp64(wl, dev, ntr=1200, seed=2):
     from q_psdm_b200 import engine as E
     sv = wl.sv
     line = wl.form_lines("plain")[0]
-    rec = wl.batch(0, 2)
+    rec, ap = wl.sample_batch() if hasattr(wl, "sample_batch") else (wl.batch(0, 2), None)
     rng = np.random.default_rng(seed)
-    rec = np.ascontiguousarray(rec[np.sort(rng.choice(rec.shape[0], ntr, replace=False))])
+    pick = np.sort(rng.choice(rec.shape[0], ntr, replace=False))
+    rec = np.ascontiguousarray(rec[pick])
+    ap = None if ap is None else np.ascontiguousarray(ap[pick])
     hdr, traces = _hdr_traces(rec)
     st = O.derive_static(sv.ntl, np.float32(sv.dt), sv.threshold, 3.0, 8.0)
     filt = O.physics_filter(st["nfft"], np.float32(sv.dt), 130.0, 140.0, sv.fpeak,
                             sv.threshold, 16, wl.DTSTAR)
     dips = [d.ravel() for d in wl.synth.dip_fields(sv.nxi, sv.nzi, float(st["contract"]))]
-    ints, geom = O.gate_traces(_gate_params(O, wl, line), hdr)
+    ints, geom = O.gate_traces(_gate_params(O, wl, line), hdr, ap)
     ok = ints[:, 0] == 3
     pan = O.physics_panels(traces[ok], np.float32(sv.dt), st["nfft"], st["nffti"], filt)
-    out = {"sample": f"{ntr} seeded traces of 2 {sv.name} shot gathers into line {line}; "
-                     f"FP64 oracle: numpy float64 panels + C imaging with the form's own tables"}
+    out = {"sample": f"{ntr} seeded traces of 2 {sv.name} shot gathers into line {line}"
+                     + ("" if ap is None else " (each with its gather's aperture)")
+                     + "; FP64 oracle: numpy float64 panels + C imaging with the form's own "
+                       "tables"}
     for form in ("batched", "plain"):
         tab = wl.tables_for(form, line)
         ref, npt = O.physics_image(_phys_params(O, wl, st, tab), geom[ok], ints[ok][:, [4, 5, 7]],
@@ -943,7 +1140,10 @@ def accuracy_vs_fp64(wl, dev, ntr=1200, seed=2):
             az = wl.aperture()
             eng.begin_offset(E.offset_params(p, 0, p.nxi, aznx1=az[0], aznx2=az[1],
                                              azny1=az[2], azny2=az[3]))
-            eng.submit(rec)
+            if ap is None:
+                eng.submit(rec)
+            else:
+                eng.submit_gathers(rec, ap)
             img = np.asarray(eng.get_image(False), np.float64).reshape(sv.nxi, sv.nzi)
             _, n = eng.counters()
         finally:
@@ -1090,6 +1290,10 @@ def main():
     else:
         res, wl = run_ours(args, rank, world, dist)
         dev = int(os.environ.get("LOCAL_RANK", "0"))
+        if args.config == "c5" and args.form == "batched" and not args.no_c3:
+            c3 = run_config3(args, rank, dev, dist)
+            if res is not None:
+                res["config3"] = c3
         if res is not None and not args.no_surrogate:
             res["surrogate"] = run_surrogate(dev, args.steps, args.warmup)
         if res is not None and not args.no_cpu:

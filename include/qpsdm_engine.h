@@ -203,6 +203,24 @@ int qpsdm_submit_traces(qpsdm_engine *e, const void *records, int ntr, int ns,
 int qpsdm_submit_traces_device(qpsdm_engine *e, const void *d_records, int ntr,
                                int ns, int big_endian);
 
+/* Shot gathers of uneven sizes and apertures in one submit: as
+ * qpsdm_submit_traces(_device), with aperture[2*i], aperture[2*i+1] the
+ * half-width in cdps and in lines of trace i's own aperture (the aperture its
+ * gather was recorded with), which caps the offset group's azimuth tables:
+ * trace i images columns cdpx - min(aznx1[iaz], aperture[2i]) ..
+ * cdpx + min(aznx2[iaz], aperture[2i]) - 1 of the lines with
+ * -min(azny2[iaz], aperture[2i+1]) <= cdpy <= min(azny1[iaz], aperture[2i+1])
+ * (the reference's per-offset-group aperture test, src/q-psdm.cu:2147-2171,
+ * per trace).  A batch of whole gathers is one persistent imaging launch.
+ * aperture: host memory for qpsdm_submit_gathers (copied with the records),
+ * device memory for qpsdm_submit_gathers_device (read when the batch runs; a
+ * captured batch reads it again at every replay).  No counterpart in the
+ * reference. */
+int qpsdm_submit_gathers(qpsdm_engine *e, const void *records, const int *aperture, int ntr,
+                         int ns, int big_endian);
+int qpsdm_submit_gathers_device(qpsdm_engine *e, const void *d_records,
+                                const int *d_aperture, int ntr, int ns, int big_endian);
+
 /* Waits for all submitted work; returns QPSDM_ETIMEOUT / QPSDM_ECUDA on a
  * device-side error. */
 int qpsdm_fence(qpsdm_engine *e);

@@ -85,6 +85,8 @@ def lib():
         L.orc_window_split.restype = None
         L.orc_gate_trace.argtypes = [C.POINTER(GateParams), C.c_int, C.c_int,
                                      C.c_int, C.c_int, _i32p, _f32p]
+        L.orc_gate_trace_cap.argtypes = [C.POINTER(GateParams), C.c_int, C.c_int,
+                                         C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _f32p]
         L.orc_gain.argtypes = [_f32p, C.c_int, C.c_float]
         L.orc_gain.restype = None
         L.orc_fetch_and_taper.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p]
@@ -192,8 +194,10 @@ def preprocess_trace(trace, dt, w):
     return re, im
 
 
-def gate_traces(gp: GateParams, hdr: np.ndarray):
-    """hdr [ntr,4] int32 (sx, sy, gx, gy).  Returns (ints [ntr,8], geom [ntr,4])."""
+def gate_traces(gp: GateParams, hdr: np.ndarray, aperture: np.ndarray | None = None):
+    """hdr [ntr,4] int32 (sx, sy, gx, gy); aperture: optional int32 [ntr,2]
+    per-trace half-widths (cdps, lines) capping the azimuth tables.  Returns
+    (ints [ntr,8], geom [ntr,4])."""
     hdr = np.ascontiguousarray(hdr, np.int32)
     ntr = hdr.shape[0]
     ints = np.zeros((ntr, 8), np.int32)
@@ -201,9 +205,11 @@ def gate_traces(gp: GateParams, hdr: np.ndarray):
     oi = np.zeros(8, np.int32)
     of = np.zeros(4, np.float32)
     L = lib()
+    big = 2 ** 31 - 1
     for i in range(ntr):
-        L.orc_gate_trace(C.byref(gp), int(hdr[i, 0]), int(hdr[i, 1]),
-                         int(hdr[i, 2]), int(hdr[i, 3]), oi, of)
+        cx, cy = (big, big) if aperture is None else (int(aperture[i, 0]), int(aperture[i, 1]))
+        L.orc_gate_trace_cap(C.byref(gp), int(hdr[i, 0]), int(hdr[i, 1]),
+                             int(hdr[i, 2]), int(hdr[i, 3]), cx, cy, oi, of)
         ints[i] = oi
         geom[i] = of
     return ints, geom

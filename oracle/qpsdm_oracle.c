@@ -25,6 +25,7 @@
  * the committed golden vectors in tests/golden/.  The physics-mode oracle
  * (FP64) lives in oracle/physics_oracle.c.
  */
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -208,8 +209,19 @@ typedef struct {
  *          2 = no image column in the block, 3 = accepted
  * out_f: [sx, sy, gx, gy] relative to (fxi, cyi), as the kernel receives them.
  */
+int orc_gate_trace_cap(const orc_gate_params *p, int isx, int isy, int igx,
+                       int igy, int capx, int capy, int *out_i, float *out_f);
+
 int orc_gate_trace(const orc_gate_params *p, int isx, int isy, int igx,
                    int igy, int *out_i, float *out_f) {
+  return orc_gate_trace_cap(p, isx, isy, igx, igy, INT_MAX, INT_MAX, out_i, out_f);
+}
+
+/* The same with the trace's own aperture (half-widths capx cdps, capy
+ * lines) capping the azimuth tables: the engine's per-trace aperture of
+ * gathers recorded with different apertures. */
+int orc_gate_trace_cap(const orc_gate_params *p, int isx, int isy, int igx,
+                       int igy, int capx, int capy, int *out_i, float *out_f) {
   double sx = isx * p->scaled, sy = isy * p->scaled;
   double gx = igx * p->scaled, gy = igy * p->scaled;
   memset(out_i, 0, sizeof(int) * 8);
@@ -235,6 +247,10 @@ int orc_gate_trace(const orc_gate_params *p, int isx, int isy, int igx,
   out_i[3] = iaz;
   int nx1 = p->aznx1[iaz], nx2 = p->aznx2[iaz];
   int ny1 = p->azny1[iaz], ny2 = p->azny2[iaz];
+  if (nx1 > capx) nx1 = capx;
+  if (nx2 > capx) nx2 = capx;
+  if (ny1 > capy) ny1 = capy;
+  if (ny2 > capy) ny2 = capy;
   if (cdpy > ny1 || cdpy < -ny2) return out_i[0] = 1;
 
   /* columns cdpx-nx1 .. cdpx+nx2-1 clipped to [ixstart, ixend); the start

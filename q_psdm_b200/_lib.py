@@ -113,6 +113,8 @@ SYMBOLS = [
     ("qpsdm_begin_offset", _I, [_P, C.POINTER(OffsetParams)]),
     ("qpsdm_submit_traces", _I, [_P, _P, _I, _I, _I]),
     ("qpsdm_submit_traces_device", _I, [_P, _P, _I, _I, _I]),
+    ("qpsdm_submit_gathers", _I, [_P, _P, _P, _I, _I, _I]),
+    ("qpsdm_submit_gathers_device", _I, [_P, _P, _P, _I, _I, _I]),
     ("qpsdm_fence", _I, [_P]),
     ("qpsdm_set_line_mask", _I, [_P, C.c_ulonglong]),
     ("qpsdm_get_image", _I, [_P, _P, _I]),

@@ -62,8 +62,15 @@ __device__ __forceinline__ bool gate_trace(const uint8_t *__restrict__ rec, int 
   o[1] = cdpx;
   o[2] = cdpy;
   o[3] = iaz;
-  const int nx1 = g.az[0][iaz], nx2 = g.az[1][iaz];
-  const int ny1 = g.az[2][iaz], ny2 = g.az[3][iaz];
+  int nx1 = g.az[0][iaz], nx2 = g.az[1][iaz];
+  int ny1 = g.az[2][iaz], ny2 = g.az[3][iaz];
+  if (g.cap) {  // the trace's own aperture caps the offset group's
+    const int cx = g.cap[2 * (size_t)itr], cy = g.cap[2 * (size_t)itr + 1];
+    nx1 = min(nx1, cx);
+    nx2 = min(nx2, cx);
+    ny1 = min(ny1, cy);
+    ny2 = min(ny2, cy);
+  }
   if (cdpy > ny1 || cdpy < -ny2) {
     o[0] = kRejY;
     return false;

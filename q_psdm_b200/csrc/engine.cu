@@ -44,6 +44,8 @@ struct qpsdm_engine {
   float *d_taper200 = nullptr;
   uint8_t *d_rec[2] = {};
   uint8_t *h_stage[2] = {};
+  int *d_cap[2] = {};  // per-trace aperture caps of the staged batch (2 ints each)
+  int *h_cap[2] = {};
   int *d_ints = nullptr;
   float *d_geom = nullptr;
   unsigned *d_err = nullptr;
@@ -67,12 +69,14 @@ struct qpsdm_engine {
   // physics state (physics.cu)
   PhysicsState *phys = nullptr;
   KernelProfiler prof;
-  // CUDA graphs of whole batches, keyed by (record buffer, ntr, big_endian)
+  // CUDA graphs of whole batches, keyed by (record buffer, aperture caps,
+  // ntr, big_endian, line mask)
   struct GraphRec {
     cudaGraphExec_t exec;
     int64_t launches[4];
   };
-  std::map<std::tuple<const void *, int, int, unsigned long long>, GraphRec> graphs;
+  std::map<std::tuple<const void *, const void *, int, int, unsigned long long>, GraphRec>
+      graphs;
   int64_t batches_run = 0;
   int64_t graph_replays = 0;
 };
@@ -176,6 +180,8 @@ extern "C" int qpsdm_engine_create(const qpsdm_static_params *p,
     CKC(cudaEventCreateWithFlags(&e->ev_rec_free[i], cudaEventDisableTiming));
     CKC(cudaMalloc(&e->d_rec[i], e->rec_bytes * e->p.max_batch));
     CKC(cudaMallocHost(&e->h_stage[i], e->rec_bytes * e->p.max_batch));
+    CKC(cudaMalloc(&e->d_cap[i], 2 * sizeof(int) * e->p.max_batch));
+    CKC(cudaMallocHost(&e->h_cap[i], 2 * sizeof(int) * e->p.max_batch));
   }
   CKC(cudaMalloc(&e->d_iaztab, sizeof(int) * naztab));
   CKC(cudaMemcpy(e->d_iaztab, iaztab, sizeof(int) * naztab, cudaMemcpyHostToDevice));
@@ -215,6 +221,8 @@ extern "C" int qpsdm_engine_destroy(qpsdm_engine *e) {
     if (e->ev_rec_free[i]) cudaEventDestroy(e->ev_rec_free[i]);
     if (e->d_rec[i]) cudaFree(e->d_rec[i]);
     if (e->h_stage[i]) cudaFreeHost(e->h_stage[i]);
+    if (e->d_cap[i]) cudaFree(e->d_cap[i]);
+    if (e->h_cap[i]) cudaFreeHost(e->h_cap[i]);
   }
   cudaFree(e->d_iaztab);
   cudaFree(e->d_taper200);
@@ -318,7 +326,7 @@ extern "C" int qpsdm_begin_offset(qpsdm_engine *e, const qpsdm_offset_params *o)
 namespace {
 
 // Kernels of one batch whose records are in device memory.
-int process_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
+int process_batch(qpsdm_engine *e, const uint8_t *d_rec, const int *d_cap, int ntr, int be) {
   const int nlines = (int)e->lines.size();
   const int nxb = e->off.ixend - e->off.ixstart;
   const size_t ints_ls = (size_t)kGateInts * e->p.max_batch;  // per-line strides
@@ -345,6 +353,7 @@ int process_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
     g.ixend = e->off.ixend;
     g.naztab = e->naztab;
     g.iaztab = e->d_iaztab;
+    g.cap = d_cap;
     memcpy(g.az[0], e->off.aznx1, sizeof(int) * QPSDM_NAZ);
     memcpy(g.az[1], e->off.aznx2, sizeof(int) * QPSDM_NAZ);
     memcpy(g.az[2], e->off.azny1, sizeof(int) * QPSDM_NAZ);
@@ -426,13 +435,14 @@ void clear_graphs(qpsdm_engine *e) {
 // One batch: replayed from a CUDA graph when use_graph is set and this
 // (buffer, size) was seen before; captured on its second occurrence (the
 // first runs eagerly so that plans, attributes and the autotuner settle).
-int run_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
+int run_batch(qpsdm_engine *e, const uint8_t *d_rec, const int *d_cap, int ntr, int be) {
   const bool graphs = e->p.use_graph != 0;
   if (!graphs || e->batches_run == 0) {
     ++e->batches_run;
-    return process_batch(e, d_rec, ntr, be);
+    return process_batch(e, d_rec, d_cap, ntr, be);
   }
-  const auto key = std::make_tuple((const void *)d_rec, ntr, be, e->line_mask);
+  const auto key = std::make_tuple((const void *)d_rec, (const void *)d_cap, ntr, be,
+                                   e->line_mask);
   auto it = e->graphs.find(key);
   if (it != e->graphs.end()) {
     CK(cudaGraphLaunch(it->second.exec, e->s_comp));
@@ -446,7 +456,7 @@ int run_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
   const bool prof_on = e->prof.on;
   e->prof.on = false;  // no timing events inside the graph
   CK(cudaStreamBeginCapture(e->s_comp, cudaStreamCaptureModeThreadLocal));
-  const int rc = process_batch(e, d_rec, ntr, be);
+  const int rc = process_batch(e, d_rec, d_cap, ntr, be);
   cudaGraph_t g = nullptr;
   const cudaError_t ce = cudaStreamEndCapture(e->s_comp, &g);
   e->prof.on = prof_on;
@@ -468,8 +478,10 @@ int run_batch(qpsdm_engine *e, const uint8_t *d_rec, int ntr, int be) {
 
 }  // namespace
 
-extern "C" int qpsdm_submit_traces_device(qpsdm_engine *e, const void *d_records,
-                                          int ntr, int ns, int be) {
+namespace {
+
+int submit_device(qpsdm_engine *e, const void *d_records, const int *d_aperture, int ntr,
+                  int ns, int be) {
   if (!e || (!d_records && ntr > 0)) return QPSDM_EINVAL;
   if (!e->offset_set) return fail(e, QPSDM_ESTATE, "submit before begin_offset");
   if (ns != e->p.ntl)
@@ -477,11 +489,11 @@ extern "C" int qpsdm_submit_traces_device(qpsdm_engine *e, const void *d_records
   if (ntr < 0 || ntr > e->p.max_batch) return fail(e, QPSDM_EINVAL, "ntr outside [0, max_batch]");
   if (ntr == 0) return QPSDM_OK;
   DeviceGuard g(e->device);
-  return run_batch(e, (const uint8_t *)d_records, ntr, be);
+  return run_batch(e, (const uint8_t *)d_records, d_aperture, ntr, be);
 }
 
-extern "C" int qpsdm_submit_traces(qpsdm_engine *e, const void *records, int ntr,
-                                   int ns, int be) {
+int submit_host(qpsdm_engine *e, const void *records, const int *aperture, int ntr, int ns,
+                int be) {
   if (!e || (!records && ntr > 0)) return QPSDM_EINVAL;
   if (!e->offset_set) return fail(e, QPSDM_ESTATE, "submit before begin_offset");
   if (ns != e->p.ntl)
@@ -501,22 +513,49 @@ extern "C" int qpsdm_submit_traces(qpsdm_engine *e, const void *records, int ntr
     const int s = e->slot;
     CK(cudaEventSynchronize(e->ev_stage_free[s]));
     if (!pinned) memcpy(e->h_stage[s], src, bytes);
+    if (aperture) memcpy(e->h_cap[s], aperture, 2 * sizeof(int) * n);
     CK(cudaStreamWaitEvent(e->s_copy, e->ev_rec_free[s], 0));
     CK(cudaMemcpyAsync(e->d_rec[s], pinned ? src : e->h_stage[s], bytes,
                        cudaMemcpyHostToDevice, e->s_copy));
+    if (aperture)
+      CK(cudaMemcpyAsync(e->d_cap[s], e->h_cap[s], 2 * sizeof(int) * n,
+                         cudaMemcpyHostToDevice, e->s_copy));
     CK(cudaEventRecord(e->ev_stage_free[s], e->s_copy));
     // a caller's pinned buffer may be reused once the call returns
     if (pinned) CK(cudaEventSynchronize(e->ev_stage_free[s]));
     CK(cudaEventRecord(e->ev_rec_ready[s], e->s_copy));
     CK(cudaStreamWaitEvent(e->s_comp, e->ev_rec_ready[s], 0));
-    int rc = run_batch(e, e->d_rec[s], n, be);
+    int rc = run_batch(e, e->d_rec[s], aperture ? e->d_cap[s] : nullptr, n, be);
     if (rc) return rc;
     CK(cudaEventRecord(e->ev_rec_free[s], e->s_comp));
     e->slot ^= 1;
     src += bytes;
+    if (aperture) aperture += 2 * n;
     ntr -= n;
   }
   return QPSDM_OK;
+}
+
+}  // namespace
+
+extern "C" int qpsdm_submit_traces_device(qpsdm_engine *e, const void *d_records,
+                                          int ntr, int ns, int be) {
+  return submit_device(e, d_records, nullptr, ntr, ns, be);
+}
+
+extern "C" int qpsdm_submit_gathers_device(qpsdm_engine *e, const void *d_records,
+                                           const int *d_aperture, int ntr, int ns, int be) {
+  return submit_device(e, d_records, d_aperture, ntr, ns, be);
+}
+
+extern "C" int qpsdm_submit_gathers(qpsdm_engine *e, const void *records, const int *aperture,
+                                    int ntr, int ns, int be) {
+  return submit_host(e, records, aperture, ntr, ns, be);
+}
+
+extern "C" int qpsdm_submit_traces(qpsdm_engine *e, const void *records, int ntr,
+                                   int ns, int be) {
+  return submit_host(e, records, nullptr, ntr, ns, be);
 }
 
 extern "C" int qpsdm_set_line_mask(qpsdm_engine *e, unsigned long long mask) {

@@ -82,6 +82,9 @@ struct GateArgs {
   int nzi, ixstart, ixend, naztab;
   const int *iaztab;              // device
   int az[4][QPSDM_NAZ];           // aznx1, aznx2, azny1, azny2
+  // device, 2 per trace (half-width in cdps, in lines) capping the azimuth
+  // tables: the aperture a gather was recorded with; null = tables only
+  const int *cap;
 };
 
 int launch_gate(const uint8_t *d_rec, int rec_bytes, int ntr, int big_endian,

@@ -216,6 +216,27 @@ class Engine:
                                                   self.p.ntl, int(big_endian)),
                  "submit_traces_device")
 
+    def submit_gathers(self, records: np.ndarray, aperture: np.ndarray,
+                       big_endian: bool = True) -> None:
+        """Gathers of uneven sizes and apertures: records uint8 [ntr, 240 + 4*ntl],
+        aperture int32 [ntr, 2] = each trace's half-width in cdps and in lines
+        (capping the offset group's azimuth tables)."""
+        records = np.ascontiguousarray(records, np.uint8)
+        aperture = np.ascontiguousarray(aperture, np.int32)
+        ntr = records.shape[0]
+        if aperture.shape != (ntr, 2):
+            raise ValueError("aperture must be int32 [ntr, 2]")
+        ns = (records.shape[1] - 240) // 4
+        self._ck(lib().qpsdm_submit_gathers(self.h, records.ctypes.data, aperture.ctypes.data,
+                                            ntr, ns, int(big_endian)), "submit_gathers")
+
+    def submit_gathers_device(self, d_records: int, d_aperture: int, ntr: int,
+                              big_endian: bool = True) -> None:
+        """Device pointers: records and int32 [ntr, 2] apertures."""
+        self._ck(lib().qpsdm_submit_gathers_device(self.h, C.c_void_p(d_records),
+                                                   C.c_void_p(d_aperture), ntr, self.p.ntl,
+                                                   int(big_endian)), "submit_gathers_device")
+
     def fence(self) -> None:
         self._ck(lib().qpsdm_fence(self.h), "fence")
 

@@ -60,3 +60,38 @@ def test_accuracy_samples_build():
         assert smp["traces"].shape == (64, sv.ntl)
         assert smp["records"].shape == (64, 240 + 4 * sv.ntl)
         assert np.isfinite(smp["tab"].qqq).all() and (smp["tab"].qqq > 0).any()
+
+
+def test_oracle_gate_aperture_cap():
+    """A per-trace aperture caps the azimuth tables: a cap at or above the
+    tables changes nothing; a smaller one narrows the columns to
+    cdpx - cap .. cdpx + cap - 1 and rejects traces whose midpoint line lies
+    beyond the cap."""
+    import ctypes as C
+    from oracle import oracle as O
+    sv = synth.config3(seed=0)
+    line = 384
+    ly = sv.line_y(line)
+    az = np.stack(synth.aperture_tables(200, 100)).astype(np.int32)
+    keep = [O.iaztab()] + [np.ascontiguousarray(az[i]) for i in range(4)]
+    ip = lambda x: x.ctypes.data_as(C.POINTER(C.c_int))
+    gp = O.GateParams(scaled=sv.scaled, fxv1=np.float32(sv.fxv - 2000.0),
+                      fyv1=np.float32(sv.fyv - 1000.0),
+                      exv1=np.float32(sv.fxv + sv.nxi * sv.dxi + 2000.0),
+                      eyv1=np.float32(sv.fyv + sv.nyi * sv.dyi + 1000.0), fxi=sv.fxv, cyi=ly,
+                      dxi=sv.dxi, dyi=sv.dyi, eps=0.001, nzi=sv.nzi, ixstart=0, ixend=sv.nxi,
+                      iaztab=ip(keep[0]), aznx1=ip(keep[1]), aznx2=ip(keep[2]),
+                      azny1=ip(keep[3]), azny2=ip(keep[4]))
+    sx, sy, gx, gy = synth.trace_geometry(sv, [int(np.argmin(np.abs(sv.shots[:, 1] - ly)))])
+    hdr = np.stack([sx, sy, gx, gy], 1).astype(np.int32)[::7]
+    base, _ = O.gate_traces(gp, hdr)
+    same, _ = O.gate_traces(gp, hdr, np.full((len(hdr), 2), 1000, np.int32))
+    assert (same == base).all()
+    cap = np.tile(np.array([[60, 25]], np.int32), (len(hdr), 1))
+    capped, _ = O.gate_traces(gp, hdr, cap)
+    acc_b, acc_c = base[:, 0] == 3, capped[:, 0] == 3
+    assert acc_c.sum() < acc_b.sum() and not (acc_c & ~acc_b).any()
+    assert (np.abs(capped[acc_c, 2]) <= 25).all()
+    cdpx = capped[acc_c, 1]
+    assert (capped[acc_c, 4] >= np.maximum(cdpx - 60, 0)).all()
+    assert (capped[acc_c, 5] <= cdpx + 59).all()
