@@ -83,7 +83,7 @@ struct PhysicsState {
   int variant = -1;          // batched kernel variant (autotuned)
   float *d_tune = nullptr;   // scratch image of the autotuner
   size_t tune_cap = 0;
-  float tune_ms[16] = {};    // autotuner timings per variant (ms)
+  float tune_ms[24] = {};    // autotuner timings per variant (ms)
 };
 
 static size_t dtype_bytes(int t) { return t == QPSDM_PANEL_FP32 ? 4 : 2; }
@@ -1428,6 +1428,342 @@ __global__ void __launch_bounds__(TZ *TX, MB)
   if (npt) add_counts(npt, s_cnt, cnt + cdrop, cdrop, cimg);
 }
 
+// Batched imaging, compacted form.  The same sums as k_image_batched, with
+// the chunk's kept members compacted in member order into shared memory
+// (int4: trace, source slot | FP16 exponent bits, tile-local column range,
+// receiver group), so that every point reads one broadcast record per member
+// instead of scanning the keep mask and loading the member from global
+// memory.  In a uniform tile the point-traces are counted per member in the
+// keep pass (coverage is a tile-level test there); other tiles count per
+// point.  Source terms are two float4 planes per (source, point):
+// A = (T, t* / dtstar, CS = ds^3 / ts, AZ), B = (PX1, PX2, PY1, PY2).  One
+// reciprocal per pair: inv = 1 / (uz r tt) gives both the taper's 1 / uz
+// (r tt inv) and the weight's 1 / (r tt) (uz inv), tt = t^2 (0.01 below
+// 0.1 s).
+template <int TZ, int TX, int MB, int U, int MW, typename T>
+__global__ void __launch_bounds__(TZ *TX, MB)
+    k_image_batched_cl(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
+                       const float *__restrict__ dips, const int *__restrict__ memgrp,
+                       const float2 *__restrict__ grppos, const int4 *__restrict__ mem,
+                       const int *__restrict__ nmem_ptr,
+                       const float2 *__restrict__ srcpos, const int *__restrict__ nsrc_ptr,
+                       const qpsdm_ttt_desc *__restrict__ dt, const float *__restrict__ ttt,
+                       const qpsdm_ttt_desc *__restrict__ dq, const float *__restrict__ qqq,
+                       const float2 *__restrict__ tqp, const T *__restrict__ panels,
+                       int *__restrict__ tile_ctr, int ntz, int ntx, int sc,
+                       unsigned long long *npt) {
+  constexpr int NT = TZ * TX, NW = NT / 32, MC = 32 * MW;
+  static_assert(NT % 32 == 0 && MW % NW == 0, "whole warps, whole words per warp");
+  const int nmem = *nmem_ptr;
+  extern __shared__ float4 smap4[];  // [2][sc][NT]: plane A, plane B
+  __shared__ int4 s_list[MC];        // the chunk's kept members, in member order
+  __shared__ unsigned s_mask[MW];    // kept members of the chunk, one bit each
+  __shared__ int s_wpos[MW + 1];     // kept members before word w (s_wpos[MW]: all)
+  __shared__ int s_col[TX + 1];      // active points of the tile's columns (prefix sums)
+  __shared__ float s_red[13][NW];
+  __shared__ TileGrid s_tg;
+  __shared__ TileBox s_box;  // the tile's box and dip-limit ranges (keep pass only)
+  __shared__ int s_tgw;
+  __shared__ int s_tile;
+  __shared__ unsigned long long s_cnt[3];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int lz = tid % TZ, lx = tid / TZ;
+  const int nsrc = *nsrc_ptr;
+  const float inv_dt1 = 1.0f / a.dt1, inv_dts = 1.0f / a.dtstar;
+  const size_t pstride = (size_t)a.nbins * a.nt;
+  float4 *const planeA = smap4, *const planeB = smap4 + (size_t)sc * NT;
+  unsigned cnt = 0, cdrop = 0, cimg = 0;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) {
+      s_tile = atomicAdd(tile_ctr, 1);
+      s_tgw = -1;
+    }
+    if (tid <= TX) s_col[tid] = 0;
+    __syncthreads();
+    const int tile = s_tile;
+    if (tile >= ntz * ntx) break;
+    const int iz0 = (tile % ntz) * TZ, ixb0 = (tile / ntz) * TX;
+    const int izi = iz0 + lz;
+    const int ixb = ixb0 + lx;
+    const bool live = izi < a.nzi && ixb < a.nxb;
+    const int ixi = ixb + a.ixstart;
+    PointCells pc;
+    pc.ok = false;
+    float tanx1 = 0.f, tanx2 = 0.f, tany1 = 0.f, tany2 = 0.f, acc = 0.f, cmp = 0.f;
+    const float z = izi * a.dzi;
+    if (live) {
+      const size_t k = (size_t)ixi * a.nzi + izi;
+      tanx1 = dips[k];
+      tanx2 = dips[a.nxz + k];
+      tany1 = dips[2 * a.nxz + k];
+      tany2 = dips[3 * a.nxz + k];
+      acc = img[(size_t)ixb * a.nzi + izi];
+      if (comp) cmp = comp[(size_t)ixb * a.nzi + izi];
+      setup_cells(pc, ixi, z, a, dt, dq);
+    }
+    const bool act = live && pc.ok;
+    const float tz = a.taperzone;
+    const float tanx1c = tanx1 - tz * (1.0f + tanx1 * tanx1);
+    const float tanx2c = tanx2 + tz * (1.0f + tanx2 * tanx2);
+    const float tany1c = tany1 - tz * (1.0f + tany1 * tany1);
+    const float tany2c = tany2 + tz * (1.0f + tany2 * tany2);
+    const float iwx1 = 1.0f / (tanx1 - tanx1c), iwx2 = 1.0f / (tanx2c - tanx2);
+    const float iwy1 = 1.0f / (tany1 - tany1c), iwy2 = 1.0f / (tany2c - tany2);
+    const float z2 = z * z;
+    const float x = ixi * a.dxi;
+    {
+      const float big = 3.0e38f;
+      block_min<NW>(act ? tanx1c : big, s_red, 0);
+      block_min<NW>(act ? -tanx1c : big, s_red, 1);
+      block_min<NW>(act ? tanx2c : big, s_red, 2);
+      block_min<NW>(act ? -tanx2c : big, s_red, 3);
+      block_min<NW>(act ? tany1c : big, s_red, 4);
+      block_min<NW>(act ? -tany1c : big, s_red, 5);
+      block_min<NW>(act ? tany2c : big, s_red, 6);
+      block_min<NW>(act ? -tany2c : big, s_red, 7);
+      block_min<NW>(act ? (float)pc.cA : big, s_red, 8);
+      block_min<NW>(act ? -(float)pc.cA : big, s_red, 9);
+      block_min<NW>(act ? (float)pc.cB : big, s_red, 10);
+      block_min<NW>(act ? -(float)pc.cB : big, s_red, 11);
+      block_min<NW>(act ? (pc.same ? 0.0f : -1.0f) : big, s_red, 12);
+      if (act) atomicAdd(&s_col[lx + 1], 1);
+    }
+    __syncthreads();
+    if (tid == 0)
+      for (int c = 1; c <= TX; ++c) s_col[c] += s_col[c - 1];
+    bool uni;
+    {
+      TileBox box;
+      float r[13];
+#pragma unroll
+      for (int k = 0; k < 13; ++k) {
+        r[k] = s_red[k][0];
+#pragma unroll
+        for (int w = 1; w < NW; ++w) r[k] = fminf(r[k], s_red[k][w]);
+      }
+      box.t1lo = r[0], box.t1hi = -r[1], box.t2lo = r[2], box.t2hi = -r[3];
+      box.u1lo = r[4], box.u1hi = -r[5], box.u2lo = r[6], box.u2hi = -r[7];
+      float tmax = 1.0f;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) tmax = fmaxf(tmax, fabsf(r[k]));
+      box.margin = -1e-4f * tmax;
+      const int ncol = min(TX, a.nxb - ixb0), nrow = min(TZ, a.nzi - iz0);
+      box.x0 = (ixb0 + a.ixstart) * a.dxi;
+      box.x1 = (ixb0 + a.ixstart + ncol - 1) * a.dxi;
+      box.z0 = iz0 * a.dzi;
+      box.z1 = (iz0 + nrow - 1) * a.dzi;
+      uni = r[8] == -r[9] && r[10] == -r[11] && r[12] == 0.0f;
+      if (tid == 0) s_box = box;
+      if (uni && act && atomicCAS(&s_tgw, -1, tid) == -1)
+        s_tg = TileGrid{pc.xc, pc.rdx, pc.rdy, pc.hx, pc.hy, pc.nxs, pc.nys};
+    }
+    __syncthreads();
+    if (s_col[TX] == 0) continue;
+    const int ixi_lo = ixb0 + a.ixstart, ixi_hi = ixi_lo + min(TX, a.nxb - ixb0) - 1;
+
+    for (int s0 = 0; s0 < nsrc; s0 += sc) {
+      const int ns = min(sc, nsrc - s0);
+      for (int s = 0; s < ns && act; ++s) {
+        const float2 sp = srcpos[s0 + s];
+        float ts, qs;
+        float4 *mA = planeA + (size_t)s * NT + tid, *mB = planeB + (size_t)s * NT + tid;
+        if (!lookup_tq(pc, dt, ttt, dq, qqq, tqp, a.nxi1, a.nzi1, sp.x, sp.y, ts, qs)) {
+          // no table value: NaN fails every member's dip test
+          *mA = make_float4(NAN, 0.0f, 0.0f, NAN);
+          *mB = make_float4(NAN, NAN, NAN, NAN);
+          continue;
+        }
+        const float dsx = sp.x - x;
+        const float ds = sqrtf(dsx * dsx + sp.y * sp.y + z2);
+        const float rds = __fdividef(1.0f, ds);
+        const float ax = dsx * rds, ay = sp.y * rds, az = z * rds;
+        *mA = make_float4(ts, qs * inv_dts, __fdividef(ds * ds * ds, ts), az);
+        *mB = make_float4(fmaf(-tanx1c, az, ax), fmaf(tanx2c, az, -ax), fmaf(-tany1c, az, ay),
+                          fmaf(tany2c, az, -ay));
+      }
+      for (int pc0 = 0; pc0 < nmem; pc0 += MC) {
+        // keep pass: one bit per member of the chunk
+#pragma unroll 4
+        for (int k = 0; k < MW / NW; ++k) {
+          const int wi = k * NW + warp;
+          const int p = pc0 + 32 * wi + lane;
+          bool keep = false;
+          if (p < nmem) {
+            const int4 mi = __ldg(mem + p);
+            const int sl = (mi.y & 0xFFFFFF) - s0;
+            const int lo = max(mi.z, ixi_lo), hi = min(mi.w, ixi_hi);
+            if (sl >= 0 && sl < ns && lo <= hi) {
+              if (uni) {
+                const float2 sp = __ldg(srcpos + s0 + sl),
+                             gp = __ldg(grppos + __ldg(memgrp + p));
+                if (tile_covers(s_tg, sp) && tile_covers(s_tg, gp)) {
+                  // every active point of columns lo..hi is a point-trace
+                  const unsigned n = s_col[hi - ixi_lo + 1] - s_col[lo - ixi_lo];
+                  cnt += n;
+                  keep = tile_keep(sp, gp, s_box);
+                  if (!keep) cdrop += n;
+                }
+              } else {
+                keep = true;  // several cells in the tile: every point decides alone
+              }
+            }
+          }
+          const unsigned bits = __ballot_sync(0xffffffffu, keep);
+          if (lane == 0) s_mask[wi] = bits;
+        }
+        __syncthreads();
+        if (warp == 0) {  // exclusive prefix of the words' kept counts
+          int run = 0;
+          for (int w0 = 0; w0 < MW; w0 += 32) {
+            const int w = w0 + lane;
+            int c = w < MW ? __popc(s_mask[w]) : 0;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+              const int v = __shfl_up_sync(0xffffffffu, c, off);
+              if (lane >= off) c += v;
+            }
+            if (w < MW) s_wpos[w + 1] = run + c;
+            run += __shfl_sync(0xffffffffu, c, 31);
+          }
+          if (lane == 0) s_wpos[0] = 0;
+        }
+        __syncthreads();
+        // the kept members' records, in member order
+#pragma unroll 4
+        for (int k = 0; k < MW / NW; ++k) {
+          const int wi = k * NW + warp;
+          const unsigned bits = s_mask[wi];
+          if (!((bits >> lane) & 1u)) continue;
+          const int p = pc0 + 32 * wi + lane;
+          const int4 mi = __ldg(mem + p);
+          const int sl = (mi.y & 0xFFFFFF) - s0;
+          const int lo = max(mi.z, ixi_lo) - ixi_lo, hi = min(mi.w, ixi_hi) - ixi_lo;
+          s_list[s_wpos[wi] + __popc(bits & ((1u << lane) - 1u))] =
+              make_int4(mi.x, sl | (int)((unsigned)mi.y & 0xFF000000u), (lo << 16) | hi,
+                        __ldg(memgrp + p));
+        }
+        __syncthreads();
+        const int nkept = s_wpos[MW];
+        if (act && nkept > 0) {
+          int cur = -1;
+          float agx = 0.f, agy = 0.f, agz = 0.f, qx1 = 0.f, qx2 = 0.f, qy1 = 0.f, qy2 = 0.f;
+          float tg = 0.f, qg = 0.f, gfac = 0.f;
+          bool rok = false;
+          int4 nx = s_list[0];
+          for (int k = 0; k < nkept;) {
+            const int g = nx.w;
+            if (g != cur) {
+              cur = g;
+              const float2 gp = __ldg(grppos + g);
+              rok = lookup_tq(pc, dt, ttt, dq, qqq, tqp, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
+              const float dgx = gp.x - x;
+              const float rdg = rsqrtf(dgx * dgx + gp.y * gp.y + z2);
+              agx = dgx * rdg, agy = gp.y * rdg, agz = z * rdg;
+              qx1 = rok ? fmaf(tanx1c, agz, -agx) : NAN;
+              qx2 = fmaf(-tanx2c, agz, agx);
+              qy1 = fmaf(tany1c, agz, -agy);
+              qy2 = fmaf(-tany2c, agz, agy);
+              gfac = tg * rdg * rdg * rdg;
+              qg *= inv_dts;
+            }
+            // up to U kept members of this receiver group
+            int4 rec[U];
+            bool val[U];
+            rec[0] = nx;
+            val[0] = true;
+            ++k;
+            nx = k < nkept ? s_list[k] : make_int4(0, 0, 0, -1);
+#pragma unroll
+            for (int u = 1; u < U; ++u) {
+              val[u] = nx.w == g;
+              rec[u] = nx;
+              if (val[u]) {
+                ++k;
+                nx = k < nkept ? s_list[k] : make_int4(0, 0, 0, -1);
+              }
+            }
+            bool on[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int lo = rec[u].z >> 16, hi = rec[u].z & 0xFFFF;
+              const bool inr = val[u] && (unsigned)(lx - lo) <= (unsigned)(hi - lo);
+              const float4 B = planeB[(size_t)(rec[u].y & 0xFF) * NT + tid];
+              if (!uni) cnt += (inr && rok && B.x == B.x) ? 1u : 0u;
+              on[u] = inr && B.x > qx1 && B.y > qx2 && B.z > qy1 && B.w > qy2;
+            }
+            const T *pp[U];
+            float fwt[U], fwb[U], fac[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              pp[u] = panels;
+              fwt[u] = fwb[u] = fac[u] = 0.0f;
+              if (!on[u]) continue;
+              on[u] = false;
+              const float4 A = planeA[(size_t)(rec[u].y & 0xFF) * NT + tid];
+              const float4 B = planeB[(size_t)(rec[u].y & 0xFF) * NT + tid];
+              const float uz = A.w + agz;
+              const float ex = fminf((B.x - qx1) * iwx1, (B.y - qx2) * iwx2);
+              const float ey = fminf((B.z - qy1) * iwy1, (B.w - qy2) * iwy2);
+              const float t = A.x + tg;
+              const float ft = t * inv_dt1;
+              const int it1 = (int)ft;
+              if (!(it1 > 0 && it1 + 1 < a.nt)) continue;
+              const float fb = fminf(fmaxf(A.y + qg, 0.0f), (float)(a.nbins - 1));
+              const int b0 = min((int)fb, a.nbins - 2);
+              fwt[u] = ft - (float)it1;
+              fwb[u] = fb - (float)b0;
+              pp[u] = panels + (size_t)rec[u].x * pstride + (unsigned)(b0 * a.nt + it1);
+              // w v (r + 1/r) = w (r^2 + 1) 100 / (r tt), tt = t^2 (0.01 below 0.1 s)
+              const float r = A.z * gfac;
+              const float rtt = r * (t > 0.1f ? t * t : 0.01f);
+              const float inv = __fdividef(1.0f, uz * rtt);
+              const float ruz = rtt * inv;
+              const float wt = fminf(1.0f, ex * ruz) * fminf(1.0f, ey * ruz);
+              fac[u] = wt * fmaf(r, r, 1.0f) * (100.0f * uz * inv);
+              if (std::is_same<T, __half>::value)  // 2^e from the record's exponent bits
+                fac[u] *= __int_as_float((int)((((unsigned)rec[u].y >> 24) - 1u) << 23));
+              on[u] = true;
+              ++cimg;
+            }
+            float smp[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              smp[u] = 0.0f;
+              if (on[u]) {
+                const T *q = pp[u];
+                const float p00 = ld_sample<T>(q), p01 = ld_sample<T>(q + 1);
+                const float p10 = ld_sample<T>(q + a.nt), p11 = ld_sample<T>(q + a.nt + 1);
+                const float s0v = p00 + fwt[u] * (p01 - p00), s1v = p10 + fwt[u] * (p11 - p10);
+                smp[u] = s0v + fwb[u] * (s1v - s0v);
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              if (!on[u]) continue;
+              const float v = fac[u] * smp[u];
+              if (comp) {
+                const float y = v - cmp;
+                const float tt = acc + y;
+                cmp = (tt - acc) - y;
+                acc = tt;
+              } else {
+                acc += v;
+              }
+            }
+          }
+        }
+        __syncthreads();  // s_mask, s_wpos and s_list are rewritten by the next chunk
+      }
+    }
+    if (live) {
+      img[(size_t)ixb * a.nzi + izi] = acc;
+      if (comp) comp[(size_t)ixb * a.nzi + izi] = cmp;
+    }
+  }
+  if (npt) add_counts(npt, s_cnt, cnt, cdrop, cimg);
+}
+
 static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p) {
   const int n = p.max_batch;
   bool ok = true;
@@ -1485,17 +1821,22 @@ struct LineView {
 // autotuner times them all on the first batch and keeps the fastest.  (U = 8
 // was slower everywhere tried: the extra registers cost more occupancy than
 // the extra loads in flight gain.)
+// Variants from 13 on are the compacted kernel (k_image_batched_cl) with
+// mw words of 32 members per chunk.
 struct BatchedVariant {
-  int tz, tx, mb, sc, u;
+  int tz, tx, mb, sc, u, cl, mw;
 };
 static const BatchedVariant kVariants[] = {
-    {32, 8, 2, 8, 4}, {32, 4, 4, 8, 4},  {32, 4, 6, 8, 4},  {64, 4, 3, 8, 4},
-    {32, 4, 3, 16, 4}, {8, 16, 4, 8, 4}, {4, 32, 4, 8, 4},  {16, 8, 4, 8, 4},
-    {8, 16, 4, 16, 4}, {16, 8, 3, 16, 4}, {8, 16, 5, 8, 4},  {8, 16, 5, 16, 4},
-    {16, 8, 5, 8, 4},
+    {32, 8, 2, 8, 4, 0, 0},   {32, 4, 4, 8, 4, 0, 0},   {32, 4, 6, 8, 4, 0, 0},
+    {64, 4, 3, 8, 4, 0, 0},   {32, 4, 3, 16, 4, 0, 0},  {8, 16, 4, 8, 4, 0, 0},
+    {4, 32, 4, 8, 4, 0, 0},   {16, 8, 4, 8, 4, 0, 0},   {8, 16, 4, 16, 4, 0, 0},
+    {16, 8, 3, 16, 4, 0, 0},  {8, 16, 5, 8, 4, 0, 0},   {8, 16, 5, 16, 4, 0, 0},
+    {16, 8, 5, 8, 4, 0, 0},   {8, 16, 5, 8, 4, 1, 16},  {8, 16, 4, 8, 4, 1, 32},
+    {16, 8, 5, 8, 4, 1, 16},  {32, 4, 5, 8, 4, 1, 16},  {8, 16, 4, 16, 4, 1, 16},
+    {16, 8, 4, 8, 4, 1, 32},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
-static_assert(kNumVariants <= 16, "tune_ms holds 16 timings");
+static_assert(kNumVariants <= 24, "tune_ms holds 24 timings");
 
 template <int TZ, int TX, int MB, int U, typename T>
 static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
@@ -1519,12 +1860,40 @@ static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const Ph
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
 
+template <int TZ, int TX, int MB, int U, int MW, typename T>
+static int launch_batched_cl(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
+                             const LineView &v, float *img, float *comp,
+                             unsigned long long *npt, int sc, cudaStream_t st) {
+  const int ntz = (a.nzi + TZ - 1) / TZ, ntx = (a.nxb + TX - 1) / TX;
+  const size_t smem = sizeof(float4) * 2 * (size_t)sc * TZ * TX;
+  auto kern = k_image_batched_cl<TZ, TX, MB, U, MW, T>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return QPSDM_ECUDA;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TZ * TX, smem);
+  const int grid = std::max(1, std::min(ntz * ntx, std::max(per_sm, 1) * s->num_sms));
+  cudaMemsetAsync(s->d_tile_ctr, 0, sizeof(int), st);
+  kern<<<grid, TZ * TX, smem, st>>>(img, comp, a, v.dips, s->d_memgrp, s->d_grppos, s->d_mem,
+                                    s->d_nmem, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
+                                    v.tab->ttt, v.tab->dq, v.tab->qqq,
+                                    v.tab->paired ? v.tab->tq : nullptr, (const T *)s->d_panels,
+                                    s->d_tile_ctr, ntz, ntx, sc, npt);
+  return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
+}
+
 template <typename T>
 static int launch_variant(int vi, PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
                           const LineView &v, float *img, float *comp, unsigned long long *npt,
                           cudaStream_t st) {
   const int sc = kVariants[vi].sc;
   switch (vi) {
+    case 13: return launch_batched_cl<8, 16, 5, 4, 16, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 14: return launch_batched_cl<8, 16, 4, 4, 32, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 15: return launch_batched_cl<16, 8, 5, 4, 16, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 16: return launch_batched_cl<32, 4, 5, 4, 16, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 17: return launch_batched_cl<8, 16, 4, 4, 16, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 18: return launch_batched_cl<16, 8, 4, 4, 32, T>(s, a, b, v, img, comp, npt, sc, st);
     case 0: return launch_batched_tile<32, 8, 2, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 1: return launch_batched_tile<32, 4, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 2: return launch_batched_tile<32, 4, 6, 4, T>(s, a, b, v, img, comp, npt, sc, st);
@@ -1537,7 +1906,8 @@ static int launch_variant(int vi, PhysicsState *s, const PhysImageArgs &a, const
     case 9: return launch_batched_tile<16, 8, 3, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 10:
     case 11: return launch_batched_tile<8, 16, 5, 4, T>(s, a, b, v, img, comp, npt, sc, st);
-    default: return launch_batched_tile<16, 8, 5, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 12: return launch_batched_tile<16, 8, 5, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    default: return QPSDM_EINVAL;
   }
 }
 

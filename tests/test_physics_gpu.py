@@ -262,10 +262,11 @@ def test_fp16_panels_any_amplitude(cuda, case, form, gain):
     assert nrmse(img, case["o_img"]) <= 2.5e-4
 
 
-@pytest.mark.parametrize("variant", list(range(1, 14)))
+@pytest.mark.parametrize("variant", list(range(1, 20)))
 def test_every_batched_variant(cuda, case, variant):
     """Each launch variant the autotuner may pick (tile, blocks per SM, source
-    chunk) images the same as the FP64 oracle."""
+    chunk, the original or the compacted kernel) images the same as the FP64
+    oracle."""
     eng, p, o = engine(case, panel_dtype=2, form=1, variant=variant)
     try:
         eng.submit(records(case))
@@ -276,3 +277,22 @@ def test_every_batched_variant(cuda, case, variant):
         eng.close()
     assert npt == case["o_npt"]
     assert nrmse(img, case["o_img"]) <= 2.5e-4
+
+
+@pytest.mark.parametrize("orig,compact", [(11, 14), (13, 16), (2, 17), (9, 18)])
+def test_compacted_kernel_counts_equal_original(cuda, case, orig, compact):
+    """The compacted kernel (kept members listed in shared memory, uniform
+    tiles counted in the keep pass) decides, counts and images exactly the
+    pairs the original kernel does for the same tile shape, and its image
+    agrees with the original's to FP32 rounding."""
+    out = {}
+    for v in (orig, compact):
+        eng, p, o = engine(case, panel_dtype=2, form=1, variant=v)
+        try:
+            eng.submit(records(case))
+            out[v] = (eng.get_image(False), eng.stats())
+        finally:
+            eng.close()
+    (a, sa), (b, sb) = out[orig], out[compact]
+    assert sa == sb
+    assert nrmse(b, a) <= 1e-5
