@@ -75,6 +75,9 @@ struct PhysicsState {
   float2 *d_grppos = nullptr;                  // [max_batch] receiver positions
   int *d_memgrp = nullptr;                     // [max_batch] group of each sorted member
   int *d_tile_ctr = nullptr;
+  int *d_defer = nullptr;    // tiles the fast form leaves to k_image_batched
+  size_t defer_cap = 0;
+  int *d_ndefer = nullptr;
   int *d_nmem = nullptr;                       // accepted members of the current line's batch
   void *d_cub = nullptr;
   size_t cub_bytes = 0;
@@ -202,6 +205,8 @@ void physics_destroy(PhysicsState *s) {
   cudaFree(s->d_grppos);
   cudaFree(s->d_memgrp);
   cudaFree(s->d_tile_ctr);
+  cudaFree(s->d_defer);
+  cudaFree(s->d_ndefer);
   cudaFree(s->d_nmem);
   cudaFree(s->d_cub);
   cudaFree(s->d_filter);
@@ -352,6 +357,13 @@ int physics_begin_offset(PhysicsState *s, const qpsdm_static_params &p,
       !grow_dev(&s->d_tune, &s->tune_cap, (size_t)(o.ixend - o.ixstart) * p.nzi)) {
     if (err) *err = "autotuner scratch allocation failed";
     return QPSDM_ENOMEM;
+  }
+  if (s->form == QPSDM_FORM_BATCHED) {
+    const size_t nxb = (size_t)(o.ixend - o.ixstart);
+    if (!grow_dev(&s->d_defer, &s->defer_cap, nxb * p.nzi / 32 + nxb + p.nzi + 1)) {
+      if (err) *err = "deferred-tile list allocation failed";
+      return QPSDM_ENOMEM;
+    }
   }
   if (p.kahan) {
     const size_t n = (size_t)(o.ixend - o.ixstart) * p.nzi * nlines;
@@ -1112,7 +1124,8 @@ __global__ void __launch_bounds__(TZ *TX, MB)
                     const qpsdm_ttt_desc *__restrict__ dq, const float *__restrict__ qqq,
                     const float2 *__restrict__ tqp, const T *__restrict__ panels,
                     int *__restrict__ tile_ctr, int ntz, int ntx, int sc,
-                    unsigned long long *npt) {
+                    unsigned long long *npt, const int *__restrict__ tile_list,
+                    const int *__restrict__ ntile_list) {
   constexpr int NT = TZ * TX, NW = NT / 32, MC = 32 * NT;
   static_assert(NT % 32 == 0, "whole warps");
   const int nmem = *nmem_ptr;  // the accepted members (sorted first)
@@ -1133,7 +1146,9 @@ __global__ void __launch_bounds__(TZ *TX, MB)
   for (;;) {
     __syncthreads();
     if (tid == 0) {
-      s_tile = atomicAdd(tile_ctr, 1);
+      // the next tile: from the counter, or the next of a list of tiles
+      const int q = atomicAdd(tile_ctr, 1);
+      s_tile = tile_list ? (q < *ntile_list ? tile_list[q] : ntz * ntx) : q;
       s_tgw = -1;
     }
     if (tid <= TX) s_col[tid] = 0;
@@ -1428,21 +1443,47 @@ __global__ void __launch_bounds__(TZ *TX, MB)
   if (npt) add_counts(npt, s_cnt, cnt + cdrop, cdrop, cimg);
 }
 
-// Batched imaging, compacted form.  The same sums as k_image_batched, with
-// the chunk's kept members compacted in member order into shared memory
-// (int4: trace, source slot | FP16 exponent bits, tile-local column range,
-// receiver group), so that every point reads one broadcast record per member
-// instead of scanning the keep mask and loading the member from global
-// memory.  In a uniform tile the point-traces are counted per member in the
-// keep pass (coverage is a tile-level test there); other tiles count per
-// point.  Source terms are two float4 planes per (source, point):
+// Receiver (or source) lookup of a point in a uniform tile with paired
+// (t, t*) tables: the tile's surface grid g, the point's two depth-node
+// blocks pA, pB (the cell's data plus the point's offset inside a surface
+// node's plane) and its depth weight c2.  The arithmetic of lookup_tq.
+__device__ __forceinline__ bool lookup_uni(const TileGrid &g, const float2 *__restrict__ pA,
+                                           const float2 *__restrict__ pB, float c2, int plane,
+                                           float px, float py, float &t, float &q) {
+  float fx, fy;
+  if (!grid_pos(px, py, g.xc, g.rdx, g.rdy, g.hx, g.hy, g.nxs, g.nys, fx, fy)) return false;
+  const int ix = min((int)fx, max(g.nxs - 2, 0));
+  const int iy = min((int)fy, max(g.nys - 2, 0));
+  const float wx = g.nxs > 1 ? __fsub_rn(fx, (float)ix) : 0.0f;
+  const float wy = g.nys > 1 ? __fsub_rn(fy, (float)iy) : 0.0f;
+  const int64_t sx = g.nxs > 1 ? plane : 0, sy = g.nys > 1 ? (int64_t)g.nxs * plane : 0;
+  const int64_t off = (int64_t)(iy * g.nxs + ix) * plane;
+  const float2 a = bilin2(pA, off, sx, sy, wx, wy);
+  const float2 b = bilin2(pB, off, sx, sy, wx, wy);
+  t = lerp(a.x, b.x, c2);
+  q = lerp(a.y, b.y, c2);
+  return true;
+}
+
+// Batched imaging, fast form: the same sums as k_image_batched for the tiles
+// whose active points all read the same table cells of paired (t, t*)
+// tables (with the tables' x-cells and depth cells aligned to the tile shape,
+// every tile); any other tile is appended to defer[] (*ndefer of them) and
+// left to k_image_batched.  The chunk's kept members are compacted in member
+// order into shared memory (int4: trace, source slot | FP16 exponent bits,
+// tile-local column range, receiver group), so that every point reads one
+// broadcast record per member instead of scanning the keep mask and loading
+// the member from global memory; the point-traces are counted per member in
+// the keep pass (coverage is a tile-level test); lookups go through the
+// tile's surface grid in shared memory and the point's two depth-node
+// pointers.  Source terms are two float4 planes per (source, point):
 // A = (T, t* / dtstar, CS = ds^3 / ts, AZ), B = (PX1, PX2, PY1, PY2).  One
 // reciprocal per pair: inv = 1 / (uz r tt) gives both the taper's 1 / uz
 // (r tt inv) and the weight's 1 / (r tt) (uz inv), tt = t^2 (0.01 below
 // 0.1 s).
 template <int TZ, int TX, int MB, int U, int MW, typename T>
 __global__ void __launch_bounds__(TZ *TX, MB)
-    k_image_batched_cl(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
+    k_image_batched_fast(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
                        const float *__restrict__ dips, const int *__restrict__ memgrp,
                        const float2 *__restrict__ grppos, const int4 *__restrict__ mem,
                        const int *__restrict__ nmem_ptr,
@@ -1451,7 +1492,8 @@ __global__ void __launch_bounds__(TZ *TX, MB)
                        const qpsdm_ttt_desc *__restrict__ dq, const float *__restrict__ qqq,
                        const float2 *__restrict__ tqp, const T *__restrict__ panels,
                        int *__restrict__ tile_ctr, int ntz, int ntx, int sc,
-                       unsigned long long *npt) {
+                       unsigned long long *npt, int *__restrict__ defer,
+                       int *__restrict__ ndefer) {
   constexpr int NT = TZ * TX, NW = NT / 32, MC = 32 * MW;
   static_assert(NT % 32 == 0 && MW % NW == 0, "whole warps, whole words per warp");
   const int nmem = *nmem_ptr;
@@ -1560,7 +1602,18 @@ __global__ void __launch_bounds__(TZ *TX, MB)
     }
     __syncthreads();
     if (s_col[TX] == 0) continue;
+    if (!uni) {  // left to k_image_batched
+      if (tid == 0) defer[atomicAdd(ndefer, 1)] = tile;
+      continue;
+    }
     const int ixi_lo = ixb0 + a.ixstart, ixi_hi = ixi_lo + min(TX, a.nxb - ixb0) - 1;
+    const int plane = a.nxi1 * a.nzi1;
+    const float2 *ptA = tqp, *ptB = tqp;
+    if (act) {
+      ptA = tqp + pc.tA + pc.offA;
+      ptB = tqp + pc.tB + pc.offB;
+    }
+    const float c2 = pc.c2;
 
     for (int s0 = 0; s0 < nsrc; s0 += sc) {
       const int ns = min(sc, nsrc - s0);
@@ -1568,7 +1621,7 @@ __global__ void __launch_bounds__(TZ *TX, MB)
         const float2 sp = srcpos[s0 + s];
         float ts, qs;
         float4 *mA = planeA + (size_t)s * NT + tid, *mB = planeB + (size_t)s * NT + tid;
-        if (!lookup_tq(pc, dt, ttt, dq, qqq, tqp, a.nxi1, a.nzi1, sp.x, sp.y, ts, qs)) {
+        if (!lookup_uni(s_tg, ptA, ptB, c2, plane, sp.x, sp.y, ts, qs)) {
           // no table value: NaN fails every member's dip test
           *mA = make_float4(NAN, 0.0f, 0.0f, NAN);
           *mB = make_float4(NAN, NAN, NAN, NAN);
@@ -1594,18 +1647,13 @@ __global__ void __launch_bounds__(TZ *TX, MB)
             const int sl = (mi.y & 0xFFFFFF) - s0;
             const int lo = max(mi.z, ixi_lo), hi = min(mi.w, ixi_hi);
             if (sl >= 0 && sl < ns && lo <= hi) {
-              if (uni) {
-                const float2 sp = __ldg(srcpos + s0 + sl),
-                             gp = __ldg(grppos + __ldg(memgrp + p));
-                if (tile_covers(s_tg, sp) && tile_covers(s_tg, gp)) {
-                  // every active point of columns lo..hi is a point-trace
-                  const unsigned n = s_col[hi - ixi_lo + 1] - s_col[lo - ixi_lo];
-                  cnt += n;
-                  keep = tile_keep(sp, gp, s_box);
-                  if (!keep) cdrop += n;
-                }
-              } else {
-                keep = true;  // several cells in the tile: every point decides alone
+              const float2 sp = __ldg(srcpos + s0 + sl), gp = __ldg(grppos + __ldg(memgrp + p));
+              if (tile_covers(s_tg, sp) && tile_covers(s_tg, gp)) {
+                // every active point of columns lo..hi is a point-trace
+                const unsigned n = s_col[hi - ixi_lo + 1] - s_col[lo - ixi_lo];
+                cnt += n;
+                keep = tile_keep(sp, gp, s_box);
+                if (!keep) cdrop += n;
               }
             }
           }
@@ -1647,19 +1695,22 @@ __global__ void __launch_bounds__(TZ *TX, MB)
         const int nkept = s_wpos[MW];
         if (act && nkept > 0) {
           int cur = -1;
-          float agx = 0.f, agy = 0.f, agz = 0.f, qx1 = 0.f, qx2 = 0.f, qy1 = 0.f, qy2 = 0.f;
+          float agz = 0.f, qx1 = 0.f, qx2 = 0.f, qy1 = 0.f, qy2 = 0.f;
           float tg = 0.f, qg = 0.f, gfac = 0.f;
-          bool rok = false;
-          int4 nx = s_list[0];
           for (int k = 0; k < nkept;) {
-            const int g = nx.w;
+            int4 rec[U];
+            rec[0] = s_list[k];
+            const int g = rec[0].w;
             if (g != cur) {
               cur = g;
+              // receiver terms, once per receiver position (a kept member's
+              // receiver lies on the tile's surface grid)
               const float2 gp = __ldg(grppos + g);
-              rok = lookup_tq(pc, dt, ttt, dq, qqq, tqp, a.nxi1, a.nzi1, gp.x, gp.y, tg, qg);
+              const bool rok = lookup_uni(s_tg, ptA, ptB, c2, plane, gp.x, gp.y, tg, qg);
               const float dgx = gp.x - x;
               const float rdg = rsqrtf(dgx * dgx + gp.y * gp.y + z2);
-              agx = dgx * rdg, agy = gp.y * rdg, agz = z * rdg;
+              const float agx = dgx * rdg, agy = gp.y * rdg;
+              agz = z * rdg;
               qx1 = rok ? fmaf(tanx1c, agz, -agx) : NAN;
               qx2 = fmaf(-tanx2c, agz, agx);
               qy1 = fmaf(tany1c, agz, -agy);
@@ -1668,20 +1719,14 @@ __global__ void __launch_bounds__(TZ *TX, MB)
               qg *= inv_dts;
             }
             // up to U kept members of this receiver group
-            int4 rec[U];
             bool val[U];
-            rec[0] = nx;
             val[0] = true;
             ++k;
-            nx = k < nkept ? s_list[k] : make_int4(0, 0, 0, -1);
 #pragma unroll
             for (int u = 1; u < U; ++u) {
-              val[u] = nx.w == g;
-              rec[u] = nx;
-              if (val[u]) {
-                ++k;
-                nx = k < nkept ? s_list[k] : make_int4(0, 0, 0, -1);
-              }
+              rec[u] = k < nkept ? s_list[k] : make_int4(0, 0, 0, -1);
+              val[u] = rec[u].w == g;
+              if (val[u]) ++k;
             }
             bool on[U];
 #pragma unroll
@@ -1689,7 +1734,6 @@ __global__ void __launch_bounds__(TZ *TX, MB)
               const int lo = rec[u].z >> 16, hi = rec[u].z & 0xFFFF;
               const bool inr = val[u] && (unsigned)(lx - lo) <= (unsigned)(hi - lo);
               const float4 B = planeB[(size_t)(rec[u].y & 0xFF) * NT + tid];
-              if (!uni) cnt += (inr && rok && B.x == B.x) ? 1u : 0u;
               on[u] = inr && B.x > qx1 && B.y > qx2 && B.z > qy1 && B.w > qy2;
             }
             const T *pp[U];
@@ -1782,6 +1826,7 @@ static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p) {
   ok &= cudaMalloc(&s->d_grppos, sizeof(float2) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_memgrp, sizeof(int) * n) == cudaSuccess;
   ok &= cudaMalloc(&s->d_tile_ctr, sizeof(int)) == cudaSuccess;
+  ok &= cudaMalloc(&s->d_ndefer, sizeof(int)) == cudaSuccess;
   ok &= cudaMalloc(&s->d_nmem, sizeof(int)) == cudaSuccess;
   if (!ok) return QPSDM_ENOMEM;
   size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
@@ -1821,8 +1866,9 @@ struct LineView {
 // autotuner times them all on the first batch and keeps the fastest.  (U = 8
 // was slower everywhere tried: the extra registers cost more occupancy than
 // the extra loads in flight gain.)
-// Variants from 13 on are the compacted kernel (k_image_batched_cl) with
-// mw words of 32 members per chunk.
+// Variants from 13 on are the fast form (k_image_batched_fast, with
+// k_image_batched over the tiles it leaves) with mw words of 32 members per
+// chunk.
 struct BatchedVariant {
   int tz, tx, mb, sc, u, cl, mw;
 };
@@ -1833,15 +1879,20 @@ static const BatchedVariant kVariants[] = {
     {16, 8, 3, 16, 4, 0, 0},  {8, 16, 5, 8, 4, 0, 0},   {8, 16, 5, 16, 4, 0, 0},
     {16, 8, 5, 8, 4, 0, 0},   {8, 16, 5, 8, 4, 1, 16},  {8, 16, 4, 8, 4, 1, 32},
     {16, 8, 5, 8, 4, 1, 16},  {32, 4, 5, 8, 4, 1, 16},  {8, 16, 4, 16, 4, 1, 16},
-    {16, 8, 4, 8, 4, 1, 32},
+    {16, 8, 4, 8, 4, 1, 32},  {8, 16, 6, 8, 2, 1, 8},   {8, 16, 6, 8, 4, 1, 8},
+    {16, 8, 6, 8, 2, 1, 8},   {8, 16, 5, 8, 2, 1, 16},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 static_assert(kNumVariants <= 24, "tune_ms holds 24 timings");
 
+// The original kernel over every tile of the image, or (tile_list) over the
+// *ntile_list tiles of a list, with one persistent CTA per SM.
 template <int TZ, int TX, int MB, int U, typename T>
 static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
                                const LineView &v, float *img, float *comp,
-                               unsigned long long *npt, int sc, cudaStream_t st) {
+                               unsigned long long *npt, int sc, cudaStream_t st,
+                               const int *tile_list = nullptr,
+                               const int *ntile_list = nullptr) {
   const int ntz = (a.nzi + TZ - 1) / TZ, ntx = (a.nxb + TX - 1) / TX;
   const size_t smem = sizeof(float2) * kMapN * (size_t)sc * TZ * TX;
   auto kern = k_image_batched<TZ, TX, MB, U, T>;
@@ -1850,23 +1901,30 @@ static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const Ph
     return QPSDM_ECUDA;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TZ * TX, smem);
-  const int grid = std::max(1, std::min(ntz * ntx, std::max(per_sm, 1) * s->num_sms));
+  const int grid = tile_list ? std::max(1, s->num_sms)
+                             : std::max(1, std::min(ntz * ntx, std::max(per_sm, 1) * s->num_sms));
   cudaMemsetAsync(s->d_tile_ctr, 0, sizeof(int), st);
   kern<<<grid, TZ * TX, smem, st>>>(img, comp, a, v.dips, s->d_memgrp, s->d_grppos, s->d_mem,
                                     s->d_nmem, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
                                     v.tab->ttt, v.tab->dq, v.tab->qqq,
                                     v.tab->paired ? v.tab->tq : nullptr, (const T *)s->d_panels,
-                                    s->d_tile_ctr, ntz, ntx, sc, npt);
+                                    s->d_tile_ctr, ntz, ntx, sc, npt, tile_list, ntile_list);
   return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
 }
 
-template <int TZ, int TX, int MB, int U, int MW, typename T>
-static int launch_batched_cl(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
-                             const LineView &v, float *img, float *comp,
-                             unsigned long long *npt, int sc, cudaStream_t st) {
+// The fast form over the image's uniform tiles, then the original kernel
+// (same tile shape, MBO blocks per SM) over the tiles it left; with unpaired
+// tables the original kernel takes every tile.
+template <int TZ, int TX, int MB, int U, int MW, int MBO, typename T>
+static int launch_batched_fast(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
+                               const LineView &v, float *img, float *comp,
+                               unsigned long long *npt, int sc, cudaStream_t st) {
+  if (!v.tab->paired)
+    return launch_batched_tile<TZ, TX, MBO, 4, T>(s, a, b, v, img, comp, npt, sc, st);
   const int ntz = (a.nzi + TZ - 1) / TZ, ntx = (a.nxb + TX - 1) / TX;
+  if ((size_t)ntz * ntx > s->defer_cap) return QPSDM_EINVAL;  // cannot happen: sized per offset
   const size_t smem = sizeof(float4) * 2 * (size_t)sc * TZ * TX;
-  auto kern = k_image_batched_cl<TZ, TX, MB, U, MW, T>;
+  auto kern = k_image_batched_fast<TZ, TX, MB, U, MW, T>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return QPSDM_ECUDA;
@@ -1874,12 +1932,15 @@ static int launch_batched_cl(PhysicsState *s, const PhysImageArgs &a, const Phys
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TZ * TX, smem);
   const int grid = std::max(1, std::min(ntz * ntx, std::max(per_sm, 1) * s->num_sms));
   cudaMemsetAsync(s->d_tile_ctr, 0, sizeof(int), st);
+  cudaMemsetAsync(s->d_ndefer, 0, sizeof(int), st);
   kern<<<grid, TZ * TX, smem, st>>>(img, comp, a, v.dips, s->d_memgrp, s->d_grppos, s->d_mem,
                                     s->d_nmem, s->d_srcpos, s->d_sid + (b.ntr - 1), v.tab->dt,
-                                    v.tab->ttt, v.tab->dq, v.tab->qqq,
-                                    v.tab->paired ? v.tab->tq : nullptr, (const T *)s->d_panels,
-                                    s->d_tile_ctr, ntz, ntx, sc, npt);
-  return cudaGetLastError() == cudaSuccess ? QPSDM_OK : QPSDM_ECUDA;
+                                    v.tab->ttt, v.tab->dq, v.tab->qqq, v.tab->tq,
+                                    (const T *)s->d_panels, s->d_tile_ctr, ntz, ntx, sc, npt,
+                                    s->d_defer, s->d_ndefer);
+  if (cudaGetLastError() != cudaSuccess) return QPSDM_ECUDA;
+  return launch_batched_tile<TZ, TX, MBO, 4, T>(s, a, b, v, img, comp, npt, sc, st, s->d_defer,
+                                                s->d_ndefer);
 }
 
 template <typename T>
@@ -1888,12 +1949,16 @@ static int launch_variant(int vi, PhysicsState *s, const PhysImageArgs &a, const
                           cudaStream_t st) {
   const int sc = kVariants[vi].sc;
   switch (vi) {
-    case 13: return launch_batched_cl<8, 16, 5, 4, 16, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 14: return launch_batched_cl<8, 16, 4, 4, 32, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 15: return launch_batched_cl<16, 8, 5, 4, 16, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 16: return launch_batched_cl<32, 4, 5, 4, 16, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 17: return launch_batched_cl<8, 16, 4, 4, 16, T>(s, a, b, v, img, comp, npt, sc, st);
-    case 18: return launch_batched_cl<16, 8, 4, 4, 32, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 13: return launch_batched_fast<8, 16, 5, 4, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 14: return launch_batched_fast<8, 16, 4, 4, 32, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 15: return launch_batched_fast<16, 8, 5, 4, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 16: return launch_batched_fast<32, 4, 5, 4, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 17: return launch_batched_fast<8, 16, 4, 4, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 18: return launch_batched_fast<16, 8, 4, 4, 32, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 19: return launch_batched_fast<8, 16, 6, 2, 8, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 20: return launch_batched_fast<8, 16, 6, 4, 8, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 21: return launch_batched_fast<16, 8, 6, 2, 8, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 22: return launch_batched_fast<8, 16, 5, 2, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 0: return launch_batched_tile<32, 8, 2, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 1: return launch_batched_tile<32, 4, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 2: return launch_batched_tile<32, 4, 6, 4, T>(s, a, b, v, img, comp, npt, sc, st);

@@ -262,7 +262,7 @@ def test_fp16_panels_any_amplitude(cuda, case, form, gain):
     assert nrmse(img, case["o_img"]) <= 2.5e-4
 
 
-@pytest.mark.parametrize("variant", list(range(1, 20)))
+@pytest.mark.parametrize("variant", list(range(1, 24)))
 def test_every_batched_variant(cuda, case, variant):
     """Each launch variant the autotuner may pick (tile, blocks per SM, source
     chunk, the original or the compacted kernel) images the same as the FP64
@@ -296,3 +296,26 @@ def test_compacted_kernel_counts_equal_original(cuda, case, orig, compact):
     (a, sa), (b, sb) = out[orig], out[compact]
     assert sa == sb
     assert nrmse(b, a) <= 1e-5
+
+
+@pytest.mark.parametrize("fast,orig", [(14, 11), (20, 11), (23, 11), (22, 13), (16, 13), (17, 2)])
+def test_fast_form_defers_straddling_tiles(cuda, fast, orig):
+    """An image block starting at cdp 30 puts table-cell edges (every 16 cdps)
+    inside tiles: the fast form leaves those tiles to the original kernel
+    (a device list of tiles), and the image and every counter equal the
+    original kernel's alone and the FP64 oracle's point-traces."""
+    c = make_case(nshots=2, ixstart=30, ixend=126)
+    ref, npt, _ = oracle_run(c)
+    out = {}
+    for v in (orig, fast):
+        eng, p, o = engine(c, panel_dtype=2, form=1, variant=v)
+        try:
+            eng.submit(records(c))
+            out[v] = (eng.get_image(False), eng.stats())
+        finally:
+            eng.close()
+    (a, sa), (b, sb) = out[orig], out[fast]
+    assert sb["point_traces"] == npt
+    assert sa == sb
+    assert nrmse(b, a) <= 1e-5
+    assert nrmse(b, ref) <= 2.5e-4
