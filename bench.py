@@ -72,7 +72,7 @@ F_PT = {"batched": 64, "plain": 64, "compat": 35}
 # DRAM bytes (read + write) per point-trace of the image kernel, from one ncu
 # capture each (profiles/): scaled to a launch by its point-traces.
 TRAFFIC_B_PER_PT = {
-    "batched": (190.7e6 + 6.6e6) / 1.943e9,   # 2 gathers x 1 line capture
+    "batched": (212.7e6 + 7.9e6) / 5.892e8,   # config 5, 2 gathers x 1 line capture
     "plain": (229.7e6 + 4.9e6) / 9.58e8,      # the plain form's own step
     "compat": 4.55e6 / 9.83e8,                # the compat form's own step
 }
@@ -96,6 +96,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-shape-tune", action="store_true",
+                    help="keep the default batch shape (8 gathers x 16 lines) instead of "
+                         "autotuning it")
+    ap.add_argument("--no-config4", action="store_true",
+                    help="skip the configuration-4 surrogate training beside the headline")
+    ap.add_argument("--config4-full", action="store_true",
+                    help="configuration 4 at full scale (4096 sources x 256^2 x 201 nodes; "
+                         "tens of minutes) instead of the default reduced scale")
     ap.add_argument("--no-c3", action="store_true",
                     help="skip configuration 3 (uneven gathers) beside the headline")
     ap.add_argument("--only-surrogate", action="store_true",
@@ -551,6 +559,34 @@ def fp32_peak_tflops(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def fma_peak_tflops(torch):
+    """Measured FP32 FMA rate: the library's k_fma_rate (16 independent FMA
+    chains per thread, 4 blocks of 512 threads per SM), best of 5 launches
+    timed with CUDA events on the launching stream."""
+    from q_psdm_b200 import _lib
+    L = _lib.lib()
+    f = L.qpsdm_internal_fma_rate
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]
+    nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    blocks = 4 * nsm
+    out = torch.empty(blocks * 512, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    flop = C.c_double(0.0)
+    best = 1e9
+    for k in range(7):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = f(blocks, 4096, out.data_ptr(), C.byref(flop), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            raise RuntimeError(f"qpsdm_internal_fma_rate: {_lib.ERRORS.get(rc, rc)}")
+        if k >= 2:
+            best = min(best, e0.elapsed_time(e1))
+    return flop.value / (best * 1e-3) / 1e12
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -725,6 +761,57 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
     return out
 
 
+# the first candidate is the default shape: the kernel-variant autotuner, which
+# runs once per image shape, times its variants on that shape's first batch
+SHAPE_CANDIDATES = ((8, 16), (4, 16), (8, 8), (16, 8), (16, 16))
+
+
+def tune_shape(wl, dev, steps=2):
+    """Gathers per batch and lines per pass of the batched form, chosen by the
+    project's batch-shape autotuner (q_psdm_b200.autotune) on this workload's
+    own gathers and brick lines; FORMS["batched"] takes the choice."""
+    import torch
+    from q_psdm_b200 import autotune as A
+    from q_psdm_b200 import engine as E
+    _, _, dt, pf = FORMS["batched"]
+    sv = wl.sv
+    stream = torch.cuda.Stream()
+    cands = [(g, nl) for g, nl in SHAPE_CANDIDATES
+             if nl <= wl.NLINES and g * (steps + 1) <= len(wl.shot_ids)]
+    tab_bytes = {}
+
+    def make_engine(g, nl):
+        FORMS["batched"] = (g, nl, dt, pf)
+        p = wl.static("batched", max_batch=g * wl.ntr_shot)
+        eng = E.Engine(p, device=dev)
+        eng.set_stream(stream.cuda_stream)
+        eng.set_lines(wl.lines("batched", p.contract))
+        az = wl.aperture()
+        eng.begin_offset(E.offset_params(p, 0, p.nxi, aznx1=az[0], aznx2=az[1],
+                                         azny1=az[2], azny2=az[3]))
+        return eng, stream
+
+    def batches_of(g):
+        return [(torch.from_numpy(wl.batch(k, g)).cuda(), g * wl.ntr_shot)
+                for k in range(steps + 1)]
+
+    def estimate(g, nl):
+        if not tab_bytes:
+            t = wl.tables_for("batched", wl.LINE0)
+            # t, t* and the (t, t*) pairs on the device
+            tab_bytes["line"] = 4 * (int(t["ttt"].numel()) * 2 + int(t["qqq"].numel()))
+        p = wl.static("batched", max_batch=g * wl.ntr_shot)
+        return A.footprint_bytes(max_batch=g * wl.ntr_shot, nlines=nl, ns=sv.ntl, nfft=p.nfft,
+                                 nffti=p.nffti, nbins=16, panel_bytes=2, nxi=sv.nxi,
+                                 nzi=sv.nzi, table_bytes_per_line=tab_bytes["line"])
+
+    ch = A.tune_batch_shape(make_engine, batches_of, estimate, cands, steps=steps, device=dev)
+    FORMS["batched"] = (ch.gathers, ch.lines, dt, pf)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return ch.as_dict()
+
+
 def run_ours(args, rank, world, dist):
     import torch
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -743,6 +830,20 @@ def run_ours(args, rank, world, dist):
     torch.cuda.synchronize()
     torch.cuda.empty_cache()   # the table generator's scratch
     setup_s = time.perf_counter() - t0
+    shape = None
+    if (args.form == "batched" and args.config == "c5" and not (args.shots or args.lines)
+            and not args.no_shape_tune):
+        t1 = time.perf_counter()
+        shape = tune_shape(wl, dev)
+        shape["tune_s"] = time.perf_counter() - t1
+        if dist:  # every rank runs rank 0's shape
+            import torch
+            t = torch.tensor([shape["gathers"], shape["lines"]], dtype=torch.int64,
+                             device="cuda")
+            dist.broadcast(t, 0)
+            g, nl = (int(v) for v in t.tolist())
+            FORMS["batched"] = (g, nl) + FORMS["batched"][2:]
+            shape["gathers"], shape["lines"] = g, nl
     head = run_form(args.form, wl, args, dev, dist, steps=args.steps, warmup=args.warmup,
                     e2e=not args.no_e2e)
     keys = ("value", "ms_per_step", "point_traces_per_step", "kernel_ms_per_step",
@@ -755,7 +856,8 @@ def run_ours(args, rank, world, dist):
         forms["batched_over_plain"] = head["value"] / pl["value"]
     if rank != 0:
         return None, wl
-    fp32 = fp32_peak_tflops(torch)
+    sgemm = fp32_peak_tflops(torch)
+    fp32 = fma_peak_tflops(torch)
     npt_launch = head["npt"] / max(head["image_launches"], 1)
     achieved = npt_launch * F_PT[args.form] / (head["image_ms_per_launch"] * 1e-3) / 1e12
     peaks = {}
@@ -776,7 +878,10 @@ def run_ours(args, rank, world, dist):
                          "(1 - kept_fraction) execute none of them, pairs that fail the dip "
                          "test or the time window (kept - imaged) about half",
             "kernel_ms_per_launch": head["image_ms_per_launch"],
-            "peak_source": "measured in this run: cuBLAS SGEMM 8192^3, TF32 off (of measured)",
+            "peak_source": "measured in this run: the library's FP32 FMA-chain kernel "
+                           "(k_fma_rate, of measured)",
+            "sgemm_tflops_measured": sgemm,
+            "frac_of_sgemm": achieved / sgemm,
             "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),
             "note": "imaging is a data-dependent FP32 gather/accumulate (not a dense "
                     "contraction, not HBM-bound); DRAM traffic per launch from ncu is in "
@@ -792,6 +897,8 @@ def run_ours(args, rank, world, dist):
            "setup_s": setup_s}
     if "tuning" in head:
         res["config"]["autotuned"] = head["tuning"]
+    if shape is not None:
+        res["config"]["batch_shape_autotuned"] = shape
     if args.form == "batched":
         res["config"]["cuda_graph"] = ("each batch replayed from a captured CUDA graph (captured "
                                        "in the warm-up steps); per-kernel times from eager steps")
@@ -824,6 +931,37 @@ def run_config3(args, rank, dev, dist):
     if rank == 0 and not (args.no_cpu or args.no_accuracy):
         out["accuracy"] = accuracy_vs_fp64(wl, dev)
     return out
+
+
+# ---------------------------------------------------------------------------
+# configuration 4: the surrogate trained on source positions x volume nodes
+# ---------------------------------------------------------------------------
+def run_config4(dev, full=False):
+    """The network trained on the eikonal / t* solver's output for a grid of
+    surface source positions over configuration 2's model (anomalies, 5 Q
+    layers) and judged against the solver between the grid's sources
+    (q_psdm_b200.surrogate.config4_training).  Default scale: 1024 of the
+    4096 positions (every 2nd in x and y, 160 m apart) x 128 x 128 x 101
+    nodes at 40 m; --config4-full: all 4096 x 256 x 256 x 201 at 20 m."""
+    import torch
+    from q_psdm_b200 import surrogate as S
+    from q_psdm_b200 import synth
+    h = 20.0 if full else 40.0
+    wide = dict(xr=(-2800.0, 7900.0), yr=(-2800.0, 7900.0))
+    model = synth.config2_model(h=h, **wide)
+    bg = synth.config2_model(h=h, anomalies=False, layered_q=False, q=80.0, **wide)
+    kw = (dict(stride=1, n=256, nz=201, h=20.0, max_batch=8) if full else
+          dict(stride=2, n=128, nz=101, h=40.0, max_batch=32))
+    sur, r = S.config4_training(model, bg, q_bg=80.0, n_side=64, spacing=80.0,
+                                per_source=4096, steps=4000, batch=8192, held=16,
+                                held_nodes=4096, device=dev, seed=0, **kw)
+    sur.mlp.close()
+    torch.cuda.empty_cache()
+    r["scale"] = ("full" if full else
+                  f"reduced: {r['pairs_solved'] / r['pairs_full']:.4f} of the configuration's "
+                  f"(source, point) pairs solved")
+    r["model"] = "config 2: v(z) = 1800 + 0.5 z with two seeded anomalies, 5 Q layers"
+    return r
 
 
 # ---------------------------------------------------------------------------
@@ -1126,12 +1264,23 @@ def accuracy_vs_fp64(wl, dev, ntr=1200, seed=2):
                      + ("" if ap is None else " (each with its gather's aperture)")
                      + "; FP64 oracle: numpy float64 panels + C imaging with the form's own "
                        "tables"}
-    for form in ("batched", "plain"):
+    refs = {}
+    # the batched form with its FP16 panels, the plain form, and the batched
+    # form with BF16 panels (the panel type the metric names) for comparison
+    for form, dtype in (("batched", None), ("plain", None), ("batched", 1)):
         tab = wl.tables_for(form, line)
-        ref, npt = O.physics_image(_phys_params(O, wl, st, tab), geom[ok], ints[ok][:, [4, 5, 7]],
-                                   pan, dips, _host_tables(tab))
-        ref = np.asarray(ref, np.float64).reshape(sv.nxi, sv.nzi)
-        p = wl.static(form, max_batch=ntr)
+        if form not in refs:
+            ref, npt = O.physics_image(_phys_params(O, wl, st, tab), geom[ok],
+                                       ints[ok][:, [4, 5, 7]], pan, dips, _host_tables(tab))
+            refs[form] = (np.asarray(ref, np.float64).reshape(sv.nxi, sv.nzi), npt)
+        ref, npt = refs[form]
+        saved = FORMS[form]
+        if dtype is not None:
+            FORMS[form] = saved[:2] + (dtype,) + saved[3:]
+        try:
+            p = wl.static(form, max_batch=ntr)
+        finally:
+            FORMS[form] = saved
         eng = E.Engine(p, device=dev)
         try:
             eng.set_lines([dict(fxi=sv.fxv, cyi=sv.line_y(line),
@@ -1149,7 +1298,7 @@ def accuracy_vs_fp64(wl, dev, ntr=1200, seed=2):
         finally:
             eng.close()
         e = float(np.sqrt(np.mean((img - ref) ** 2)) / np.sqrt(np.mean(ref ** 2)))
-        dt_name = DTYPE_NAME[FORMS[form][2]]
+        dt_name = DTYPE_NAME[FORMS[form][2] if dtype is None else dtype]
         out[f"nrmse_{form}_{dt_name}_panels_vs_fp64"] = e
         out[f"point_traces_{form}"] = int(n)
         if n != npt:
@@ -1296,6 +1445,8 @@ def main():
                 res["config3"] = c3
         if res is not None and not args.no_surrogate:
             res["surrogate"] = run_surrogate(dev, args.steps, args.warmup)
+            if not args.no_config4:
+                res["surrogate"]["config4"] = run_config4(dev, full=args.config4_full)
         if res is not None and not args.no_cpu:
             # the CPU leg: the oracle timed on a host sample and, unless
             # --no-accuracy, the oracle's FP64 images of seeded samples (this

@@ -56,6 +56,7 @@ class Candidate:
     point_traces: float = 0.0
     gpt_per_s: float = 0.0
     skipped: str = ""
+    kernel_tuning: dict = None  # the engine's kernel-variant autotuner, if it ran here
 
 
 @dataclass
@@ -63,6 +64,7 @@ class Choice:
     gathers: int
     lines: int
     candidates: list = field(default_factory=list)
+    kernel_tuning: dict = None
 
     def as_dict(self):
         return {"gathers": self.gathers, "lines": self.lines,
@@ -72,7 +74,13 @@ class Choice:
                      "estimate_gb": round(c.estimate_bytes / 1e9, 2),
                      "measured_gb": round(c.measured_bytes / 1e9, 2),
                      **({"skipped": c.skipped} if c.skipped else {})}
-                    for c in self.candidates]}
+                    for c in self.candidates],
+                **({"kernel_variants": {
+                    "tuned_on": next(f"{c.gathers} x {c.lines}" for c in self.candidates
+                                     if c.kernel_tuning),
+                    "variant": self.kernel_tuning["variant"],
+                    "variant_ms": [round(x, 3) for x in self.kernel_tuning["variant_ms"]]}}
+                   if self.kernel_tuning else {})}
 
 
 def tune_batch_shape(make_engine, batches_of, estimate, candidates, *, steps: int = 2,
@@ -105,6 +113,9 @@ def tune_batch_shape(make_engine, batches_of, estimate, candidates, *, steps: in
             eng.submit_device(bats[0][0].data_ptr(), bats[0][1])
             torch.cuda.synchronize()
             c.measured_bytes = int(free0 - torch.cuda.mem_get_info()[0])
+            tu = eng.tuning()
+            if any(x > 0 for x in tu["variant_ms"]):
+                c.kernel_tuning = tu
             s0 = eng.stats()["point_traces"]
             ev = []
             ntr = 0
@@ -131,4 +142,6 @@ def tune_batch_shape(make_engine, batches_of, estimate, candidates, *, steps: in
     if not done:
         raise RuntimeError("batch-shape autotuner: no candidate fits the device")
     best = max(done, key=lambda c: c.gpt_per_s)
-    return Choice(best.gathers, best.lines, out)
+    ch = Choice(best.gathers, best.lines, out)
+    ch.kernel_tuning = next((c.kernel_tuning for c in out if c.kernel_tuning), None)
+    return ch

@@ -652,3 +652,199 @@ def truth_error_sample(sur: Surrogate, model, background, *, q_bg: float, line_y
                 surrogate_max_ms=float(np.abs(en).max()),
                 tables_rms_ms=float(np.sqrt(np.mean(ep ** 2))),
                 tables_max_ms=float(np.abs(ep).max()))
+
+
+# ---------------------------------------------------------------------------
+# configuration 4: the network trained on source positions x volume points
+# ---------------------------------------------------------------------------
+def source_grid(n_side: int, spacing: float, x0: float = 0.0, y0: float = 0.0):
+    """n_side x n_side surface source positions (model x, y) every `spacing` m."""
+    g = x0 + np.arange(n_side) * spacing
+    gy = y0 + np.arange(n_side) * spacing
+    X, Y = np.meshgrid(g, gy, indexing="xy")
+    return np.stack([X.ravel(), Y.ravel()], 1).astype(np.float32)
+
+
+def _local_origin(src, n: int, h: float):
+    """(ox, oy) of each source's n x n horizontal grid, centred on it (a
+    source on the h lattice gets a grid on the same lattice)."""
+    return np.asarray(src, np.float32) - np.float32(((n - 1) // 2) * h)
+
+
+def _solve_grids(L, d_models, src, n: int, nz: int, h: float, max_batch: int, dev, on_batch):
+    """Solves every source on its own n x n x nz grid (spacing h, centred on
+    it), model and background, in batches; on_batch(d_T, d_S, d_Tb, d_Sb,
+    grid, d_sp, s0, ns) sees each batch while it is on the device."""
+    import ctypes as C
+
+    import torch
+    grid = _lib.EikGrid(n, n, nz, h)
+    npt = n * n * nz
+    nb = min(max_batch, len(src))
+    d_T = [torch.empty(nb * npt, dtype=torch.float32, device=dev) for _ in d_models]
+    d_S = [torch.empty(nb * npt, dtype=torch.float32, device=dev) for _ in d_models]
+    d_w = torch.empty(4 * nb * npt + 4, dtype=torch.float32, device=dev)
+    for s0 in range(0, len(src), nb):
+        ns = min(nb, len(src) - s0)
+        sp = np.zeros((ns, 4), np.float32)
+        sp[:, 0:2] = src[s0:s0 + ns]
+        sp[:, 2:4] = _local_origin(src[s0:s0 + ns], n, h)
+        d_sp = torch.from_numpy(sp).to(dev)
+        for k, (dv, dq, mdl) in enumerate(d_models):
+            rc = L.qpsdm_eikonal_solve(dv.data_ptr(), dq.data_ptr(), C.byref(mdl),
+                                       d_sp.data_ptr(), ns, C.byref(grid), 3.0 * h,
+                                       4 * (2 * n + nz), d_w.data_ptr(), d_T[k].data_ptr(),
+                                       d_S[k].data_ptr(), None)
+            _lib.check(rc, what="eikonal_solve")
+        on_batch(d_T[0], d_S[0], d_T[1], d_S[1], grid, d_sp, s0, ns)
+
+
+def config4_training(model, background, *, q_bg: float, n_side: int = 64,
+                     spacing: float = 80.0, stride: int = 1, n: int = 256, nz: int = 201,
+                     h: float = 20.0, per_source: int = 4096, steps: int = 4000,
+                     batch: int = 8192, held: int = 16, held_nodes: int = 4096,
+                     gate_ms: float = 2.0, max_batch: int = 16, device: int = 0,
+                     seed: int = 0):
+    """Configuration 4 end to end on one GPU: the network trained on the
+    traveltimes and t* of a grid of surface source positions (n_side x
+    n_side every `spacing` m; every `stride`-th in x and y is solved) to
+    every node of an n x n x nz volume around each source (spacing h), from
+    the eikonal / t* solver on `model` (background-corrected), then judged
+    against the solver itself at `held` seeded source positions between the
+    grid's sources, `held_nodes` seeded volume nodes each:
+
+    * the network: T and t* predicted from (source, point);
+    * the tables, as the imaging kernels read them: bilinear interpolation
+      in source position between the four surrounding solved sources (the
+      same grids, so the node lies on all five grids);
+    * the gate: the share of judged nodes where the network misses by more
+      than gate_ms (those would keep the tables).
+
+    Samples (per_source per solved source, uniform over its volume) are drawn
+    while each batch of grids is on the device; the set of sources x nodes
+    (n_side^2 x n^2 nz) is never formed.  Returns the trained Surrogate and
+    a dict of sizes, timings and errors (ms)."""
+    import time
+
+    import torch
+    L = _lib.lib()
+    dev = torch.device("cuda", device)
+    src_all = source_grid(n_side, spacing)
+    sel = np.zeros((n_side, n_side), bool)
+    sel[::stride, ::stride] = True
+    src = src_all[sel.ravel()]
+    d_models = []
+    for m in (model, background):
+        d_models.append((torch.from_numpy(np.ascontiguousarray(m.vel, np.float32)).to(dev),
+                         torch.from_numpy(np.ascontiguousarray(m.invq, np.float32)).to(dev),
+                         _lib.EikModel(m.vel.shape[2], m.vel.shape[1], m.vel.shape[0], m.h,
+                                       m.ox, m.oy, m.v0, m.kz)))
+    bg = Background(background.v0, background.kz, q_bg)
+    sampler = EikonalSamples(bg, q_bg, per_source=per_source, device=device, seed=seed)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    _solve_grids(L, d_models, src, n, nz, h, max_batch, dev,
+                 lambda T, S, Tb, Sb, grid, sp, s0, ns: sampler(T, S, Tb, Sb, grid, sp, ns))
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    X, Y = sampler.tensors()
+    sur = train_device(X, Y, bg, steps=steps, batch=batch, seed=seed, device=device)
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
+
+    # judged positions: between solved sources, away from the grid's edge
+    rng = np.random.default_rng([seed, 4])
+    step = spacing * stride
+    lim = (n_side - 1) // stride * step
+    hx = (np.round(rng.uniform(step, lim - step, held) / h) * h).astype(np.float32)
+    hy = (np.round(rng.uniform(step, lim - step, held) / h) * h).astype(np.float32)
+    hsrc = np.stack([hx, hy], 1)
+    # corners: the four solved sources around each judged position
+    ix = np.floor(hx / step).astype(int)
+    iy = np.floor(hy / step).astype(int)
+    corners = []
+    for dy in (0, 1):
+        for dx in (0, 1):
+            corners.append(np.stack([(ix + dx) * step, (iy + dy) * step], 1))
+    corners = np.concatenate(corners).astype(np.float32)      # [4*held] (00,10,01,11)
+    # judged nodes: on the h lattice (all five grids hold them), inside the
+    # judged source's grid and within reach of the corners' grids
+    half = ((n - 1) // 2) * h - step - h
+    nodes = np.empty((held, held_nodes, 3), np.float64)
+    for k in range(held):
+        px = np.round((hx[k] + rng.uniform(-half, half, held_nodes)) / h) * h
+        py = np.round((hy[k] + rng.uniform(-half, half, held_nodes)) / h) * h
+        pz = rng.integers(1, nz, held_nodes) * h
+        nodes[k] = np.stack([px, py, pz], 1)
+
+    def values(points_src, grids_T, grids_S, grids_Tb, grids_Sb, s0, ns, which):
+        """Background-corrected (T, t*) of sources s0..s0+ns-1 at the judged
+        nodes of `which[s]` (index into nodes)."""
+        out_t, out_q = [], []
+        Tm = grids_T.view(-1)
+        for j in range(ns):
+            s = points_src[s0 + j]
+            k = which[s0 + j]
+            o = _local_origin(s[None], n, h)[0]
+            p = nodes[k]
+            li = np.rint((p[:, 0] - o[0]) / h).astype(np.int64)
+            lj = np.rint((p[:, 1] - o[1]) / h).astype(np.int64)
+            lk = np.rint(p[:, 2] / h).astype(np.int64)
+            idx = torch.from_numpy(j * n * n * nz + (lk * n + lj) * n + li).to(dev)
+            T = Tm.index_select(0, idx).double().cpu().numpy()
+            S = grids_S.view(-1).index_select(0, idx).double().cpu().numpy()
+            Tb = grids_Tb.view(-1).index_select(0, idx).double().cpu().numpy()
+            Sb = grids_Sb.view(-1).index_select(0, idx).double().cpu().numpy()
+            r = np.hypot(p[:, 0] - s[0], p[:, 1] - s[1])
+            te = background_time(r, p[:, 2], bg.v0, bg.kz)
+            out_t.append(te + T - Tb)
+            out_q.append(S * (te / q_bg) / np.where(Sb > 0, Sb, 1.0))
+        return out_t, out_q
+
+    pts = np.concatenate([hsrc, corners])
+    which = np.concatenate([np.arange(held), np.tile(np.arange(held), 4)])
+    got_t, got_q = [], []
+
+    def on_batch(T, S, Tb, Sb, grid, sp, s0, ns):
+        a, b = values(pts, T, S, Tb, Sb, s0, ns, which)
+        got_t.extend(a)
+        got_q.extend(b)
+    _solve_grids(L, d_models, pts, n, nz, h, max_batch, dev, on_batch)
+    truth_t, truth_q = got_t[:held], got_q[:held]
+    c_t = [got_t[held * (1 + c):held * (2 + c)] for c in range(4)]
+    c_q = [got_q[held * (1 + c):held * (2 + c)] for c in range(4)]
+    wx = (hx - ix * step) / step
+    wy = (hy - iy * step) / step
+    en_t, en_q, et_t, et_q = [], [], [], []
+    for k in range(held):
+        p = nodes[k]
+        F = np.stack([np.full(held_nodes, hx[k]), np.full(held_nodes, hy[k]), p[:, 0], p[:, 1],
+                      p[:, 2]], 1).astype(np.float32)
+        Tn, Qn = sur.predict(F)
+        tab_t = ((1 - wy[k]) * ((1 - wx[k]) * c_t[0][k] + wx[k] * c_t[1][k])
+                 + wy[k] * ((1 - wx[k]) * c_t[2][k] + wx[k] * c_t[3][k]))
+        tab_q = ((1 - wy[k]) * ((1 - wx[k]) * c_q[0][k] + wx[k] * c_q[1][k])
+                 + wy[k] * ((1 - wx[k]) * c_q[2][k] + wx[k] * c_q[3][k]))
+        en_t.append(Tn - truth_t[k])
+        en_q.append(Qn - truth_q[k])
+        et_t.append(tab_t - truth_t[k])
+        et_q.append(tab_q - truth_q[k])
+    torch.cuda.synchronize(dev)
+    t3 = time.perf_counter()
+    ms = lambda e: np.concatenate(e) * 1e3
+    en_t, en_q, et_t, et_q = ms(en_t), ms(en_q), ms(et_t), ms(et_q)
+    rms = lambda e: float(np.sqrt(np.mean(e ** 2)))
+    full = n_side * n_side * 256 * 256 * 201   # the configuration: 256^3 points (z: 4 km at 20 m)
+    return sur, dict(
+        sources=int(len(src)), sources_full=n_side * n_side, source_spacing_m=float(step),
+        volume_nodes_per_source=n * n * nz, volume=f"{n} x {n} x {nz} nodes at {h:g} m",
+        pairs_solved=int(len(src)) * n * n * nz, pairs_full=full,
+        samples=int(X.shape[0]), train_steps=steps, train_batch=batch,
+        eikonal_s=t1 - t0, train_s=t2 - t1, judge_s=t3 - t2,
+        train_samples_per_s=steps * batch / (t2 - t1),
+        loss_first_last=[sur.history[0][1], sur.history[-1][1]],
+        judged=dict(sources=held, nodes=int(en_t.size)),
+        traveltime_ms=dict(surrogate_rms=rms(en_t), surrogate_max=float(np.abs(en_t).max()),
+                           tables_rms=rms(et_t), tables_max=float(np.abs(et_t).max())),
+        tstar_ms=dict(surrogate_rms=rms(en_q), tables_rms=rms(et_q)),
+        gated_fraction=float(np.mean(np.abs(en_t) > gate_ms)), gate_ms=gate_ms)
