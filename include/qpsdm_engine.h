@@ -238,6 +238,21 @@ int qpsdm_set_line_mask(qpsdm_engine *e, unsigned long long mask);
  * host_img: [nxb][nzi] floats (nxb = ixend - ixstart). */
 int qpsdm_get_image(qpsdm_engine *e, float *host_img, int apply_nsb_scale);
 
+/* The same read as qpsdm_get_image, enqueued instead of waited for, so that
+ * a caller can overlap the next batch's host-to-device copy with this one's
+ * kernels and still read every batch's result (the reference's D2H + host sum
+ * + /nsb of src/q-psdm.cu:1745-1765, which it does once per offset group).
+ * host_img: page-locked host memory (cudaMallocHost / cudaHostRegister) of
+ * [lines][nxb][nzi] floats; the copy runs on the engine's compute stream
+ * after every kernel of the submits so far and before those of any later
+ * submit.  *ticket identifies it; qpsdm_image_wait(e, ticket) returns once
+ * the image is in host_img (divided by nsb if apply_nsb_scale).  At most 4
+ * reads are outstanding: a fifth first waits for the oldest.  host_img must
+ * stay untouched until its wait returns. */
+int qpsdm_get_image_async(qpsdm_engine *e, float *host_img, int apply_nsb_scale,
+                          int64_t *ticket);
+int qpsdm_image_wait(qpsdm_engine *e, int64_t ticket);
+
 /* Device pointer of the block image [nxb][nzi] (FP32) for zero-copy use. */
 int qpsdm_image_device_ptr(qpsdm_engine *e, float **d_img);
 

@@ -118,6 +118,8 @@ SYMBOLS = [
     ("qpsdm_fence", _I, [_P]),
     ("qpsdm_set_line_mask", _I, [_P, C.c_ulonglong]),
     ("qpsdm_get_image", _I, [_P, _P, _I]),
+    ("qpsdm_get_image_async", _I, [_P, _P, _I, C.POINTER(C.c_int64)]),
+    ("qpsdm_image_wait", _I, [_P, C.c_int64]),
     ("qpsdm_image_device_ptr", _I, [_P, C.POINTER(C.c_void_p)]),
     ("qpsdm_set_stream", _I, [_P, _P]),
     ("qpsdm_tuning_info", _I, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),

@@ -79,6 +79,18 @@ struct qpsdm_engine {
       graphs;
   int64_t batches_run = 0;
   int64_t graph_replays = 0;
+  // asynchronous image reads (qpsdm_get_image_async): a ring of outstanding
+  // copies, ticket t in slot t % kReads
+  static constexpr int kReads = 4;
+  struct ImageRead {
+    cudaEvent_t done = nullptr;
+    float *host = nullptr;
+    size_t n = 0;
+    int scale = 0;
+    int64_t ticket = -1;
+  };
+  ImageRead reads[kReads];
+  int64_t next_ticket = 0;
 };
 
 namespace {
@@ -214,6 +226,8 @@ extern "C" int qpsdm_engine_destroy(qpsdm_engine *e) {
   if (e->s_comp) cudaStreamSynchronize(e->s_comp);
   if (e->s_copy) cudaStreamSynchronize(e->s_copy);
   clear_graphs(e);
+  for (auto &r : e->reads)
+    if (r.done) cudaEventDestroy(r.done);
   if (e->phys) physics_destroy(e->phys);
   for (int i = 0; i < 2; ++i) {
     if (e->ev_stage_free[i]) cudaEventDestroy(e->ev_stage_free[i]);
@@ -596,6 +610,59 @@ extern "C" int qpsdm_get_image(qpsdm_engine *e, float *host_img, int apply_nsb_s
   if (apply_nsb_scale)
     for (size_t i = 0; i < n; ++i) host_img[i] /= e->off.nsb;  // src/q-psdm.cu:1761-1765
   return QPSDM_OK;
+}
+
+namespace {
+
+// Waits for the read in ring slot r and applies its /nsb scale on the host.
+int finish_read(qpsdm_engine *e, qpsdm_engine::ImageRead &r) {
+  if (r.ticket < 0) return QPSDM_OK;
+  CK(cudaEventSynchronize(r.done));
+  if (r.scale)
+    for (size_t i = 0; i < r.n; ++i) r.host[i] /= e->off.nsb;  // src/q-psdm.cu:1761-1765
+  r.ticket = -1;
+  return QPSDM_OK;
+}
+
+}  // namespace
+
+extern "C" int qpsdm_get_image_async(qpsdm_engine *e, float *host_img, int apply_nsb_scale,
+                                     int64_t *ticket) {
+  if (!e || !host_img || !ticket) return QPSDM_EINVAL;
+  if (!e->offset_set) return fail(e, QPSDM_ESTATE, "get_image_async before begin_offset");
+  DeviceGuard g(e->device);
+  cudaPointerAttributes pa;
+  if (cudaPointerGetAttributes(&pa, host_img) != cudaSuccess ||
+      pa.type != cudaMemoryTypeHost) {
+    cudaGetLastError();
+    return fail(e, QPSDM_EINVAL, "get_image_async needs page-locked host memory");
+  }
+  const size_t n = (size_t)(e->off.ixend - e->off.ixstart) * e->p.nzi * e->lines.size();
+  qpsdm_engine::ImageRead &r = e->reads[e->next_ticket % qpsdm_engine::kReads];
+  int rc = finish_read(e, r);  // the oldest read still in this slot
+  if (rc) return rc;
+  if (!r.done) CK(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming));
+  if (e->p.mode == QPSDM_MODE_PHYSICS) {
+    rc = physics_finalize_image(e->phys, e->d_img, n, e->s_comp, &e->err);
+    if (rc) return rc;
+  }
+  CK(cudaMemcpyAsync(host_img, e->d_img, sizeof(float) * n, cudaMemcpyDeviceToHost,
+                     e->s_comp));
+  CK(cudaEventRecord(r.done, e->s_comp));
+  r.host = host_img;
+  r.n = n;
+  r.scale = apply_nsb_scale != 0;
+  r.ticket = e->next_ticket;
+  *ticket = e->next_ticket++;
+  return QPSDM_OK;
+}
+
+extern "C" int qpsdm_image_wait(qpsdm_engine *e, int64_t ticket) {
+  if (!e || ticket < 0 || ticket >= e->next_ticket) return QPSDM_EINVAL;
+  DeviceGuard g(e->device);
+  qpsdm_engine::ImageRead &r = e->reads[ticket % qpsdm_engine::kReads];
+  if (r.ticket != ticket) return QPSDM_OK;  // finished already (or reused after finishing)
+  return finish_read(e, r);
 }
 
 extern "C" int qpsdm_set_stream(qpsdm_engine *e, void *stream) {

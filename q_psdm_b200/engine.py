@@ -253,6 +253,25 @@ class Engine:
                  "get_image")
         return img[0] if nl == 1 else img
 
+    def image_shape(self):
+        """Shape of the full image buffer: (nlines, nxb, nzi)."""
+        return (getattr(self, "nlines", 1), self.off.ixend - self.off.ixstart, self.p.nzi)
+
+    def get_image_async(self, host_img: np.ndarray, apply_nsb_scale: bool = True) -> int:
+        """Enqueue the image read into host_img (a page-locked float32 array
+        of image_shape(), e.g. a pinned torch tensor's numpy view); returns
+        the ticket for image_wait.  host_img must stay untouched until then."""
+        assert host_img.dtype == np.float32 and host_img.flags.c_contiguous
+        assert host_img.size == int(np.prod(self.image_shape()))
+        t = C.c_int64(-1)
+        self._ck(lib().qpsdm_get_image_async(self.h, host_img.ctypes.data,
+                                             int(apply_nsb_scale), C.byref(t)),
+                 "get_image_async")
+        return t.value
+
+    def image_wait(self, ticket: int) -> None:
+        self._ck(lib().qpsdm_image_wait(self.h, int(ticket)), "image_wait")
+
     def set_stream(self, stream_handle: int | None) -> None:
         """Run engine kernels on a caller stream (e.g. torch's
         ``torch.cuda.current_stream().cuda_stream``); None = the engine's own."""
