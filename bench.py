@@ -965,7 +965,7 @@ def run_config3(args, rank, dev, dist):
 def run_config4(dev, full=False):
     """The network trained on the eikonal / t* solver's output for a grid of
     surface source positions over configuration 2's model (anomalies, 5 Q
-    layers) and judged against the solver between the grid's sources
+    layers) and evaluated against the solver between the grid's sources
     (q_psdm_b200.surrogate.config4_training).  Default scale: 1024 of the
     4096 positions (every 2nd in x and y, 160 m apart) x 128 x 128 x 101
     nodes at 40 m; --config4-full: all 4096 x 256 x 256 x 201 at 20 m."""

@@ -709,7 +709,7 @@ def config4_training(model, background, *, q_bg: float, n_side: int = 64,
     traveltimes and t* of a grid of surface source positions (n_side x
     n_side every `spacing` m; every `stride`-th in x and y is solved) to
     every node of an n x n x nz volume around each source (spacing h), from
-    the eikonal / t* solver on `model` (background-corrected), then judged
+    the eikonal / t* solver on `model` (background-corrected), then evaluated
     against the solver itself at `held` seeded source positions between the
     grid's sources, `held_nodes` seeded volume nodes each:
 
@@ -717,7 +717,7 @@ def config4_training(model, background, *, q_bg: float, n_side: int = 64,
     * the tables, as the imaging kernels read them: bilinear interpolation
       in source position between the four surrounding solved sources (the
       same grids, so the node lies on all five grids);
-    * the gate: the share of judged nodes where the network misses by more
+    * the gate: the share of evaluated nodes where the network misses by more
       than gate_ms (those would keep the tables).
 
     Samples (per_source per solved source, uniform over its volume) are drawn
@@ -752,14 +752,14 @@ def config4_training(model, background, *, q_bg: float, n_side: int = 64,
     torch.cuda.synchronize(dev)
     t2 = time.perf_counter()
 
-    # judged positions: between solved sources, away from the grid's edge
+    # evaluated positions: between solved sources, away from the grid's edge
     rng = np.random.default_rng([seed, 4])
     step = spacing * stride
     lim = (n_side - 1) // stride * step
     hx = (np.round(rng.uniform(step, lim - step, held) / h) * h).astype(np.float32)
     hy = (np.round(rng.uniform(step, lim - step, held) / h) * h).astype(np.float32)
     hsrc = np.stack([hx, hy], 1)
-    # corners: the four solved sources around each judged position
+    # corners: the four solved sources around each evaluated position
     ix = np.floor(hx / step).astype(int)
     iy = np.floor(hy / step).astype(int)
     corners = []
@@ -767,8 +767,8 @@ def config4_training(model, background, *, q_bg: float, n_side: int = 64,
         for dx in (0, 1):
             corners.append(np.stack([(ix + dx) * step, (iy + dy) * step], 1))
     corners = np.concatenate(corners).astype(np.float32)      # [4*held] (00,10,01,11)
-    # judged nodes: on the h lattice (all five grids hold them), inside the
-    # judged source's grid and within reach of the corners' grids
+    # evaluated nodes: on the h lattice (all five grids hold them), inside the
+    # evaluated source's grid and within reach of the corners' grids
     half = ((n - 1) // 2) * h - step - h
     nodes = np.empty((held, held_nodes, 3), np.float64)
     for k in range(held):
@@ -778,7 +778,7 @@ def config4_training(model, background, *, q_bg: float, n_side: int = 64,
         nodes[k] = np.stack([px, py, pz], 1)
 
     def values(points_src, grids_T, grids_S, grids_Tb, grids_Sb, s0, ns, which):
-        """Background-corrected (T, t*) of sources s0..s0+ns-1 at the judged
+        """Background-corrected (T, t*) of sources s0..s0+ns-1 at the evaluated
         nodes of `which[s]` (index into nodes)."""
         out_t, out_q = [], []
         Tm = grids_T.view(-1)
@@ -840,10 +840,10 @@ def config4_training(model, background, *, q_bg: float, n_side: int = 64,
         volume_nodes_per_source=n * n * nz, volume=f"{n} x {n} x {nz} nodes at {h:g} m",
         pairs_solved=int(len(src)) * n * n * nz, pairs_full=full,
         samples=int(X.shape[0]), train_steps=steps, train_batch=batch,
-        eikonal_s=t1 - t0, train_s=t2 - t1, judge_s=t3 - t2,
+        eikonal_s=t1 - t0, train_s=t2 - t1, eval_s=t3 - t2,
         train_samples_per_s=steps * batch / (t2 - t1),
         loss_first_last=[sur.history[0][1], sur.history[-1][1]],
-        judged=dict(sources=held, nodes=int(en_t.size)),
+        evaluated=dict(sources=held, nodes=int(en_t.size)),
         traveltime_ms=dict(surrogate_rms=rms(en_t), surrogate_max=float(np.abs(en_t).max()),
                            tables_rms=rms(et_t), tables_max=float(np.abs(et_t).max())),
         tstar_ms=dict(surrogate_rms=rms(en_q), tables_rms=rms(et_q)),

@@ -1,7 +1,7 @@
 """Configuration 4 at a reduced, stated scale: the network trained on the
 eikonal / t* solver's traveltimes from a grid of surface source positions to
 every node of a volume around each (config-2 model: velocity anomalies and
-5 Q layers), then judged against the solver at seeded source positions
+5 Q layers), then evaluated against the solver at seeded source positions
 between the grid's sources.  Scale here: 64 of the 4096 source positions
 (every 8th in x and y, 640 m apart) x 64 x 64 x 51 nodes at 40 m (of 256^3),
 so about 0.08 % of the configuration's (source, point) pairs; the bench's
