@@ -38,6 +38,29 @@
 
 namespace qpsdm {
 
+// One set of the batched form's grouping buffers (receiver keys, members,
+// source positions, tile queue, deferred-tile list).  Consecutive image lines
+// of a brick alternate between two sets, so that a line's grouping and image
+// kernels can run on a second stream beside the previous line's: the tail of
+// one line's persistent launch overlaps the start of the next.
+struct GroupSet {
+  unsigned long long *d_key[2] = {};
+  int *d_val[2] = {};
+  unsigned long long *d_ukey = nullptr;
+  int *d_count = nullptr, *d_off = nullptr, *d_nruns = nullptr;
+  int *d_srcflag = nullptr, *d_sid = nullptr;
+  float2 *d_srcpos = nullptr;
+  int4 *d_mem = nullptr;
+  float2 *d_grppos = nullptr;
+  int *d_memgrp = nullptr;
+  int *d_tile_ctr = nullptr;
+  int *d_defer = nullptr;
+  size_t defer_cap = 0;
+  int *d_ndefer = nullptr;
+  int *d_nmem = nullptr;
+  void *d_cub = nullptr;
+};
+
 struct PhysicsState {
   int nfft = 0, nffti = 0, nbins = 0, max_batch = 0, dtype = 0;
   float dtstar = 0.0f;
@@ -87,7 +110,39 @@ struct PhysicsState {
   float *d_tune = nullptr;   // scratch image of the autotuner
   size_t tune_cap = 0;
   float tune_ms[24] = {};    // autotuner timings per variant (ms)
+  // the two grouping sets (the d_key .. d_cub fields above are the selected
+  // one) and the second stream of the line loop
+  GroupSet sets[2];
+  int cur_set = 0;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
+
+// Points the grouping fields at set i (the launches enqueued afterwards use it).
+static void select_set(PhysicsState *s, int i) {
+  const GroupSet &g = s->sets[i];
+  for (int k = 0; k < 2; ++k) {
+    s->d_key[k] = g.d_key[k];
+    s->d_val[k] = g.d_val[k];
+  }
+  s->d_ukey = g.d_ukey;
+  s->d_count = g.d_count;
+  s->d_off = g.d_off;
+  s->d_nruns = g.d_nruns;
+  s->d_srcflag = g.d_srcflag;
+  s->d_sid = g.d_sid;
+  s->d_srcpos = g.d_srcpos;
+  s->d_mem = g.d_mem;
+  s->d_grppos = g.d_grppos;
+  s->d_memgrp = g.d_memgrp;
+  s->d_tile_ctr = g.d_tile_ctr;
+  s->d_defer = g.d_defer;
+  s->defer_cap = g.defer_cap;
+  s->d_ndefer = g.d_ndefer;
+  s->d_nmem = g.d_nmem;
+  s->d_cub = g.d_cub;
+  s->cur_set = i;
+}
 
 static size_t dtype_bytes(int t) { return t == QPSDM_PANEL_FP32 ? 4 : 2; }
 static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p);
@@ -190,25 +245,31 @@ int physics_create(PhysicsState **out, const qpsdm_static_params &p, std::string
 
 void physics_destroy(PhysicsState *s) {
   if (!s) return;
-  for (int i = 0; i < 2; ++i) {
-    cudaFree(s->d_key[i]);
-    cudaFree(s->d_val[i]);
+  if (s->aux) cudaStreamSynchronize(s->aux);
+  for (GroupSet &g : s->sets) {
+    for (int i = 0; i < 2; ++i) {
+      cudaFree(g.d_key[i]);
+      cudaFree(g.d_val[i]);
+    }
+    cudaFree(g.d_ukey);
+    cudaFree(g.d_count);
+    cudaFree(g.d_off);
+    cudaFree(g.d_nruns);
+    cudaFree(g.d_srcflag);
+    cudaFree(g.d_sid);
+    cudaFree(g.d_srcpos);
+    cudaFree(g.d_mem);
+    cudaFree(g.d_grppos);
+    cudaFree(g.d_memgrp);
+    cudaFree(g.d_tile_ctr);
+    cudaFree(g.d_defer);
+    cudaFree(g.d_ndefer);
+    cudaFree(g.d_nmem);
+    cudaFree(g.d_cub);
   }
-  cudaFree(s->d_ukey);
-  cudaFree(s->d_count);
-  cudaFree(s->d_off);
-  cudaFree(s->d_nruns);
-  cudaFree(s->d_srcflag);
-  cudaFree(s->d_sid);
-  cudaFree(s->d_srcpos);
-  cudaFree(s->d_mem);
-  cudaFree(s->d_grppos);
-  cudaFree(s->d_memgrp);
-  cudaFree(s->d_tile_ctr);
-  cudaFree(s->d_defer);
-  cudaFree(s->d_ndefer);
-  cudaFree(s->d_nmem);
-  cudaFree(s->d_cub);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->aux) cudaStreamDestroy(s->aux);
   cudaFree(s->d_filter);
   cudaFree(s->d_spec);
   cudaFree(s->d_fmax);
@@ -360,10 +421,12 @@ int physics_begin_offset(PhysicsState *s, const qpsdm_static_params &p,
   }
   if (s->form == QPSDM_FORM_BATCHED) {
     const size_t nxb = (size_t)(o.ixend - o.ixstart);
-    if (!grow_dev(&s->d_defer, &s->defer_cap, nxb * p.nzi / 32 + nxb + p.nzi + 1)) {
-      if (err) *err = "deferred-tile list allocation failed";
-      return QPSDM_ENOMEM;
-    }
+    for (GroupSet &g : s->sets)
+      if (!grow_dev(&g.d_defer, &g.defer_cap, nxb * p.nzi / 32 + nxb + p.nzi + 1)) {
+        if (err) *err = "deferred-tile list allocation failed";
+        return QPSDM_ENOMEM;
+      }
+    select_set(s, s->cur_set);
   }
   if (p.kahan) {
     const size_t n = (size_t)(o.ixend - o.ixstart) * p.nzi * nlines;
@@ -1811,33 +1874,42 @@ __global__ void __launch_bounds__(TZ *TX, MB)
 static int batched_alloc(PhysicsState *s, const qpsdm_static_params &p) {
   const int n = p.max_batch;
   bool ok = true;
-  for (int i = 0; i < 2; ++i) {
-    ok &= cudaMalloc(&s->d_key[i], sizeof(unsigned long long) * n) == cudaSuccess;
-    ok &= cudaMalloc(&s->d_val[i], sizeof(int) * n) == cudaSuccess;
+  for (GroupSet &g : s->sets) {
+    for (int i = 0; i < 2; ++i) {
+      ok &= cudaMalloc(&g.d_key[i], sizeof(unsigned long long) * n) == cudaSuccess;
+      ok &= cudaMalloc(&g.d_val[i], sizeof(int) * n) == cudaSuccess;
+    }
+    ok &= cudaMalloc(&g.d_ukey, sizeof(unsigned long long) * n) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_count, sizeof(int) * n) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_off, sizeof(int) * n) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_nruns, sizeof(int)) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_srcflag, sizeof(int) * n) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_sid, sizeof(int) * n) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_srcpos, sizeof(float2) * n) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_mem, sizeof(int4) * n) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_grppos, sizeof(float2) * n) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_memgrp, sizeof(int) * n) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_tile_ctr, sizeof(int)) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_ndefer, sizeof(int)) == cudaSuccess;
+    ok &= cudaMalloc(&g.d_nmem, sizeof(int)) == cudaSuccess;
   }
-  ok &= cudaMalloc(&s->d_ukey, sizeof(unsigned long long) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_count, sizeof(int) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_off, sizeof(int) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_nruns, sizeof(int)) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_srcflag, sizeof(int) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_sid, sizeof(int) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_srcpos, sizeof(float2) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_mem, sizeof(int4) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_grppos, sizeof(float2) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_memgrp, sizeof(int) * n) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_tile_ctr, sizeof(int)) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_ndefer, sizeof(int)) == cudaSuccess;
-  ok &= cudaMalloc(&s->d_nmem, sizeof(int)) == cudaSuccess;
   if (!ok) return QPSDM_ENOMEM;
+  GroupSet &g0 = s->sets[0];
   size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, b1, s->d_key[0], s->d_key[1], s->d_val[0],
-                                  s->d_val[1], n);
-  cub::DeviceRunLengthEncode::Encode(nullptr, b2, s->d_key[1], s->d_ukey, s->d_count,
-                                     s->d_nruns, n);
-  cub::DeviceScan::ExclusiveSum(nullptr, b3, s->d_count, s->d_off, n);
-  cub::DeviceScan::InclusiveSum(nullptr, b4, s->d_srcflag, s->d_sid, n);
+  cub::DeviceRadixSort::SortPairs(nullptr, b1, g0.d_key[0], g0.d_key[1], g0.d_val[0],
+                                  g0.d_val[1], n);
+  cub::DeviceRunLengthEncode::Encode(nullptr, b2, g0.d_key[1], g0.d_ukey, g0.d_count,
+                                     g0.d_nruns, n);
+  cub::DeviceScan::ExclusiveSum(nullptr, b3, g0.d_count, g0.d_off, n);
+  cub::DeviceScan::InclusiveSum(nullptr, b4, g0.d_srcflag, g0.d_sid, n);
   s->cub_bytes = std::max(std::max(b1, b2), std::max(b3, b4));
-  if (cudaMalloc(&s->d_cub, s->cub_bytes) != cudaSuccess) return QPSDM_ENOMEM;
+  for (GroupSet &g : s->sets)
+    if (cudaMalloc(&g.d_cub, s->cub_bytes) != cudaSuccess) return QPSDM_ENOMEM;
+  if (cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess)
+    return QPSDM_ECUDA;
+  select_set(s, 0);
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -2224,31 +2296,46 @@ int physics_process(PhysicsState *s, const qpsdm_static_params &p,
   rc = run_panels(s, p, b, s->d_any, 1, st, err);
   b.prof->end(st);
   if (rc) return rc;
-  for (int il = 0; il < b.nlines; ++il) {
+  // Lines alternate between the engine's stream (grouping set 0) and the
+  // second stream (set 1), which starts after the panels; the engine's stream
+  // waits for the second one before returning, so the next batch (which
+  // rewrites the panels) and any read of the image come after every line.
+  int nactive = 0;
+  for (int il = 0; il < b.nlines; ++il) nactive += batch_line_on(b, il);
+  const bool forked = nactive > 1;
+  if (forked && (cudaEventRecord(s->ev_fork, st) != cudaSuccess ||
+                 cudaStreamWaitEvent(s->aux, s->ev_fork, 0) != cudaSuccess))
+    return QPSDM_ECUDA;
+  int nrun = 0;
+  for (int il = 0; il < b.nlines && !rc; ++il) {
     if (!batch_line_on(b, il)) continue;
+    const int set = nrun++ & 1;
+    cudaStream_t ss = set ? s->aux : st;
+    select_set(s, set);
     const LineView v = view(il);
-    b.prof->begin(QPSDM_K_OTHER, st);
-    rc = batched_group(s, p, v, b, st);
-    b.prof->end(st);
+    b.prof->begin(QPSDM_K_OTHER, ss);
+    rc = batched_group(s, p, v, b, ss);
+    b.prof->end(ss);
     if (rc) {
       if (err) *err = "batched grouping failed";
-      return rc;
+      break;
     }
     const PhysImageArgs a = image_args(s, p, lines[il], o, b.nxz);
-    b.prof->begin(QPSDM_K_IMAGE, st);
+    b.prof->begin(QPSDM_K_IMAGE, ss);
     if (s->dtype == QPSDM_PANEL_FP32)
-      rc = launch_batched_image<float>(s, a, b, v, st);
+      rc = launch_batched_image<float>(s, a, b, v, ss);
     else if (s->dtype == QPSDM_PANEL_BF16)
-      rc = launch_batched_image<__nv_bfloat16>(s, a, b, v, st);
+      rc = launch_batched_image<__nv_bfloat16>(s, a, b, v, ss);
     else
-      rc = launch_batched_image<__half>(s, a, b, v, st);
-    b.prof->end(st);
-    if (rc) {
-      if (err) *err = "batched image launch failed";
-      return rc;
-    }
+      rc = launch_batched_image<__half>(s, a, b, v, ss);
+    b.prof->end(ss);
+    if (rc && err) *err = "batched image launch failed";
   }
-  return QPSDM_OK;
+  if (forked && (cudaEventRecord(s->ev_join, s->aux) != cudaSuccess ||
+                 cudaStreamWaitEvent(st, s->ev_join, 0) != cudaSuccess) && !rc)
+    rc = QPSDM_ECUDA;
+  select_set(s, 0);
+  return rc;
 }
 
 int physics_tuning(const PhysicsState *s, int *variant, int *tz, int *tx, int *mb,
