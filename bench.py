@@ -702,10 +702,11 @@ def run_form(form, wl, args, dev, dist, *, steps, warmup, e2e=True, clocks=True)
         kms = {k: v[0] / nst for k, v in kte.items()}
         img_launch = kte["image"][0] / max(kte["image"][1], 1)
         # consecutive lines run on two streams, so launch durations overlap:
-        # the image kernel's share of the step is the step's wall time less
+        # the image kernel's share of a timed step is the step's time less
         # the gate and the panels (the grouping kernels, 1-3 % of it, run
         # beside the other stream's image launch and stay in)
-        img_effective = (wall - kms["gate"] - kms["panels"]) / max(kte["image"][1] / nst, 1)
+        img_effective = ((ms / steps - kms["gate"] - kms["panels"])
+                         / max(kte["image"][1] / nst, 1))
         kms["eager_step_wall"] = wall
     t = torch.tensor([ms, float(npt)], dtype=torch.float64, device="cuda")
     if dist:
@@ -919,7 +920,7 @@ def run_ours(args, rank, world, dist):
                          "(1 - kept_fraction) execute none of them, pairs that fail the dip "
                          "test or the time window (kept - imaged) about half",
             "kernel_ms_per_launch": head["image_ms_per_launch"],
-            "kernel_ms_note": "effective time per launch: the eager step's wall time less the "
+            "kernel_ms_note": "effective time per launch: the timed step's time less the "
                               "gate and panel kernels, over the step's image launches "
                               "(consecutive lines run on two streams and their launches "
                               "overlap; each launch's own duration is "

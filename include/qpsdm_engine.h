@@ -259,7 +259,11 @@ int qpsdm_image_device_ptr(qpsdm_engine *e, float **d_img);
 /* Runs the engine's kernels on `stream` (a cudaStream_t of the engine's
  * device) instead of its own stream; NULL restores the engine's stream.
  * Lets a caller order engine work with its own kernels, time it with its own
- * events, or capture it into a CUDA graph. */
+ * events, or capture it into a CUDA graph.  In the batched physics form the
+ * lines of a brick alternate between this stream and an internal second
+ * stream, which forks from this stream after the batch's panels and joins
+ * it again before the submit's work ends, so everything a submit enqueues is
+ * ordered before the stream's later work (and captured with it). */
 int qpsdm_set_stream(qpsdm_engine *e, void *stream);
 
 /* Kernel timing: with profiling on, every launch of the engine is bracketed

@@ -699,6 +699,39 @@ def _solve_grids(L, d_models, src, n: int, nz: int, h: float, max_batch: int, de
         on_batch(d_T[0], d_S[0], d_T[1], d_S[1], grid, d_sp, s0, ns)
 
 
+def config4_eval_points(*, n_side: int, spacing: float, stride: int, n: int, nz: int,
+                        h: float, held: int, held_nodes: int, seed: int):
+    """Where configuration 4's network is evaluated: `held` seeded source
+    positions on the h lattice between the solved sources (every `stride`-th
+    of the n_side x n_side grid every `spacing` m), away from the grid's
+    edge; the four solved sources around each (corners [4*held] in the order
+    (0,0), (1,0), (0,1), (1,1)); and `held_nodes` seeded volume nodes per
+    position, on the h lattice, inside the position's own n x n x nz grid and
+    the corners' grids (grids centred on their source by _local_origin).
+    Returns hx, hy, ix, iy (the lower corner's grid indices), step, corners,
+    nodes [held][held_nodes][3] (x, y, z)."""
+    rng = np.random.default_rng([seed, 4])
+    step = spacing * stride
+    lim = (n_side - 1) // stride * step
+    hx = (np.round(rng.uniform(step, lim - step, held) / h) * h).astype(np.float32)
+    hy = (np.round(rng.uniform(step, lim - step, held) / h) * h).astype(np.float32)
+    ix = np.floor(hx / step).astype(int)
+    iy = np.floor(hy / step).astype(int)
+    corners = []
+    for dy in (0, 1):
+        for dx in (0, 1):
+            corners.append(np.stack([(ix + dx) * step, (iy + dy) * step], 1))
+    corners = np.concatenate(corners).astype(np.float32)
+    half = ((n - 1) // 2) * h - step - h
+    nodes = np.empty((held, held_nodes, 3), np.float64)
+    for k in range(held):
+        px = np.round((hx[k] + rng.uniform(-half, half, held_nodes)) / h) * h
+        py = np.round((hy[k] + rng.uniform(-half, half, held_nodes)) / h) * h
+        pz = rng.integers(1, nz, held_nodes) * h
+        nodes[k] = np.stack([px, py, pz], 1)
+    return hx, hy, ix, iy, step, corners, nodes
+
+
 def config4_training(model, background, *, q_bg: float, n_side: int = 64,
                      spacing: float = 80.0, stride: int = 1, n: int = 256, nz: int = 201,
                      h: float = 20.0, per_source: int = 4096, steps: int = 4000,
@@ -752,30 +785,10 @@ def config4_training(model, background, *, q_bg: float, n_side: int = 64,
     torch.cuda.synchronize(dev)
     t2 = time.perf_counter()
 
-    # evaluated positions: between solved sources, away from the grid's edge
-    rng = np.random.default_rng([seed, 4])
-    step = spacing * stride
-    lim = (n_side - 1) // stride * step
-    hx = (np.round(rng.uniform(step, lim - step, held) / h) * h).astype(np.float32)
-    hy = (np.round(rng.uniform(step, lim - step, held) / h) * h).astype(np.float32)
+    hx, hy, ix, iy, step, corners, nodes = config4_eval_points(
+        n_side=n_side, spacing=spacing, stride=stride, n=n, nz=nz, h=h, held=held,
+        held_nodes=held_nodes, seed=seed)
     hsrc = np.stack([hx, hy], 1)
-    # corners: the four solved sources around each evaluated position
-    ix = np.floor(hx / step).astype(int)
-    iy = np.floor(hy / step).astype(int)
-    corners = []
-    for dy in (0, 1):
-        for dx in (0, 1):
-            corners.append(np.stack([(ix + dx) * step, (iy + dy) * step], 1))
-    corners = np.concatenate(corners).astype(np.float32)      # [4*held] (00,10,01,11)
-    # evaluated nodes: on the h lattice (all five grids hold them), inside the
-    # evaluated source's grid and within reach of the corners' grids
-    half = ((n - 1) // 2) * h - step - h
-    nodes = np.empty((held, held_nodes, 3), np.float64)
-    for k in range(held):
-        px = np.round((hx[k] + rng.uniform(-half, half, held_nodes)) / h) * h
-        py = np.round((hy[k] + rng.uniform(-half, half, held_nodes)) / h) * h
-        pz = rng.integers(1, nz, held_nodes) * h
-        nodes[k] = np.stack([px, py, pz], 1)
 
     def values(points_src, grids_T, grids_S, grids_Tb, grids_Sb, s0, ns, which):
         """Background-corrected (T, t*) of sources s0..s0+ns-1 at the evaluated
