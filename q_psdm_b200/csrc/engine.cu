@@ -87,6 +87,7 @@ struct qpsdm_engine {
     float *host = nullptr;
     size_t n = 0;
     int scale = 0;
+    float nsb = 1.0f;  // the offset group's nsb when the read was enqueued
     int64_t ticket = -1;
   };
   ImageRead reads[kReads];
@@ -619,7 +620,7 @@ int finish_read(qpsdm_engine *e, qpsdm_engine::ImageRead &r) {
   if (r.ticket < 0) return QPSDM_OK;
   CK(cudaEventSynchronize(r.done));
   if (r.scale)
-    for (size_t i = 0; i < r.n; ++i) r.host[i] /= e->off.nsb;  // src/q-psdm.cu:1761-1765
+    for (size_t i = 0; i < r.n; ++i) r.host[i] /= r.nsb;  // src/q-psdm.cu:1761-1765
   r.ticket = -1;
   return QPSDM_OK;
 }
@@ -652,6 +653,7 @@ extern "C" int qpsdm_get_image_async(qpsdm_engine *e, float *host_img, int apply
   r.host = host_img;
   r.n = n;
   r.scale = apply_nsb_scale != 0;
+  r.nsb = (float)e->off.nsb;
   r.ticket = e->next_ticket;
   *ticket = e->next_ticket++;
   return QPSDM_OK;
