@@ -109,7 +109,7 @@ struct PhysicsState {
   int variant = -1;          // batched kernel variant (autotuned)
   float *d_tune = nullptr;   // scratch image of the autotuner
   size_t tune_cap = 0;
-  float tune_ms[24] = {};    // autotuner timings per variant (ms)
+  float tune_ms[32] = {};    // autotuner timings per variant (ms)
   // the two grouping sets (the d_key .. d_cub fields above are the selected
   // one) and the second stream of the line loop
   GroupSet sets[2];
@@ -659,6 +659,42 @@ __device__ __forceinline__ bool grid_pos(float px, float py, float xc, float rdx
   fx = __fmaf_rn(__fsub_rn(px, xc), rdx, hx);
   fy = __fmaf_rn(py, rdy, hy);
   return fx >= 0.0f && fx <= (float)(nxs - 1) && fy >= 0.0f && fy <= (float)(nys - 1);
+}
+
+// Packed FP32 pairs (sm_100's f32x2 instructions): two values in one 64-bit
+// register pair, one instruction for both.  Each operation is the IEEE
+// single-precision operation of each half (round to nearest), the same
+// result as two scalar ones.
+__device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float2 f2_unpack(unsigned long long r) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return v;
+}
+__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
 }
 
 // a + w (b - a) as one fused multiply-add (the form every table and sample
@@ -1543,8 +1579,12 @@ __device__ __forceinline__ bool lookup_uni(const TileGrid &g, const float2 *__re
 // A = (T, t* / dtstar, CS = ds^3 / ts, AZ), B = (PX1, PX2, PY1, PY2).  One
 // reciprocal per pair: inv = 1 / (uz r tt) gives both the taper's 1 / uz
 // (r tt inv) and the weight's 1 / (r tt) (uz inv), tt = t^2 (0.01 below
-// 0.1 s).
-template <int TZ, int TX, int MB, int U, int MW, typename T>
+// 0.1 s).  PK (two members per block): the two members' pick, weight and
+// sample blend run as packed FP32 pairs (one f32x2 instruction for both
+// members; minima, conversions and the sums stay scalar); every value that
+// decides a pair -- t, t / dt1, the t* bin -- is the same IEEE add or
+// multiply as in the scalar walk, so the same pairs are imaged.
+template <int TZ, int TX, int MB, int U, int MW, bool PK, typename T>
 __global__ void __launch_bounds__(TZ *TX, MB)
     k_image_batched_fast(float *__restrict__ img, float *__restrict__ comp, PhysImageArgs a,
                        const float *__restrict__ dips, const int *__restrict__ memgrp,
@@ -1791,6 +1831,103 @@ __global__ void __launch_bounds__(TZ *TX, MB)
               val[u] = rec[u].w == g;
               if (val[u]) ++k;
             }
+            if constexpr (PK) {
+              static_assert(U == 2, "packed walk: two members per block");
+              bool on[2];
+              float4 A[2], B[2];
+#pragma unroll
+              for (int u = 0; u < 2; ++u) {
+                const int lo = rec[u].z >> 16, hi = rec[u].z & 0xFFFF;
+                const bool inr = val[u] && (unsigned)(lx - lo) <= (unsigned)(hi - lo);
+                B[u] = planeB[(size_t)(rec[u].y & 0xFF) * NT + tid];
+                on[u] = inr && B[u].x > qx1 && B[u].y > qx2 && B[u].z > qy1 && B[u].w > qy2;
+              }
+              if (!(on[0] || on[1])) continue;
+#pragma unroll
+              for (int u = 0; u < 2; ++u) A[u] = planeA[(size_t)(rec[u].y & 0xFF) * NT + tid];
+              const unsigned long long Ax = f2_pack(A[0].x, A[1].x), Ay = f2_pack(A[0].y, A[1].y);
+              const unsigned long long Az = f2_pack(A[0].z, A[1].z), Aw = f2_pack(A[0].w, A[1].w);
+              const unsigned long long uz = f2_add(Aw, f2_pack(agz, agz));
+              const float2 ex1 = f2_unpack(f2_mul(f2_sub(f2_pack(B[0].x, B[1].x), f2_pack(qx1, qx1)),
+                                                  f2_pack(iwx1, iwx1)));
+              const float2 ex2 = f2_unpack(f2_mul(f2_sub(f2_pack(B[0].y, B[1].y), f2_pack(qx2, qx2)),
+                                                  f2_pack(iwx2, iwx2)));
+              const float2 ey1 = f2_unpack(f2_mul(f2_sub(f2_pack(B[0].z, B[1].z), f2_pack(qy1, qy1)),
+                                                  f2_pack(iwy1, iwy1)));
+              const float2 ey2 = f2_unpack(f2_mul(f2_sub(f2_pack(B[0].w, B[1].w), f2_pack(qy2, qy2)),
+                                                  f2_pack(iwy2, iwy2)));
+              const unsigned long long t = f2_add(Ax, f2_pack(tg, tg));
+              const unsigned long long ft = f2_mul(t, f2_pack(inv_dt1, inv_dt1));
+              const float2 ftv = f2_unpack(ft), tv = f2_unpack(t);
+              const float2 fbr = f2_unpack(f2_add(Ay, f2_pack(qg, qg)));
+              const int it0 = (int)ftv.x, it1v = (int)ftv.y;
+              on[0] = on[0] && it0 > 0 && it0 + 1 < a.nt;
+              on[1] = on[1] && it1v > 0 && it1v + 1 < a.nt;
+              const float fb0 = fminf(fmaxf(fbr.x, 0.0f), (float)(a.nbins - 1));
+              const float fb1 = fminf(fmaxf(fbr.y, 0.0f), (float)(a.nbins - 1));
+              const int b00 = min((int)fb0, a.nbins - 2), b01 = min((int)fb1, a.nbins - 2);
+              const unsigned long long fwt = f2_sub(ft, f2_pack((float)it0, (float)it1v));
+              const unsigned long long fwb =
+                  f2_sub(f2_pack(fb0, fb1), f2_pack((float)b00, (float)b01));
+              // w v (r + 1/r) = w (r^2 + 1) 100 / (r tt), tt = t^2 (0.01 below 0.1 s)
+              const unsigned long long r = f2_mul(Az, f2_pack(gfac, gfac));
+              const float2 t2 = f2_unpack(f2_mul(t, t));
+              const unsigned long long rtt =
+                  f2_mul(r, f2_pack(tv.x > 0.1f ? t2.x : 0.01f, tv.y > 0.1f ? t2.y : 0.01f));
+              const float2 den = f2_unpack(f2_mul(uz, rtt));
+              const unsigned long long inv =
+                  f2_pack(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y));
+              const unsigned long long ruz = f2_mul(rtt, inv);
+              const float2 exr = f2_unpack(f2_mul(f2_pack(fminf(ex1.x, ex2.x), fminf(ex1.y, ex2.y)), ruz));
+              const float2 eyr = f2_unpack(f2_mul(f2_pack(fminf(ey1.x, ey2.x), fminf(ey1.y, ey2.y)), ruz));
+              const unsigned long long wt = f2_mul(f2_pack(fminf(1.0f, exr.x), fminf(1.0f, exr.y)),
+                                                   f2_pack(fminf(1.0f, eyr.x), fminf(1.0f, eyr.y)));
+              unsigned long long fac = f2_mul(f2_mul(wt, f2_fma(r, r, f2_pack(1.0f, 1.0f))),
+                                              f2_mul(f2_mul(f2_pack(100.0f, 100.0f), uz), inv));
+              if (std::is_same<T, __half>::value)  // 2^e from the records' exponent bits
+                fac = f2_mul(fac, f2_pack(
+                    __int_as_float((int)((((unsigned)rec[0].y >> 24) - 1u) << 23)),
+                    __int_as_float((int)((((unsigned)rec[1].y >> 24) - 1u) << 23))));
+              // samples (index clamped into the panel; loads only for imaged members)
+              const T *q0 = panels + (size_t)rec[0].x * pstride +
+                            (unsigned)(b00 * a.nt + min(max(it0, 0), a.nt - 2));
+              const T *q1 = panels + (size_t)rec[1].x * pstride +
+                            (unsigned)(b01 * a.nt + min(max(it1v, 0), a.nt - 2));
+              float s00 = 0.f, s01 = 0.f, s10 = 0.f, s11 = 0.f;
+              float u00 = 0.f, u01 = 0.f, u10 = 0.f, u11 = 0.f;
+              if (on[0]) {
+                s00 = ld_sample<T>(q0);
+                s01 = ld_sample<T>(q0 + 1);
+                s10 = ld_sample<T>(q0 + a.nt);
+                s11 = ld_sample<T>(q0 + a.nt + 1);
+              }
+              if (on[1]) {
+                u00 = ld_sample<T>(q1);
+                u01 = ld_sample<T>(q1 + 1);
+                u10 = ld_sample<T>(q1 + a.nt);
+                u11 = ld_sample<T>(q1 + a.nt + 1);
+              }
+              const unsigned long long p00 = f2_pack(s00, u00), p01 = f2_pack(s01, u01);
+              const unsigned long long p10 = f2_pack(s10, u10), p11 = f2_pack(s11, u11);
+              const unsigned long long sa = f2_fma(fwt, f2_sub(p01, p00), p00);
+              const unsigned long long sb = f2_fma(fwt, f2_sub(p11, p10), p10);
+              const float2 v = f2_unpack(f2_mul(fac, f2_fma(fwb, f2_sub(sb, sa), sa)));
+#pragma unroll
+              for (int u = 0; u < 2; ++u) {
+                if (!on[u]) continue;
+                ++cimg;
+                const float vu = u ? v.y : v.x;
+                if (comp) {
+                  const float y = vu - cmp;
+                  const float tt = acc + y;
+                  cmp = (tt - acc) - y;
+                  acc = tt;
+                } else {
+                  acc += vu;
+                }
+              }
+              continue;
+            }
             bool on[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -1940,7 +2077,7 @@ struct LineView {
 // the extra loads in flight gain.)
 // Variants from 13 on are the fast form (k_image_batched_fast, with
 // k_image_batched over the tiles it leaves) with mw words of 32 members per
-// chunk.
+// chunk; cl = 2: the walk on packed FP32 pairs.
 struct BatchedVariant {
   int tz, tx, mb, sc, u, cl, mw;
 };
@@ -1952,10 +2089,11 @@ static const BatchedVariant kVariants[] = {
     {16, 8, 5, 8, 4, 0, 0},   {8, 16, 5, 8, 4, 1, 16},  {8, 16, 4, 8, 4, 1, 32},
     {16, 8, 5, 8, 4, 1, 16},  {32, 4, 5, 8, 4, 1, 16},  {8, 16, 4, 16, 4, 1, 16},
     {16, 8, 4, 8, 4, 1, 32},  {8, 16, 6, 8, 2, 1, 8},   {8, 16, 6, 8, 4, 1, 8},
-    {16, 8, 6, 8, 2, 1, 8},   {8, 16, 5, 8, 2, 1, 16},
+    {16, 8, 6, 8, 2, 1, 8},   {8, 16, 5, 8, 2, 1, 16},  {8, 16, 6, 8, 2, 2, 8},
+    {8, 16, 5, 8, 2, 2, 8},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
-static_assert(kNumVariants <= 24, "tune_ms holds 24 timings");
+static_assert(kNumVariants <= 32, "tune_ms holds 32 timings");
 
 // The original kernel over every tile of the image, or (tile_list) over the
 // *ntile_list tiles of a list, with one persistent CTA per SM.
@@ -1987,7 +2125,7 @@ static int launch_batched_tile(PhysicsState *s, const PhysImageArgs &a, const Ph
 // The fast form over the image's uniform tiles, then the original kernel
 // (same tile shape, MBO blocks per SM) over the tiles it left; with unpaired
 // tables the original kernel takes every tile.
-template <int TZ, int TX, int MB, int U, int MW, int MBO, typename T>
+template <int TZ, int TX, int MB, int U, int MW, int MBO, typename T, bool PK = false>
 static int launch_batched_fast(PhysicsState *s, const PhysImageArgs &a, const PhysicsBatch &b,
                                const LineView &v, float *img, float *comp,
                                unsigned long long *npt, int sc, cudaStream_t st) {
@@ -1996,7 +2134,7 @@ static int launch_batched_fast(PhysicsState *s, const PhysImageArgs &a, const Ph
   const int ntz = (a.nzi + TZ - 1) / TZ, ntx = (a.nxb + TX - 1) / TX;
   if ((size_t)ntz * ntx > s->defer_cap) return QPSDM_EINVAL;  // cannot happen: sized per offset
   const size_t smem = sizeof(float4) * 2 * (size_t)sc * TZ * TX;
-  auto kern = k_image_batched_fast<TZ, TX, MB, U, MW, T>;
+  auto kern = k_image_batched_fast<TZ, TX, MB, U, MW, PK, T>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return QPSDM_ECUDA;
@@ -2031,6 +2169,8 @@ static int launch_variant(int vi, PhysicsState *s, const PhysImageArgs &a, const
     case 20: return launch_batched_fast<8, 16, 6, 4, 8, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 21: return launch_batched_fast<16, 8, 6, 2, 8, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 22: return launch_batched_fast<8, 16, 5, 2, 16, 4, T>(s, a, b, v, img, comp, npt, sc, st);
+    case 23: return launch_batched_fast<8, 16, 6, 2, 8, 4, T, true>(s, a, b, v, img, comp, npt, sc, st);
+    case 24: return launch_batched_fast<8, 16, 5, 2, 8, 4, T, true>(s, a, b, v, img, comp, npt, sc, st);
     case 0: return launch_batched_tile<32, 8, 2, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 1: return launch_batched_tile<32, 4, 4, 4, T>(s, a, b, v, img, comp, npt, sc, st);
     case 2: return launch_batched_tile<32, 4, 6, 4, T>(s, a, b, v, img, comp, npt, sc, st);

@@ -290,7 +290,7 @@ class Engine:
     def tuning(self) -> dict:
         """The batched form's autotuned image-kernel variant and timings."""
         v, tz, tx, mb = C.c_int(), C.c_int(), C.c_int(), C.c_int()
-        ms = np.zeros(24, np.float32)
+        ms = np.zeros(32, np.float32)
         n = lib().qpsdm_tuning_info(self.h, C.byref(v), C.byref(tz), C.byref(tx),
                                     C.byref(mb), ms.ctypes.data, ms.size)
         if n < 0:

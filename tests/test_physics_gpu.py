@@ -315,7 +315,7 @@ def test_fp16_panels_any_amplitude(cuda, case, form, gain):
     assert nrmse(img, case["o_img"]) <= 2.5e-4
 
 
-@pytest.mark.parametrize("variant", list(range(1, 24)))
+@pytest.mark.parametrize("variant", list(range(1, 26)))
 def test_every_batched_variant(cuda, case, variant):
     """Each launch variant the autotuner may pick (tile, blocks per SM, source
     chunk, the original or the compacted kernel) images the same as the FP64
@@ -351,7 +351,8 @@ def test_compacted_kernel_counts_equal_original(cuda, case, orig, compact):
     assert nrmse(b, a) <= 1e-5
 
 
-@pytest.mark.parametrize("fast,orig", [(14, 11), (20, 11), (23, 11), (22, 13), (16, 13), (17, 2)])
+@pytest.mark.parametrize("fast,orig", [(14, 11), (20, 11), (23, 11), (22, 13), (16, 13), (17, 2),
+                                       (24, 11), (25, 11)])
 def test_fast_form_defers_straddling_tiles(cuda, fast, orig):
     """An image block starting at cdp 30 puts table-cell edges (every 16 cdps)
     inside tiles: the fast form leaves those tiles to the original kernel
@@ -372,3 +373,26 @@ def test_fast_form_defers_straddling_tiles(cuda, fast, orig):
     assert sa == sb
     assert nrmse(b, a) <= 1e-5
     assert nrmse(b, ref) <= 2.5e-4
+
+
+@pytest.mark.parametrize("scalar,packed", [(20, 24), (20, 25)])
+def test_packed_walk_equals_scalar_walk(cuda, scalar, packed):
+    """The walk on packed FP32 pairs (two members per f32x2 instruction)
+    images exactly the pairs the scalar walk images -- every deciding value
+    is the same IEEE operation -- with equal counters and the image equal to
+    FP32 rounding, FP16 and FP32 panels, also with tiles left to the
+    original kernel (an image block starting at cdp 30) and Kahan sums."""
+    for c, kw in ((make_case(nshots=2), dict(panel_dtype=2)),
+                  (make_case(nshots=2), dict(panel_dtype=0, kahan=1)),
+                  (make_case(nshots=2, ixstart=30, ixend=126), dict(panel_dtype=2))):
+        out = {}
+        for v in (scalar, packed):
+            eng, p, o = engine(c, form=1, variant=v, **kw)
+            try:
+                eng.submit(records(c))
+                out[v] = (eng.get_image(False), eng.stats())
+            finally:
+                eng.close()
+        (a, sa), (b, sb) = out[scalar], out[packed]
+        assert sa == sb
+        assert np.abs(b - a).max() <= 1e-6 * np.abs(a).max()
