@@ -107,8 +107,16 @@ def tune_batch_shape(make_engine, batches_of, estimate, candidates, *, steps: in
             c.skipped = (f"estimated {c.estimate_bytes / 1e9:.1f} GB > {hbm_share:.0%} of "
                          f"{free0 / 1e9:.1f} GB free")
             continue
-        bats = batches_of(g)
-        eng, stream = make_engine(g, nl)
+        bats = None
+        try:
+            bats = batches_of(g)
+            eng, stream = make_engine(g, nl)
+        except Exception as exc:  # e.g. out of device memory despite the estimate
+            c.skipped = f"not built: {exc}"
+            del bats
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            continue
         try:
             eng.submit_device(bats[0][0].data_ptr(), bats[0][1])
             torch.cuda.synchronize()
