@@ -221,7 +221,16 @@ bool read_header(FILE *fp, long k, int ns, TraceHdr &t) {
 struct Tables {
   int cdp1 = 0, cdp2 = 0, nzg = 0, nxg = 0, nzi1 = 0, nxi1 = 0;
   std::vector<qpsdm_ttt_desc> desc;
-  std::vector<float> data;
+  std::vector<float> data;     // values of the bracketing line lo
+  std::vector<float> data_hi;  // values of line hi (empty when the line has its own file)
+  int lo = 0, hi = 0;
+  float *d = nullptr;          // the line's values on the device (tables_on_device)
+  Tables() = default;
+  Tables(const Tables &) = delete;
+  Tables &operator=(const Tables &) = delete;
+  ~Tables() {
+    if (d) cudaFree(d);
+  }
 };
 bool load_tables(const std::string &ttpath, bool q, int line, int line1, int line2, Tables &t) {
   const std::string idx = ttpath + (q ? "/Lxxx.qidx" : "/Lxxx.tidx");
@@ -278,14 +287,45 @@ bool load_tables(const std::string &ttpath, bool q, int line, int line1, int lin
     std::fclose(f);
   };
   read_all(lo, t.data);
+  t.lo = lo;
+  t.hi = hi;
+  t.data_hi.clear();
   if (hi != lo) {
-    std::vector<float> b;
-    read_all(hi, b);
-    if (b.size() != t.data.size()) die("table sizes of lines %d and %d differ", lo, hi);
-    const float c2 = (float)(1.0 * (line - lo) / (hi - lo)), c1 = 1.0f - c2;
-    for (size_t i = 0; i < b.size(); ++i) t.data[i] = t.data[i] * c1 + b[i] * c2;
+    read_all(hi, t.data_hi);
+    if (t.data_hi.size() != t.data.size()) die("table sizes of lines %d and %d differ", lo, hi);
   }
   return true;
+}
+
+// The line's table values on the current device: line lo's values, or the
+// interpolation between lines lo and hi with get_ttt_all's float arithmetic
+// (src/q-psdm.cu:2584-2596), computed on the GPU by qpsdm_tables_lerp
+// instead of a host loop over the tens of millions of values of a line.
+// The host copies are released; the engine copies the device values at
+// qpsdm_set_lines.
+float *tables_on_device(Tables &t, int line) {
+  const size_t n = t.data.size(), bytes = n * sizeof(float);
+  auto ck = [&](cudaError_t c, const char *what) {
+    if (c != cudaSuccess) die("tables of line %d: %s: %s", line, what, cudaGetErrorString(c));
+  };
+  ck(cudaMalloc(&t.d, bytes ? bytes : sizeof(float)), "cudaMalloc");
+  if (t.data_hi.empty()) {
+    ck(cudaMemcpy(t.d, t.data.data(), bytes, cudaMemcpyHostToDevice), "upload");
+  } else {
+    float *d_lo = nullptr, *d_hi = nullptr;
+    ck(cudaMalloc(&d_lo, bytes), "cudaMalloc");
+    ck(cudaMalloc(&d_hi, bytes), "cudaMalloc");
+    ck(cudaMemcpy(d_lo, t.data.data(), bytes, cudaMemcpyHostToDevice), "upload");
+    ck(cudaMemcpy(d_hi, t.data_hi.data(), bytes, cudaMemcpyHostToDevice), "upload");
+    if (qpsdm_tables_lerp(d_lo, d_hi, (int64_t)n, line, t.lo, t.hi, t.d, nullptr) != QPSDM_OK)
+      die("tables of line %d: qpsdm_tables_lerp failed", line);
+    ck(cudaDeviceSynchronize(), "interpolation");
+    cudaFree(d_lo);
+    cudaFree(d_hi);
+  }
+  std::vector<float>().swap(t.data);
+  std::vector<float>().swap(t.data_hi);
+  return t.d;
 }
 
 // ---------------------------------------------------------------------------
@@ -644,6 +684,7 @@ int main(int argc, char **argv) {
   const int naz = qpsdm_build_iaztab(sp.eps, iaz.data(), (int)iaz.size());
   qpsdm_engine *eng = nullptr;
   check_engine(qpsdm_engine_create(&sp, iaz.data(), naz, igpu, &eng), nullptr, "engine create");
+  cudaSetDevice(igpu);  // the driver's own device buffers (tables) on the engine's GPU
 
   // constant dip limits (src/q-psdm.cu:1463-1472): the argument summed in
   // double and rounded to float, then the float tangent
@@ -717,10 +758,10 @@ int main(int argc, char **argv) {
         lp.ttt_cdp2 = tt[j].cdp2;
         lp.ttt_desc = tt[j].desc.data();
         lp.qqq_desc = tq[j].desc.data();
-        lp.ttt = tt[j].data.data();
-        lp.qqq = tq[j].data.data();
         lp.ttt_len = (int64_t)tt[j].data.size();
         lp.qqq_len = (int64_t)tq[j].data.size();
+        lp.ttt = tables_on_device(tt[j], line);
+        lp.qqq = tables_on_device(tq[j], line);
       }
     }
     check_engine(qpsdm_set_lines(eng, lps.data(), nl), eng, "set_lines");
